@@ -1,0 +1,188 @@
+/*
+ * spectral_gpu.h - C ABI of the B200 per-timestep hot path of spectral_rs.
+ *
+ * This is the drop-in boundary.  The reference (pcrumley/spectral_rs, Rust) has
+ * no FFI; its hot path is the crate-internal API that `run` (src/lib.rs:119-202)
+ * calls.  Each entry point below names the reference method it replaces, so a
+ * `#[cfg(feature = "gpu")]` body of that method can forward to it.
+ *
+ * Conventions
+ *   - Every call returns an int status: 0 (SPX_OK) on success, a positive
+ *     SPX_ERR_* code otherwise; spx_last_error() gives the message.  The
+ *     reference panics on its asserts (e.g. src/prtls.rs:98-102,154-171); here
+ *     those asserts become SPX_ERR_BOUNDS / SPX_ERR_WALL statuses.
+ *   - Device memory belongs to the context.  Host pointers are caller-owned and
+ *     copied; no host pointer is retained after a call returns.
+ *   - One host thread and one CUDA stream per context.  Calls are ordered on
+ *     that stream; getters synchronize it.
+ *   - Arithmetic is FP32 (the reference's default `Float`, src/lib.rs:18-19).
+ *     There is no FP64 device path and no CPU fallback inside the library.
+ *   - Grid layouts are the reference's: a spatial field is row-major
+ *     (size_y+2) x (size_x+2) with a one-cell ghost frame (src/flds/field.rs:57);
+ *     particle cell indices include the +1 ghost offset (src/prtls.rs:206-207).
+ */
+#ifndef SPECTRAL_GPU_H
+#define SPECTRAL_GPU_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SPX_API __attribute__((visibility("default")))
+#else
+#define SPX_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPX_OK 0
+#define SPX_ERR_ARG 1        /* invalid argument or unsupported size            */
+#define SPX_ERR_CUDA 2       /* a CUDA runtime call failed                      */
+#define SPX_ERR_BOUNDS 3     /* particle index out of the grid (ix or iy == 0)  */
+#define SPX_ERR_WALL 4       /* reflecting-wall assertion (src/prtls.rs:154-171) */
+#define SPX_ERR_NOMEM 5      /* device allocation failed                        */
+#define SPX_ERR_STATE 6      /* call out of order (e.g. no species yet)         */
+#define SPX_ERR_GAMMA 7      /* supplied Lorentz factors inconsistent with p    */
+#define SPX_ERR_TIMEOUT 8    /* a bounded device wait gave up                    */
+
+/* Field ids (the reference's Flds members, src/flds/mod.rs:15-37). */
+#define SPX_EX 0
+#define SPX_EY 1
+#define SPX_EZ 2
+#define SPX_BX 3
+#define SPX_BY 4
+#define SPX_BZ 5
+#define SPX_JX 6
+#define SPX_JY 7
+#define SPX_JZ 8
+#define SPX_DSTY 9 /* "Rho": charge density */
+#define SPX_DENS 10 /* number density        */
+#define SPX_NUM_FIELDS 11
+
+/* Particle paths. */
+#define SPX_PATH_SPLIT 0 /* integer cell + FP32 offset (the reference layout), fused, cell-ordered */
+#define SPX_PATH_PLAIN 1 /* global FP32 positions x = ix + dx, per-phase kernels, global atomics    */
+
+/* Simulation parameters.  The first block is the reference's [params] table
+ * (config.toml, src/lib.rs:56-66) plus its compile-time `periodic` feature;
+ * the second block is additive and defaults to 0 = automatic. */
+typedef struct spx_params {
+  uint64_t size_x;     /* cells in x, even (src/lib.rs:76); powers of two on the GPU FFT */
+  uint64_t size_y;     /* cells in y                                                      */
+  uint64_t delta;      /* wall offset (src/prtls.rs:153)                                  */
+  float dt;            /* time step in 1/omega_pe                                         */
+  float c;             /* speed of light in cells per 1/omega_pe                          */
+  uint32_t dens;       /* particles per cell per species (normalises rho, src/flds/mod.rs:80) */
+  float gamma_inj;     /* upstream Lorentz factor (init only)                             */
+  uint32_t n_pass;     /* binomial filter passes per step                                 */
+  int32_t periodic_x;  /* 1: periodic particles in x (cargo feature `periodic`), 0: wall  */
+  int32_t left_wall;   /* 1: also reflect at ix = delta+1, mirroring the right wall; 0: the
+                          reference's assertion min(ix) > delta (src/prtls.rs:163-170)     */
+  /* --- B200 additions (0 = automatic) --- */
+  int32_t path;        /* SPX_PATH_SPLIT or SPX_PATH_PLAIN                                */
+  int32_t tile_x;      /* cells per tile in x (split path); power of two                   */
+  int32_t tile_y;      /* cells per tile in y                                              */
+  int32_t slot_capacity; /* minimum particle slots per cell and species (split path);
+                          negative: exactly -slot_capacity (testing the overflow path)  */
+  int32_t device;      /* CUDA device ordinal                                              */
+} spx_params;
+
+typedef struct spx_ctx spx_ctx;
+
+/* Flds::new (src/flds/mod.rs:40-65) + Sim::new (src/lib.rs:247-264). */
+SPX_API int spx_create(const spx_params* params, spx_ctx** out);
+SPX_API int spx_destroy(spx_ctx* ctx);
+/* Message of the last failed call on ctx (or of the last failed spx_create if ctx is NULL). */
+SPX_API const char* spx_last_error(const spx_ctx* ctx);
+/* Static description of the library build (compile flags, arch). */
+SPX_API const char* spx_version(void);
+
+/* Prtl::new (src/prtls.rs:60-84) with caller-supplied state, in the order of
+ * the Prtl fields (src/prtls.rs:8-16).  `usize` cell indices cross as uint64.
+ * psa (Lorentz factors) must equal sqrt(1 + |p|^2 / c^2) as the reference keeps
+ * them (src/prtls.rs:237-249,440); the GPU recomputes it and does not store it.
+ * The species id (0, 1, ...) is written to *species_out. */
+SPX_API int spx_add_species(spx_ctx* ctx, float charge, float mass, float vth, uint64_t n, const uint64_t* ix,
+                    const uint64_t* iy, const float* dx, const float* dy, const float* px, const float* py,
+                    const float* pz, const float* psa, int32_t* species_out);
+
+/* Seeded on-device initialisation (replaces src/prtls.rs:191-261, whose RNG is
+ * unseeded): `ppc` particles per cell in columns [x0, x1) of every row,
+ * positions uniform in the cell (random_positions=1) or on the reference's
+ * diagonal (0); momenta Maxwellian N(0, vth*c) per component, then a drift
+ * with Lorentz factor gamma_drift along sign_x*x with the Zenitani flip
+ * (src/prtls.rs:240-249).  gamma_drift <= 1 means no drift. */
+SPX_API int spx_init_species(spx_ctx* ctx, float charge, float mass, float vth, uint32_t ppc, uint64_t x0, uint64_t x1,
+                     float gamma_drift, float sign_x, int32_t random_positions, uint64_t seed,
+                     int32_t* species_out);
+
+SPX_API uint64_t spx_species_count(const spx_ctx* ctx, int32_t species);
+SPX_API int32_t spx_num_species(const spx_ctx* ctx);
+
+/* Copy species state back in the reference's particle order.  Any pointer may
+ * be NULL to skip that array.  `stride` > 1 returns every stride-th particle,
+ * as save_output does (src/save/mod.rs:36-72). */
+SPX_API int spx_get_species(spx_ctx* ctx, int32_t species, uint64_t stride, uint64_t* ix, uint64_t* iy, float* dx,
+                    float* dy, float* px, float* py, float* pz, float* psa);
+
+/* Zero j_x, j_y, j_z, dsty, dens, ghosts included (src/lib.rs:157-167). */
+SPX_API int spx_zero_sources(spx_ctx* ctx);
+/* Sim::move_and_deposit (src/lib.rs:478-489) for one species. */
+SPX_API int spx_move_and_deposit(spx_ctx* ctx, int32_t species);
+/* Field::deposit_ghosts (src/flds/field.rs:260-373) on one field id. */
+SPX_API int spx_deposit_ghosts(spx_ctx* ctx, int32_t field);
+/* Flds::update (src/flds/mod.rs:87-309). */
+SPX_API int spx_fields_update(spx_ctx* ctx);
+/* Prtl::boris_push (src/prtls.rs:262-443) for one species. */
+SPX_API int spx_boris_push(spx_ctx* ctx, int32_t species);
+
+/* The pre-loop move+deposit and ghost fold of run() (src/lib.rs:130-142). */
+SPX_API int spx_prepare(spx_ctx* ctx);
+/* `n` iterations of run()'s loop body (src/lib.rs:151-200) without output:
+ * zero sources, move_and_deposit every species, fold, Flds::update,
+ * boris_push every species.  Production path: the push of step t is fused
+ * with the move+deposit of step t+1 and each step is one CUDA graph launch;
+ * the last push stays pending until a particle getter or a per-phase call
+ * needs it, so observable state always equals the reference's. */
+SPX_API int spx_step(spx_ctx* ctx, uint32_t n);
+/* Complete any pending push (see spx_step). */
+SPX_API int spx_flush(spx_ctx* ctx);
+SPX_API int spx_synchronize(spx_ctx* ctx);
+
+/* Field access in the reference layout: with_ghosts=1 copies (size_y+2)*(size_x+2)
+ * floats, 0 copies the size_y*size_x interior (save_fld_spatial, src/save/mod.rs:8-23). */
+SPX_API int spx_get_field(spx_ctx* ctx, int32_t field, int32_t with_ghosts, float* out);
+/* Overwrite a spatial field (with ghosts).  Used by tests to impose fields. */
+SPX_API int spx_set_field(spx_ctx* ctx, int32_t field, const float* in_with_ghosts);
+/* The persistent k-space magnetic field at t+1/2 (Flds::b_*_wrk, src/flds/mod.rs:31-33),
+ * size_y*size_x interleaved complex. comp 0,1,2 = x,y,z. */
+SPX_API int spx_get_bwrk(spx_ctx* ctx, int32_t comp, float* out_complex);
+SPX_API int spx_set_bwrk(spx_ctx* ctx, int32_t comp, const float* in_complex);
+
+/* FP64 device diagnostics: out[0] = sum E^2/2, out[1] = sum B^2/2 (interior
+ * cells), out[2] = sum over particles of m (gamma - 1) c^2, out[3] = sum of
+ * the interior of dsty (net deposited charge), out[4] = particle count. */
+SPX_API int spx_diag(spx_ctx* ctx, double* out5);
+
+/* Standalone field operations on caller arrays (the reference's Field and
+ * Fft2D methods, used by the known-answer tests): op 0 = deposit_ghosts,
+ * 1 = update_ghosts, 2 = n_pass x binomial_filter_2_d.  In/out in place. */
+SPX_API int spx_field_op(uint64_t size_x, uint64_t size_y, int32_t op, uint32_t n_pass, float* spatial_with_ghosts);
+/* Fft2D::fft / inv_fft (src/flds/fft_2d.rs:91-172) on a size_y*size_x
+ * interleaved complex array, in place; inverse includes the 1/(nx*ny) scale.
+ * Power-of-two sizes only. */
+SPX_API int spx_fft2d(uint64_t size_x, uint64_t size_y, int32_t inverse, float* data_complex);
+
+/* Time of the last spx_step call's kernels on the context stream, in ms,
+ * split as [0] push+move+deposit, [1] fold+filter, [2] spectral solve,
+ * [3] whole step (CUDA events; filled only when timing is enabled). */
+SPX_API int spx_set_timing(spx_ctx* ctx, int32_t enable);
+SPX_API int spx_get_timing(spx_ctx* ctx, float* out4);
+/* Number of kernel launches issued by the last spx_step call. */
+SPX_API uint64_t spx_last_launch_count(const spx_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPECTRAL_GPU_H */

@@ -1,0 +1,874 @@
+// C ABI of the B200 hot path (include/spectral_gpu.h): context, species
+// management, the per-phase entry points and the graph-captured step.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "fields.cuh"
+#include "particles.cuh"
+
+using namespace spx;
+
+struct spx_ctx {
+  spx_params prm{};
+  Grid g{};
+  FieldBuffers fb;
+  ParticleGeom pg;
+  PhysParams pp{};
+  std::vector<Species> species;
+  cudaStream_t st = nullptr;
+  int* d_err = nullptr;
+  double* d_diag = nullptr;
+  uint32_t* d_u32 = nullptr;  // scratch scalars
+  uint32_t* d_counts = nullptr;
+  bool pending_push = false;
+  bool plain = false;
+  std::string err;
+  // graphs of one fused step, keyed by the species' buffer parities
+  std::map<uint32_t, cudaGraphExec_t> graphs;
+  bool use_graphs = true;
+  // timing ring
+  bool timing = false;
+  std::vector<cudaEvent_t> ev;  // 4 per step
+  int ev_steps = 0;
+  float last_timing[4] = {0, 0, 0, 0};
+  uint64_t last_launches = 0;
+};
+
+static std::string g_create_err;
+
+static int fail(spx_ctx* c, int code, const std::string& m) {
+  if (c) c->err = m;
+  else g_create_err = m;
+  return code;
+}
+
+#define SPX_GUARD(ctx, ...)                           \
+  try {                                               \
+    __VA_ARGS__;                                      \
+  } catch (const spx::Error& e) {                     \
+    return fail(ctx, e.code, e.msg);                  \
+  } catch (const std::exception& e) {                 \
+    return fail(ctx, SPX_ERR_CUDA, e.what());         \
+  }
+
+static int check_device_error(spx_ctx* c) {
+  int h = 0;
+  SPX_CUDA_TRY(cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+  if (!h) return SPX_OK;
+  SPX_CUDA_TRY(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st));
+  if (h & DERR_WALL) return fail(c, SPX_ERR_WALL, "reflecting wall assertion: a particle is beyond wall_loc+1 or at ix <= delta");
+  if (h & DERR_BOUNDS) return fail(c, SPX_ERR_BOUNDS, "particle cell index out of the grid");
+  if (h & DERR_OVERFLOW_LOST) return fail(c, SPX_ERR_STATE, "particle overflow list full: slot capacity too small");
+  return fail(c, SPX_ERR_STATE, "device error word " + std::to_string(h));
+}
+
+static void invalidate_graphs(spx_ctx* c) {
+  for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+  c->graphs.clear();
+}
+
+static FieldPtrs field_ptrs(spx_ctx* c) {
+  FieldPtrs f;
+  for (int i = 0; i < 3; ++i) {
+    f.E[i] = c->fb.spatial[SPX_EX + i];
+    f.B[i] = c->fb.spatial[SPX_BX + i];
+    f.J[i] = c->fb.spatial[SPX_JX + i];
+  }
+  f.dsty = c->fb.spatial[SPX_DSTY];
+  f.dens = c->fb.spatial[SPX_DENS];
+  return f;
+}
+
+// ---------------------------------------------------------------- create / destroy
+extern "C" int spx_create(const spx_params* p, spx_ctx** out) {
+  if (!p || !out) return fail(nullptr, SPX_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (p->size_x % 2 || p->size_y % 2) return fail(nullptr, SPX_ERR_ARG, "Number of cells must be even (src/lib.rs:76)");
+  if (!is_pow2(p->size_x) || !is_pow2(p->size_y) || p->size_x < 8 || p->size_y < 8 || p->size_x > 32768 ||
+      p->size_y > 32768)
+    return fail(nullptr, SPX_ERR_ARG, "GPU FFT needs power-of-two sizes in [8, 32768]");
+  if (!p->periodic_x && p->delta * 2 >= p->size_x)
+    return fail(nullptr, SPX_ERR_ARG, "Delta must be less than 1/2 the size of size_x (src/lib.rs:88)");
+  if (p->dens == 0 || !(p->c > 0) || !(p->dt > 0)) return fail(nullptr, SPX_ERR_ARG, "dens, c and dt must be positive");
+  spx_ctx* c = new spx_ctx();
+  c->prm = *p;
+  try {
+    SPX_CUDA_TRY(cudaSetDevice(p->device));
+    SPX_CUDA_TRY(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    c->g.nx = (int)p->size_x;
+    c->g.ny = (int)p->size_y;
+    c->g.W = c->g.nx + 2;
+    c->g.log2nx = ilog2(p->size_x);
+    c->g.log2ny = ilog2(p->size_y);
+    c->fb.dt = p->dt;
+    c->fb.c = p->c;
+    c->fb.dens = p->dens;
+    c->fb.n_pass = p->n_pass;
+    c->fb.allocate(c->g);
+    // tiles: power-of-two, at least 2 waves of CTAs when the grid allows
+    int tx = p->tile_x > 0 ? p->tile_x : 16, ty = p->tile_y > 0 ? p->tile_y : 16;
+    if (p->tile_x <= 0 && p->tile_y <= 0) {
+      while ((uint64_t)(c->g.nx / tx) * (c->g.ny / ty) < 2 * 148 && tx * ty > 64) {
+        if (ty >= tx && ty > 4) ty /= 2;
+        else if (tx > 4) tx /= 2;
+        else break;
+      }
+    }
+    tx = std::min(tx, c->g.nx);
+    ty = std::min(ty, c->g.ny);
+    if (!is_pow2(tx) || !is_pow2(ty) || tx * ty > 256 || tx * ty < 32) {
+      delete c;
+      return fail(nullptr, SPX_ERR_ARG, "tile_x*tile_y must be a power-of-two product in [32, 256]");
+    }
+    c->pg.g = c->g;
+    c->pg.TX = tx;
+    c->pg.TY = ty;
+    c->pg.logTX = ilog2(tx);
+    c->pg.logTY = ilog2(ty);
+    c->pg.NTX = c->g.nx / tx;
+    c->pg.NTY = c->g.ny / ty;
+    c->pp.dt = p->dt;
+    c->pp.c = p->c;
+    c->pp.csqinv = 1.0f / (p->c * p->c);  // src/prtls.rs:265
+    c->pp.periodic_x = p->periodic_x;
+    c->pp.left_wall = p->left_wall;
+    c->pp.wall_loc = (int)(p->size_x + 1 - p->delta);  // src/prtls.rs:153
+    c->pp.delta = (int)p->delta;
+    c->plain = p->path == SPX_PATH_PLAIN;
+    SPX_CUDA_TRY(cudaMalloc(&c->d_err, sizeof(int)));
+    SPX_CUDA_TRY(cudaMemset(c->d_err, 0, sizeof(int)));
+    SPX_CUDA_TRY(cudaMalloc(&c->d_diag, 8 * sizeof(double)));
+    SPX_CUDA_TRY(cudaMalloc(&c->d_u32, 8 * sizeof(uint32_t)));
+    SPX_CUDA_TRY(cudaMalloc(&c->d_counts, c->pg.ncells() * sizeof(uint32_t)));
+  } catch (const spx::Error& e) {
+    spx_destroy(c);
+    return fail(nullptr, e.code, e.msg);
+  }
+  *out = c;
+  return SPX_OK;
+}
+
+extern "C" int spx_destroy(spx_ctx* c) {
+  if (!c) return SPX_OK;
+  if (c->st) cudaStreamSynchronize(c->st);
+  invalidate_graphs(c);
+  for (auto& s : c->species) {
+    slot_release(s);
+    for (float* p : {s.plain.x, s.plain.y, s.plain.px, s.plain.py, s.plain.pz})
+      if (p) cudaFree(p);
+  }
+  c->fb.release();
+  for (void* p : {(void*)c->d_err, (void*)c->d_diag, (void*)c->d_u32, (void*)c->d_counts})
+    if (p) cudaFree(p);
+  for (auto e : c->ev) cudaEventDestroy(e);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+  return SPX_OK;
+}
+
+extern "C" const char* spx_last_error(const spx_ctx* c) { return c ? c->err.c_str() : g_create_err.c_str(); }
+
+extern "C" const char* spx_version(void) {
+  return "spectral_rs_b200 hot path: sm_100a, FP32, particle TU -fmad=false, IEEE div/sqrt";
+}
+
+extern "C" int32_t spx_num_species(const spx_ctx* c) { return c ? (int32_t)c->species.size() : 0; }
+extern "C" uint64_t spx_species_count(const spx_ctx* c, int32_t s) {
+  if (!c || s < 0 || s >= (int)c->species.size()) return 0;
+  return c->species[s].n;
+}
+
+// ---------------------------------------------------------------- species upload
+// Device staging of one species in the reference order, then packing.
+struct Staging {
+  uint32_t* cell = nullptr;
+  float *dx = nullptr, *dy = nullptr, *px = nullptr, *py = nullptr, *pz = nullptr;
+  void alloc(uint64_t n) {
+    SPX_CUDA_TRY(cudaMalloc(&cell, std::max<uint64_t>(n, 1) * 4));
+    SPX_CUDA_TRY(cudaMalloc(&dx, std::max<uint64_t>(n, 1) * 4));
+    SPX_CUDA_TRY(cudaMalloc(&dy, std::max<uint64_t>(n, 1) * 4));
+    SPX_CUDA_TRY(cudaMalloc(&px, std::max<uint64_t>(n, 1) * 4));
+    SPX_CUDA_TRY(cudaMalloc(&py, std::max<uint64_t>(n, 1) * 4));
+    SPX_CUDA_TRY(cudaMalloc(&pz, std::max<uint64_t>(n, 1) * 4));
+  }
+  ~Staging() {
+    for (void* p : {(void*)cell, (void*)dx, (void*)dy, (void*)px, (void*)py, (void*)pz})
+      if (p) cudaFree(p);
+  }
+};
+
+__global__ void k_plain_from_cells(uint64_t n, const uint32_t* cell, const float* dx, const float* dy, float* x,
+                                   float* y) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    x[i] = (float)(cell[i] & 0xFFFFu) + dx[i];
+    y[i] = (float)(cell[i] >> 16) + dy[i];
+  }
+}
+
+static int choose_K(spx_ctx* c, uint64_t n) {
+  uint32_t mx = 0;
+  SPX_CUDA_TRY(cudaMemsetAsync(c->d_u32, 0, sizeof(uint32_t), c->st));
+  // max over the counts array
+  Species tmp;
+  tmp.slot.nlow[0] = c->d_counts;
+  tmp.slot.cur = 0;
+  uint32_t* zeros = nullptr;
+  SPX_CUDA_TRY(cudaMallocAsync(&zeros, c->pg.ncells() * sizeof(uint32_t), c->st));
+  SPX_CUDA_TRY(cudaMemsetAsync(zeros, 0, c->pg.ncells() * sizeof(uint32_t), c->st));
+  tmp.slot.ntop[0] = zeros;
+  slot_max_occupancy(tmp, c->pg, c->d_u32, c->st);
+  SPX_CUDA_TRY(cudaMemcpyAsync(&mx, c->d_u32, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
+  SPX_CUDA_TRY(cudaFreeAsync(zeros, c->st));
+  SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+  if (c->prm.slot_capacity < 0) return std::max((int)mx, -c->prm.slot_capacity);  // exact K (tests)
+  const double mean = (double)n / (double)c->pg.ncells();
+  int K = (int)std::ceil(std::max(1.5 * mx, mean + 10.0 * std::sqrt(mean))) + 16;
+  if (c->prm.slot_capacity > 0) K = std::max(K, c->prm.slot_capacity);
+  return K;
+}
+
+static int finish_species(spx_ctx* c, Species& s, Staging& st, uint64_t n, const uint32_t* d_tag) {
+  if (c->plain) {
+    for (float** p : {&s.plain.x, &s.plain.y, &s.plain.px, &s.plain.py, &s.plain.pz})
+      SPX_CUDA_TRY(cudaMalloc(p, std::max<uint64_t>(n, 1) * 4));
+    if (n) k_plain_from_cells<<<148 * 8, 256, 0, c->st>>>(n, st.cell, st.dx, st.dy, s.plain.x, s.plain.y);
+    SPX_CUDA_TRY(cudaMemcpyAsync(s.plain.px, st.px, n * 4, cudaMemcpyDeviceToDevice, c->st));
+    SPX_CUDA_TRY(cudaMemcpyAsync(s.plain.py, st.py, n * 4, cudaMemcpyDeviceToDevice, c->st));
+    SPX_CUDA_TRY(cudaMemcpyAsync(s.plain.pz, st.pz, n * 4, cudaMemcpyDeviceToDevice, c->st));
+  } else {
+    slot_count(c->pg, n, st.cell, c->d_counts, c->st);
+    const int K = choose_K(c, n);
+    slot_allocate(s, c->pg, K, n);
+    slot_scatter(s, c->pg, n, st.cell, st.dx, st.dy, st.px, st.py, st.pz, d_tag, c->d_counts, c->st);
+  }
+  SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+  return SPX_OK;
+}
+
+__global__ void k_check_cells(uint64_t n, const uint32_t* cell, int nx, int ny, int* derr) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const int ix = (int)(cell[i] & 0xFFFFu), iy = (int)(cell[i] >> 16);
+    if (ix < 1 || ix > nx || iy < 1 || iy > ny) atomicOr(derr, DERR_BOUNDS);
+  }
+}
+
+__global__ void k_check_gamma(uint64_t n, const float* px, const float* py, const float* pz, const float* psa,
+                              float csqinv, int* derr) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const float g = __fsqrt_rn(__fadd_rn(1.0f, __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(px[i], px[i]),
+                                                                             __fmul_rn(py[i], py[i])),
+                                                                   __fmul_rn(pz[i], pz[i])),
+                                                         csqinv)));
+    if (g != psa[i]) atomicOr(derr, DERR_GAMMA);
+  }
+}
+
+extern "C" int spx_add_species(spx_ctx* c, float charge, float mass, float vth, uint64_t n, const uint64_t* ix,
+                               const uint64_t* iy, const float* dx, const float* dy, const float* px, const float* py,
+                               const float* pz, const float* psa, int32_t* species_out) {
+  if (!c) return fail(nullptr, SPX_ERR_ARG, "null context");
+  if ((int)c->species.size() >= MAX_SPECIES) return fail(c, SPX_ERR_ARG, "at most 4 species");
+  if (n && (!ix || !iy || !dx || !dy || !px || !py || !pz)) return fail(c, SPX_ERR_ARG, "null particle array");
+  if (n >= (1ull << 32)) return fail(c, SPX_ERR_ARG, "at most 2^32-1 particles per species");
+  if (!(mass != 0.0f)) return fail(c, SPX_ERR_ARG, "mass must be non-zero");
+  SPX_GUARD(c, {
+    if (int e = spx_flush(c)) return e;
+    Species s;
+    s.charge = charge;
+    s.mass = mass;
+    s.vth = vth;
+    // src/prtls.rs:61-62, FP32 left to right
+    s.beta = (charge / mass) * 0.5f * c->prm.dt;
+    s.alpha = (charge / mass) * 0.5f * c->prm.dt / c->prm.c;
+    s.n = n;
+    Staging st;
+    st.alloc(n);
+    std::vector<uint32_t> cells(n);
+    for (uint64_t i = 0; i < n; ++i) {
+      if (ix[i] < 1 || iy[i] < 1 || ix[i] > (uint64_t)c->g.nx || iy[i] > (uint64_t)c->g.ny)
+        return fail(c, SPX_ERR_BOUNDS, "particle " + std::to_string(i) + " outside the grid");
+      cells[i] = (uint32_t)ix[i] | ((uint32_t)iy[i] << 16);
+    }
+    SPX_CUDA_TRY(cudaMemcpyAsync(st.cell, cells.data(), n * 4, cudaMemcpyHostToDevice, c->st));
+    SPX_CUDA_TRY(cudaMemcpyAsync(st.dx, dx, n * 4, cudaMemcpyHostToDevice, c->st));
+    SPX_CUDA_TRY(cudaMemcpyAsync(st.dy, dy, n * 4, cudaMemcpyHostToDevice, c->st));
+    SPX_CUDA_TRY(cudaMemcpyAsync(st.px, px, n * 4, cudaMemcpyHostToDevice, c->st));
+    SPX_CUDA_TRY(cudaMemcpyAsync(st.py, py, n * 4, cudaMemcpyHostToDevice, c->st));
+    SPX_CUDA_TRY(cudaMemcpyAsync(st.pz, pz, n * 4, cudaMemcpyHostToDevice, c->st));
+    if (psa && n) {
+      float* d_psa = nullptr;
+      SPX_CUDA_TRY(cudaMallocAsync(&d_psa, n * 4, c->st));
+      SPX_CUDA_TRY(cudaMemcpyAsync(d_psa, psa, n * 4, cudaMemcpyHostToDevice, c->st));
+      k_check_gamma<<<148 * 8, 256, 0, c->st>>>(n, st.px, st.py, st.pz, d_psa, c->pp.csqinv, c->d_err);
+      SPX_CUDA_TRY(cudaFreeAsync(d_psa, c->st));
+      int h = 0;
+      SPX_CUDA_TRY(cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+      SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+      if (h & DERR_GAMMA) {
+        SPX_CUDA_TRY(cudaMemset(c->d_err, 0, sizeof(int)));
+        return fail(c, SPX_ERR_GAMMA, "psa differs from sqrt(1 + |p|^2/c^2); the GPU derives gamma from p");
+      }
+    }
+    finish_species(c, s, st, n, nullptr);
+    c->species.push_back(s);
+    if (species_out) *species_out = (int32_t)c->species.size() - 1;
+    invalidate_graphs(c);
+  });
+  return SPX_OK;
+}
+
+extern "C" int spx_init_species(spx_ctx* c, float charge, float mass, float vth, uint32_t ppc, uint64_t x0,
+                                uint64_t x1, float gamma_drift, float sign_x, int32_t random_positions,
+                                uint64_t seed, int32_t* species_out) {
+  if (!c) return fail(nullptr, SPX_ERR_ARG, "null context");
+  if ((int)c->species.size() >= MAX_SPECIES) return fail(c, SPX_ERR_ARG, "at most 4 species");
+  if (x1 > (uint64_t)c->g.nx || x0 >= x1 || ppc == 0) return fail(c, SPX_ERR_ARG, "bad column range or ppc");
+  if (!(mass != 0.0f)) return fail(c, SPX_ERR_ARG, "mass must be non-zero");
+  const uint64_t n = (uint64_t)c->g.ny * (x1 - x0) * ppc;
+  if (n >= (1ull << 32)) return fail(c, SPX_ERR_ARG, "at most 2^32-1 particles per species");
+  SPX_GUARD(c, {
+    if (spx_flush(c) != SPX_OK) return SPX_ERR_STATE;
+    Species s;
+    s.charge = charge;
+    s.mass = mass;
+    s.vth = vth;
+    s.beta = (charge / mass) * 0.5f * c->prm.dt;
+    s.alpha = (charge / mass) * 0.5f * c->prm.dt / c->prm.c;
+    s.n = n;
+    Staging st;
+    st.alloc(n);
+    InitSpec is;
+    is.charge = charge;
+    is.mass = mass;
+    is.vth = vth;
+    is.gamma_drift = gamma_drift;
+    is.sign_x = sign_x;
+    is.c = c->prm.c;
+    is.ppc = ppc;
+    is.x0 = (int)x0;
+    is.x1 = (int)x1;
+    is.random_positions = random_positions;
+    is.seed = seed;
+    init_particles(is, c->g, n, st.cell, st.dx, st.dy, st.px, st.py, st.pz, c->st);
+    finish_species(c, s, st, n, nullptr);
+    c->species.push_back(s);
+    if (species_out) *species_out = (int32_t)c->species.size() - 1;
+    invalidate_graphs(c);
+  });
+  return SPX_OK;
+}
+
+// ---------------------------------------------------------------- species download
+__global__ void k_stride_u32(const uint32_t* in, uint64_t n, uint64_t stride, uint64_t* out) {
+  const uint64_t m = (n + stride - 1) / stride;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = in[i * stride];
+}
+__global__ void k_stride_f32(const float* in, uint64_t n, uint64_t stride, float* out) {
+  const uint64_t m = (n + stride - 1) / stride;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = in[i * stride];
+}
+__global__ void k_plain_to_cells(uint64_t n, const float* x, const float* y, uint32_t* ix, uint32_t* iy, float* dx,
+                                 float* dy) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const int cx = (int)floorf(x[i] + 0.5f), cy = (int)floorf(y[i] + 0.5f);
+    ix[i] = (uint32_t)cx;
+    iy[i] = (uint32_t)cy;
+    dx[i] = x[i] - (float)cx;
+    dy[i] = y[i] - (float)cy;
+  }
+}
+__global__ void k_gamma_arr(uint64_t n, const float* px, const float* py, const float* pz, float csqinv, float* g) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    g[i] = sqrtf(1.0f + (px[i] * px[i] + py[i] * py[i] + pz[i] * pz[i]) * csqinv);
+}
+
+extern "C" int spx_get_species(spx_ctx* c, int32_t sidx, uint64_t stride, uint64_t* ix, uint64_t* iy, float* dx,
+                               float* dy, float* px, float* py, float* pz, float* psa) {
+  if (!c) return fail(nullptr, SPX_ERR_ARG, "null context");
+  if (sidx < 0 || sidx >= (int)c->species.size()) return fail(c, SPX_ERR_ARG, "no such species");
+  if (stride == 0) stride = 1;
+  SPX_GUARD(c, {
+    int e = spx_flush(c);
+    if (e) return e;
+    Species& s = c->species[sidx];
+    const uint64_t n = s.n;
+    const uint64_t m = (n + stride - 1) / stride;
+    if (n == 0) return SPX_OK;
+    uint32_t *d_ix, *d_iy;
+    float *d_dx, *d_dy, *d_px, *d_py, *d_pz, *d_g;
+    SPX_CUDA_TRY(cudaMallocAsync(&d_ix, n * 4, c->st));
+    SPX_CUDA_TRY(cudaMallocAsync(&d_iy, n * 4, c->st));
+    SPX_CUDA_TRY(cudaMallocAsync(&d_dx, n * 4, c->st));
+    SPX_CUDA_TRY(cudaMallocAsync(&d_dy, n * 4, c->st));
+    SPX_CUDA_TRY(cudaMallocAsync(&d_px, n * 4, c->st));
+    SPX_CUDA_TRY(cudaMallocAsync(&d_py, n * 4, c->st));
+    SPX_CUDA_TRY(cudaMallocAsync(&d_pz, n * 4, c->st));
+    SPX_CUDA_TRY(cudaMallocAsync(&d_g, n * 4, c->st));
+    if (c->plain) {
+      k_plain_to_cells<<<148 * 8, 256, 0, c->st>>>(n, s.plain.x, s.plain.y, d_ix, d_iy, d_dx, d_dy);
+      SPX_CUDA_TRY(cudaMemcpyAsync(d_px, s.plain.px, n * 4, cudaMemcpyDeviceToDevice, c->st));
+      SPX_CUDA_TRY(cudaMemcpyAsync(d_py, s.plain.py, n * 4, cudaMemcpyDeviceToDevice, c->st));
+      SPX_CUDA_TRY(cudaMemcpyAsync(d_pz, s.plain.pz, n * 4, cudaMemcpyDeviceToDevice, c->st));
+      k_gamma_arr<<<148 * 8, 256, 0, c->st>>>(n, d_px, d_py, d_pz, c->pp.csqinv, d_g);
+    } else {
+      slot_unpack(s, c->pg, d_ix, d_iy, d_dx, d_dy, d_px, d_py, d_pz, d_g, c->pp.csqinv, c->st);
+    }
+    // stride on the device, then copy out
+    uint64_t* d_u64;
+    float* d_f;
+    SPX_CUDA_TRY(cudaMallocAsync(&d_u64, m * 8, c->st));
+    SPX_CUDA_TRY(cudaMallocAsync(&d_f, m * 4, c->st));
+    const int blocks = 148 * 8;
+    if (ix) {
+      k_stride_u32<<<blocks, 256, 0, c->st>>>(d_ix, n, stride, d_u64);
+      SPX_CUDA_TRY(cudaMemcpyAsync(ix, d_u64, m * 8, cudaMemcpyDeviceToHost, c->st));
+      SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+    }
+    if (iy) {
+      k_stride_u32<<<blocks, 256, 0, c->st>>>(d_iy, n, stride, d_u64);
+      SPX_CUDA_TRY(cudaMemcpyAsync(iy, d_u64, m * 8, cudaMemcpyDeviceToHost, c->st));
+      SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+    }
+    const float* srcs[6] = {d_dx, d_dy, d_px, d_py, d_pz, d_g};
+    float* dsts[6] = {dx, dy, px, py, pz, psa};
+    for (int k = 0; k < 6; ++k) {
+      if (!dsts[k]) continue;
+      k_stride_f32<<<blocks, 256, 0, c->st>>>(srcs[k], n, stride, d_f);
+      SPX_CUDA_TRY(cudaMemcpyAsync(dsts[k], d_f, m * 4, cudaMemcpyDeviceToHost, c->st));
+      SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+    }
+    for (void* p : {(void*)d_ix, (void*)d_iy, (void*)d_dx, (void*)d_dy, (void*)d_px, (void*)d_py, (void*)d_pz,
+                    (void*)d_g, (void*)d_u64, (void*)d_f})
+      SPX_CUDA_TRY(cudaFreeAsync(p, c->st));
+    SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+  });
+  return SPX_OK;
+}
+
+// ---------------------------------------------------------------- per-phase calls
+static void zero_sources(spx_ctx* c) {
+  for (int f : {SPX_JX, SPX_JY, SPX_JZ, SPX_DSTY, SPX_DENS})
+    SPX_CUDA_TRY(cudaMemsetAsync(c->fb.spatial[f], 0, c->g.spatial_size() * sizeof(float), c->st));
+}
+
+static int run_move(spx_ctx* c, int s0, int s1, bool push) {
+  FieldPtrs fp = field_ptrs(c);
+  int launches = 0;
+  if (c->plain) {
+    for (int s = s0; s < s1; ++s) {
+      if (push) launches += plain_push(c->species[s], c->species[s].n, c->pg, c->pp, fp, c->d_err, c->st);
+      launches += plain_move_deposit(c->species[s], c->species[s].n, c->pg, c->pp, fp, c->d_err, c->st);
+    }
+    return launches;
+  }
+  return slot_step(c->species.data(), s0, s1, c->pg, c->pp, fp, push, true, c->d_err, c->st);
+}
+
+static int run_push_only(spx_ctx* c, int s0, int s1) {
+  FieldPtrs fp = field_ptrs(c);
+  if (c->plain) {
+    int l = 0;
+    for (int s = s0; s < s1; ++s) l += plain_push(c->species[s], c->species[s].n, c->pg, c->pp, fp, c->d_err, c->st);
+    return l;
+  }
+  return slot_step(c->species.data(), s0, s1, c->pg, c->pp, fp, true, false, c->d_err, c->st);
+}
+
+static int fold_all(spx_ctx* c) {
+  float* f[5] = {c->fb.spatial[SPX_JX], c->fb.spatial[SPX_JY], c->fb.spatial[SPX_JZ], c->fb.spatial[SPX_DSTY],
+                 c->fb.spatial[SPX_DENS]};
+  launch_fold(c->g, f, 5, c->st);
+  return 1;
+}
+
+extern "C" int spx_flush(spx_ctx* c) {
+  if (!c) return SPX_ERR_ARG;
+  if (!c->pending_push) return SPX_OK;
+  SPX_GUARD(c, {
+    c->pending_push = false;
+    run_push_only(c, 0, (int)c->species.size());
+    return check_device_error(c);
+  });
+  return SPX_OK;
+}
+
+extern "C" int spx_synchronize(spx_ctx* c) {
+  if (!c) return SPX_ERR_ARG;
+  SPX_GUARD(c, { SPX_CUDA_TRY(cudaStreamSynchronize(c->st)); });
+  return SPX_OK;
+}
+
+extern "C" int spx_zero_sources(spx_ctx* c) {
+  if (!c) return SPX_ERR_ARG;
+  SPX_GUARD(c, {
+    if (int e = spx_flush(c)) return e;
+    zero_sources(c);
+    SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+  });
+  return SPX_OK;
+}
+
+extern "C" int spx_move_and_deposit(spx_ctx* c, int32_t s) {
+  if (!c) return SPX_ERR_ARG;
+  if (s < 0 || s >= (int)c->species.size()) return fail(c, SPX_ERR_ARG, "no such species");
+  SPX_GUARD(c, {
+    if (int e = spx_flush(c)) return e;
+    run_move(c, s, s + 1, false);
+    invalidate_graphs(c);
+    return check_device_error(c);
+  });
+  return SPX_OK;
+}
+
+extern "C" int spx_boris_push(spx_ctx* c, int32_t s) {
+  if (!c) return SPX_ERR_ARG;
+  if (s < 0 || s >= (int)c->species.size()) return fail(c, SPX_ERR_ARG, "no such species");
+  SPX_GUARD(c, {
+    if (int e = spx_flush(c)) return e;
+    run_push_only(c, s, s + 1);
+    return check_device_error(c);
+  });
+  return SPX_OK;
+}
+
+extern "C" int spx_deposit_ghosts(spx_ctx* c, int32_t field) {
+  if (!c) return SPX_ERR_ARG;
+  if (field < 0 || field >= SPX_NUM_FIELDS) return fail(c, SPX_ERR_ARG, "no such field");
+  SPX_GUARD(c, {
+    float* f = c->fb.spatial[field];
+    launch_fold(c->g, &f, 1, c->st);
+    SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+  });
+  return SPX_OK;
+}
+
+extern "C" int spx_fields_update(spx_ctx* c) {
+  if (!c) return SPX_ERR_ARG;
+  SPX_GUARD(c, {
+    if (int e = spx_flush(c)) return e;
+    field_update(c->fb, c->st);
+    SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+  });
+  return SPX_OK;
+}
+
+extern "C" int spx_prepare(spx_ctx* c) {
+  if (!c) return SPX_ERR_ARG;
+  SPX_GUARD(c, {
+    if (int e = spx_flush(c)) return e;
+    run_move(c, 0, (int)c->species.size(), false);  // src/lib.rs:130-132
+    fold_all(c);                                      // src/lib.rs:134-142
+    invalidate_graphs(c);
+    return check_device_error(c);
+  });
+  return SPX_OK;
+}
+
+__global__ void k_pack_cells(uint64_t n, const uint32_t* ix, const uint32_t* iy, uint32_t* cell) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    cell[i] = ix[i] | (iy[i] << 16);
+}
+void pack_cells(uint64_t n, const uint32_t* ix, const uint32_t* iy, uint32_t* cell, cudaStream_t st) {
+  if (n) k_pack_cells<<<148 * 8, 256, 0, st>>>(n, ix, iy, cell);
+}
+
+// Overflow handling: if a species parked particles in its overflow list or a
+// cell is close to its capacity, rebuild its slots with a larger K.
+static void maybe_repack(spx_ctx* c) {
+  if (c->plain) return;
+  for (auto& s : c->species) {
+    SlotSpecies& S = s.slot;
+    uint32_t h[2] = {0, 0};
+    SPX_CUDA_TRY(cudaMemsetAsync(c->d_u32, 0, sizeof(uint32_t), c->st));
+    slot_max_occupancy(s, c->pg, c->d_u32, c->st);
+    SPX_CUDA_TRY(cudaMemcpyAsync(&h[0], c->d_u32, 4, cudaMemcpyDeviceToHost, c->st));
+    SPX_CUDA_TRY(cudaMemcpyAsync(&h[1], S.ocount + S.cur, 4, cudaMemcpyDeviceToHost, c->st));
+    SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+    if (h[1] == 0 && h[0] + 8 < (uint32_t)S.K) continue;
+    // unpack (reference order) and pack again with a larger capacity
+    const uint64_t n = s.n;
+    Staging st;
+    st.alloc(n);
+    uint32_t *d_ix, *d_iy;
+    SPX_CUDA_TRY(cudaMallocAsync(&d_ix, n * 4, c->st));
+    SPX_CUDA_TRY(cudaMallocAsync(&d_iy, n * 4, c->st));
+    slot_unpack(s, c->pg, d_ix, d_iy, st.dx, st.dy, st.px, st.py, st.pz, nullptr, c->pp.csqinv, c->st);
+    pack_cells(n, d_ix, d_iy, st.cell, c->st);  // cell = ix | iy << 16
+    slot_count(c->pg, n, st.cell, c->d_counts, c->st);
+    int K = choose_K(c, n);
+    K = std::max(K, S.K + std::max(S.K / 2, 4));
+    slot_release(s);
+    slot_allocate(s, c->pg, K, n);
+    slot_scatter(s, c->pg, n, st.cell, st.dx, st.dy, st.px, st.py, st.pz, nullptr, c->d_counts, c->st);
+    SPX_CUDA_TRY(cudaFreeAsync(d_ix, c->st));
+    SPX_CUDA_TRY(cudaFreeAsync(d_iy, c->st));
+    SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+    invalidate_graphs(c);
+  }
+}
+
+
+// One loop iteration of run() in fused form.  Returns launches.
+static int step_body(spx_ctx* c, bool timed, int slot) {
+  int launches = 0;
+  const int ns = (int)c->species.size();
+  cudaEvent_t* e = timed ? &c->ev[4 * slot] : nullptr;
+  if (e) SPX_CUDA_TRY(cudaEventRecord(e[0], c->st));
+  zero_sources(c);
+  launches += 5;
+  if (c->plain) {
+    launches += run_move(c, 0, ns, false);
+  } else if (c->pending_push) {
+    launches += run_move(c, 0, ns, true);  // P(t-1) fused with M(t)
+  } else {
+    launches += run_move(c, 0, ns, false);
+  }
+  if (e) SPX_CUDA_TRY(cudaEventRecord(e[1], c->st));
+  launches += fold_all(c);
+  if (e) SPX_CUDA_TRY(cudaEventRecord(e[2], c->st));
+  launches += field_update(c->fb, c->st);
+  if (c->plain) {
+    launches += run_push_only(c, 0, ns);
+  } else {
+    c->pending_push = true;
+  }
+  if (e) SPX_CUDA_TRY(cudaEventRecord(e[3], c->st));
+  return launches;
+}
+
+static uint32_t parity_key(spx_ctx* c) {
+  uint32_t k = c->pending_push ? 1u : 0u;
+  for (size_t i = 0; i < c->species.size(); ++i) k |= (uint32_t)c->species[i].slot.cur << (i + 1);
+  return k;
+}
+
+extern "C" int spx_step(spx_ctx* c, uint32_t n) {
+  if (!c) return SPX_ERR_ARG;
+  if (c->species.empty()) return fail(c, SPX_ERR_STATE, "no species");
+  SPX_GUARD(c, {
+    uint64_t launches = 0;
+    if (c->timing) {
+      if ((int)c->ev.size() < 4 * (int)n) {
+        for (auto ev : c->ev) cudaEventDestroy(ev);
+        c->ev.assign(4 * n, nullptr);
+        for (auto& ev : c->ev) SPX_CUDA_TRY(cudaEventCreate(&ev));
+      }
+      for (uint32_t i = 0; i < n; ++i) launches += step_body(c, true, (int)i);
+      c->ev_steps = (int)n;
+    } else if (!c->use_graphs) {
+      for (uint32_t i = 0; i < n; ++i) launches += step_body(c, false, 0);
+    } else {
+      for (uint32_t i = 0; i < n; ++i) {
+        // graphs are captured in the steady state (a push pending on the split
+        // path); the first step after prepare runs uncaptured
+        if (!c->plain && !c->pending_push) {
+          launches += step_body(c, false, 0);
+          continue;
+        }
+        const uint32_t key = parity_key(c);
+        auto it = c->graphs.find(key);
+        if (it == c->graphs.end()) {
+          std::vector<int> cur_before(c->species.size());
+          for (size_t s = 0; s < c->species.size(); ++s) cur_before[s] = c->species[s].slot.cur;
+          cudaGraph_t gr;
+          SPX_CUDA_TRY(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+          const int l = step_body(c, false, 0);
+          SPX_CUDA_TRY(cudaStreamEndCapture(c->st, &gr));
+          cudaGraphExec_t ex;
+          SPX_CUDA_TRY(cudaGraphInstantiate(&ex, gr, 0));
+          SPX_CUDA_TRY(cudaGraphDestroy(gr));
+          // capturing recorded the work without running it: undo the host-side
+          // parity flips, then execute
+          for (size_t s = 0; s < c->species.size(); ++s) c->species[s].slot.cur = cur_before[s];
+          it = c->graphs.emplace(key, ex).first;
+          launches += l - 1;
+        }
+        SPX_CUDA_TRY(cudaGraphLaunch(it->second, c->st));
+        if (!c->plain)
+          for (size_t s = 0; s < c->species.size(); ++s) c->species[s].slot.cur ^= 1;
+        launches += 1;
+      }
+    }
+    c->last_launches = launches;
+    if (int e = check_device_error(c)) return e;
+    if (c->timing) {
+      float acc[4] = {0, 0, 0, 0};
+      for (int i = 0; i < c->ev_steps; ++i) {
+        float a, b, d, t;
+        SPX_CUDA_TRY(cudaEventElapsedTime(&a, c->ev[4 * i], c->ev[4 * i + 1]));
+        SPX_CUDA_TRY(cudaEventElapsedTime(&b, c->ev[4 * i + 1], c->ev[4 * i + 2]));
+        SPX_CUDA_TRY(cudaEventElapsedTime(&d, c->ev[4 * i + 2], c->ev[4 * i + 3]));
+        SPX_CUDA_TRY(cudaEventElapsedTime(&t, c->ev[4 * i], c->ev[4 * i + 3]));
+        acc[0] += a;
+        acc[1] += b;
+        acc[2] += d;
+        acc[3] += t;
+      }
+      for (int k = 0; k < 4; ++k) c->last_timing[k] = acc[k];
+    }
+    maybe_repack(c);
+  });
+  return SPX_OK;
+}
+
+extern "C" int spx_set_timing(spx_ctx* c, int32_t enable) {
+  if (!c) return SPX_ERR_ARG;
+  c->timing = enable != 0;
+  return SPX_OK;
+}
+extern "C" int spx_get_timing(spx_ctx* c, float* out4) {
+  if (!c || !out4) return SPX_ERR_ARG;
+  for (int k = 0; k < 4; ++k) out4[k] = c->last_timing[k];
+  return SPX_OK;
+}
+extern "C" uint64_t spx_last_launch_count(const spx_ctx* c) { return c ? c->last_launches : 0; }
+
+// ---------------------------------------------------------------- field access
+extern "C" int spx_get_field(spx_ctx* c, int32_t field, int32_t with_ghosts, float* out) {
+  if (!c || !out) return SPX_ERR_ARG;
+  if (field < 0 || field >= SPX_NUM_FIELDS) return fail(c, SPX_ERR_ARG, "no such field");
+  SPX_GUARD(c, {
+    const float* src = c->fb.spatial[field];
+    if (with_ghosts) {
+      SPX_CUDA_TRY(cudaMemcpyAsync(out, src, c->g.spatial_size() * 4, cudaMemcpyDeviceToHost, c->st));
+    } else {
+      // interior rows (save_fld_spatial, src/save/mod.rs:14-17)
+      SPX_CUDA_TRY(cudaMemcpy2DAsync(out, c->g.nx * 4, src + c->g.W + 1, c->g.W * 4, c->g.nx * 4, c->g.ny,
+                                     cudaMemcpyDeviceToHost, c->st));
+    }
+    SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+  });
+  return SPX_OK;
+}
+
+extern "C" int spx_set_field(spx_ctx* c, int32_t field, const float* in) {
+  if (!c || !in) return SPX_ERR_ARG;
+  if (field < 0 || field >= SPX_NUM_FIELDS) return fail(c, SPX_ERR_ARG, "no such field");
+  SPX_GUARD(c, {
+    if (int e = spx_flush(c)) return e;
+    SPX_CUDA_TRY(cudaMemcpyAsync(c->fb.spatial[field], in, c->g.spatial_size() * 4, cudaMemcpyHostToDevice, c->st));
+    SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+  });
+  return SPX_OK;
+}
+
+extern "C" int spx_get_bwrk(spx_ctx* c, int32_t comp, float* out) {
+  if (!c || !out || comp < 0 || comp > 2) return SPX_ERR_ARG;
+  SPX_GUARD(c, {
+    SPX_CUDA_TRY(cudaMemcpyAsync(out, c->fb.spec[SP_BWX + comp], c->g.spectral_size() * 8, cudaMemcpyDeviceToHost,
+                                 c->st));
+    SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+  });
+  return SPX_OK;
+}
+
+extern "C" int spx_set_bwrk(spx_ctx* c, int32_t comp, const float* in) {
+  if (!c || !in || comp < 0 || comp > 2) return SPX_ERR_ARG;
+  SPX_GUARD(c, {
+    if (int e = spx_flush(c)) return e;
+    SPX_CUDA_TRY(cudaMemcpyAsync(c->fb.spec[SP_BWX + comp], in, c->g.spectral_size() * 8, cudaMemcpyHostToDevice,
+                                 c->st));
+    SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+  });
+  return SPX_OK;
+}
+
+// ---------------------------------------------------------------- diagnostics
+__global__ void k_field_energy(const float* a, const float* b, const float* cc, Grid g, double* out) {
+  double e = 0;
+  const size_t n = (size_t)g.nx * g.ny;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = i / g.nx + 1, col = i % g.nx + 1;
+    const size_t o = r * g.W + col;
+    const double x = a[o], y = b[o], z = cc ? cc[o] : 0.0;
+    e += cc ? 0.5 * (x * x + y * y + z * z) : x;
+  }
+  for (int o = 16; o; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, e);
+}
+
+extern "C" int spx_diag(spx_ctx* c, double* out5) {
+  if (!c || !out5) return SPX_ERR_ARG;
+  SPX_GUARD(c, {
+    if (int e = spx_flush(c)) return e;
+    SPX_CUDA_TRY(cudaMemsetAsync(c->d_diag, 0, 8 * sizeof(double), c->st));
+    k_field_energy<<<148 * 4, 256, 0, c->st>>>(c->fb.spatial[SPX_EX], c->fb.spatial[SPX_EY], c->fb.spatial[SPX_EZ],
+                                                c->g, c->d_diag + 0);
+    k_field_energy<<<148 * 4, 256, 0, c->st>>>(c->fb.spatial[SPX_BX], c->fb.spatial[SPX_BY], c->fb.spatial[SPX_BZ],
+                                                c->g, c->d_diag + 1);
+    for (auto& s : c->species) kinetic_energy(s, c->pg, c->plain, c->prm.c, c->d_diag + 2, c->st);
+    // net charge: interior sum of dsty (the third pointer null -> plain sum)
+    k_field_energy<<<148 * 4, 256, 0, c->st>>>(c->fb.spatial[SPX_DSTY], nullptr, nullptr, c->g, c->d_diag + 4);
+    double h[8];
+    SPX_CUDA_TRY(cudaMemcpyAsync(h, c->d_diag, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+    out5[0] = h[0];
+    out5[1] = h[1];
+    out5[2] = h[2];
+    out5[3] = h[4];
+    out5[4] = h[3];
+  });
+  return SPX_OK;
+}
+
+// ---------------------------------------------------------------- standalone ops
+extern "C" int spx_field_op(uint64_t nx, uint64_t ny, int32_t op, uint32_t n_pass, float* spatial) {
+  if (!spatial || nx < 2 || ny < 2 || op < 0 || op > 2) return fail(nullptr, SPX_ERR_ARG, "bad field op arguments");
+  try {
+    Grid g{(int)nx, (int)ny, (int)nx + 2, 0, 0};
+    const size_t bytes = g.spatial_size() * 4;
+    float *a = nullptr, *b = nullptr;
+    SPX_CUDA_TRY(cudaMalloc(&a, bytes));
+    SPX_CUDA_TRY(cudaMalloc(&b, bytes));
+    SPX_CUDA_TRY(cudaMemcpy(a, spatial, bytes, cudaMemcpyHostToDevice));
+    if (op == 0) launch_fold(g, &a, 1, 0);
+    else if (op == 1) launch_update_ghosts(g, &a, 1, 0);
+    else {
+      for (uint32_t p = 0; p < n_pass; ++p) {
+        launch_filter_pass(g, &a, &b, 1, 0);
+        std::swap(a, b);
+      }
+    }
+    SPX_CUDA_TRY(cudaGetLastError());
+    SPX_CUDA_TRY(cudaMemcpy(spatial, a, bytes, cudaMemcpyDeviceToHost));
+    cudaFree(a);
+    cudaFree(b);
+  } catch (const spx::Error& e) {
+    return fail(nullptr, e.code, e.msg);
+  }
+  return SPX_OK;
+}
+
+extern "C" int spx_fft2d(uint64_t nx, uint64_t ny, int32_t inverse, float* data) {
+  if (!data || !is_pow2(nx) || !is_pow2(ny) || nx < 8 || ny < 8 || nx > 32768 || ny > 32768)
+    return fail(nullptr, SPX_ERR_ARG, "GPU FFT needs power-of-two sizes in [8, 32768]");
+  try {
+    Grid g{(int)nx, (int)ny, (int)nx + 2, ilog2(nx), ilog2(ny)};
+    const size_t bytes = nx * ny * 8;
+    float2* d = nullptr;
+    float2 *tx = nullptr, *ty = nullptr;
+    SPX_CUDA_TRY(cudaMalloc(&d, bytes));
+    SPX_CUDA_TRY(cudaMalloc(&tx, nx * 8));
+    SPX_CUDA_TRY(cudaMalloc(&ty, ny * 8));
+    std::vector<float2> t(std::max(nx, ny));
+    make_twiddles((int)nx, t.data());
+    SPX_CUDA_TRY(cudaMemcpy(tx, t.data(), nx * 8, cudaMemcpyHostToDevice));
+    make_twiddles((int)ny, t.data());
+    SPX_CUDA_TRY(cudaMemcpy(ty, t.data(), ny * 8, cudaMemcpyHostToDevice));
+    SPX_CUDA_TRY(cudaMemcpy(d, data, bytes, cudaMemcpyHostToDevice));
+    fft2d_inplace(g, d, tx, ty, inverse != 0, 0);
+    SPX_CUDA_TRY(cudaMemcpy(data, d, bytes, cudaMemcpyDeviceToHost));
+    cudaFree(d);
+    cudaFree(tx);
+    cudaFree(ty);
+  } catch (const spx::Error& e) {
+    return fail(nullptr, e.code, e.msg);
+  }
+  return SPX_OK;
+}

@@ -1,0 +1,591 @@
+// Pseudo-spectral Maxwell solver on the B200 (replaces src/flds/*.rs of the reference).
+//
+// Data layout in HBM
+//   spatial fields: reference layout, (ny+2) x (nx+2) floats with a one-cell ghost frame
+//   spectral fields: ny x nx float2, row-major (ky rows, kx columns), numpy fft2 convention
+//
+// Kernels per Flds::update (src/flds/mod.rs:87-309):
+//   k_filter      x n_pass : 3x3 binomial stencil of jx, jy, jz, dsty, ghost frame refilled
+//   k_rows<fwd>            : copy_to_spectral (+ dsty * 1/dens) fused with the row FFTs of 7 fields
+//   k_cols<fwd>            : column FFTs of the 7 fields, strip of W columns per CTA
+//   k_kspace               : Ampere, divergence correction, Faraday, Nyquist, B average
+//   k_cols<inv>            : column inverse FFTs of B(t) and E
+//   k_rows<inv>            : row inverse FFTs, 1/(nx ny) scale, copy_to_spatial + update_ghosts fused
+//
+// The FFT is a shared-memory Stockham autosort transform (radix 8 passes, one
+// radix 4 or 2 pass for the remaining factor), one radix-8 butterfly per
+// thread per pass, twiddles from an FP64-generated table.  Inverse transforms
+// use ifft(x) = conj(fft(conj(x))), conjugating on load and store.
+#include <cmath>
+#include <vector>
+
+#include "fields.cuh"
+
+namespace spx {
+
+bool is_pow2(uint64_t v) { return v && !(v & (v - 1)); }
+int ilog2(uint64_t v) {
+  int l = 0;
+  while ((1ull << l) < v) ++l;
+  return l;
+}
+
+void make_twiddles(int n, float2* out) {
+  // exp(-2 pi i m / n) evaluated in long double, using the octant symmetries so
+  // that every entry is the correctly rounded value of an exact-angle sin/cos.
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  for (int m = 0; m < n; ++m) {
+    long double a = two_pi * (long double)m / (long double)n;
+    long double c = cosl(a), s = sinl(a);
+    if (4 * m == n) { c = 0; s = 1; }
+    if (2 * m == n) { c = -1; s = 0; }
+    if (4 * m == 3 * n) { c = 0; s = -1; }
+    if (m == 0) { c = 1; s = 0; }
+    out[m] = make_float2((float)(double)c, (float)(double)(-s));
+  }
+}
+
+// ---------------------------------------------------------------- complex
+__device__ __forceinline__ float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 c_mul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 c_conj(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ float2 c_scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+
+// ---------------------------------------------------------------- radix kernels (forward)
+__device__ __forceinline__ void dft2(float2& a, float2& b) {
+  float2 t = a;
+  a = c_add(t, b);
+  b = c_sub(t, b);
+}
+__device__ __forceinline__ void dft4(float2& v0, float2& v1, float2& v2, float2& v3) {
+  float2 t0 = c_add(v0, v2), t1 = c_sub(v0, v2), t2 = c_add(v1, v3), t3 = c_sub(v1, v3);
+  t3 = make_float2(t3.y, -t3.x);  // -i * (v1 - v3)
+  v0 = c_add(t0, t2);
+  v2 = c_sub(t0, t2);
+  v1 = c_add(t1, t3);
+  v3 = c_sub(t1, t3);
+}
+__device__ __forceinline__ void dft8(float2 (&v)[8]) {
+  float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+  dft4(e0, e1, e2, e3);
+  dft4(o0, o1, o2, o3);
+  const float r = 0.70710678118654752440f;  // 1/sqrt(2): W8 = (1 - i)/sqrt(2)
+  float2 w1 = make_float2((o1.x + o1.y) * r, (o1.y - o1.x) * r);
+  float2 w2 = make_float2(o2.y, -o2.x);
+  float2 w3 = make_float2((o3.y - o3.x) * r, -(o3.x + o3.y) * r);
+  v[0] = c_add(e0, o0);
+  v[4] = c_sub(e0, o0);
+  v[1] = c_add(e1, w1);
+  v[5] = c_sub(e1, w1);
+  v[2] = c_add(e2, w2);
+  v[6] = c_sub(e2, w2);
+  v[3] = c_add(e3, w3);
+  v[7] = c_sub(e3, w3);
+}
+
+// One in-place Stockham pass of radix R over B transforms of length N = 2^logN
+// stored in shared memory at s[e*ES + t*TS].  blockDim.x == N*B/8; each thread
+// does 8/R butterflies.  Ns = product of the radices of the previous passes.
+template <int R>
+__device__ __forceinline__ void fft_pass(float2* s, int logN, int logB, int ES, int TS, bool t_fast, int Ns,
+                                         const float2* __restrict__ tw) {
+  constexpr int PER = 8 / R;
+  constexpr int LR = R == 8 ? 3 : R == 4 ? 2 : 1;
+  const int nthr = blockDim.x, tid = threadIdx.x;
+  const int logNb = logN - LR;
+  const int nb = 1 << logNb;
+  const int N = 1 << logN;
+  float2 v[8];
+  int out_base[PER];
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int b = tid + q * nthr;
+    int t, j;
+    if (t_fast) {
+      t = b & ((1 << logB) - 1);
+      j = b >> logB;
+    } else {
+      t = b >> logNb;
+      j = b & (nb - 1);
+    }
+    const int k = j & (Ns - 1);
+    const float2* src = s + t * TS;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[q * R + r] = src[(j + r * nb) * ES];
+    if (Ns > 1) {
+      const int step = N / (Ns * R);
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[q * R + r] = c_mul(v[q * R + r], __ldg(&tw[r * k * step]));
+    }
+    if constexpr (R == 8) {
+      dft8(v);
+    } else if constexpr (R == 4) {
+      dft4(v[q * 4 + 0], v[q * 4 + 1], v[q * 4 + 2], v[q * 4 + 3]);
+    } else {
+      dft2(v[q * 2 + 0], v[q * 2 + 1]);
+    }
+    out_base[q] = t * TS + (((j - k) * R) + k) * ES;  // idxD = (j/Ns)*Ns*R + k
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < PER; ++q)
+#pragma unroll
+    for (int r = 0; r < R; ++r) s[out_base[q] + r * Ns * ES] = v[q * R + r];
+  __syncthreads();
+}
+
+// Forward FFT of B = 2^logB transforms of length 2^logN in shared memory.
+__device__ void block_fft(float2* s, int logN, int logB, int ES, int TS, bool t_fast, const float2* tw) {
+  int Ns = 1, rem = logN;
+  while (rem >= 3) {
+    fft_pass<8>(s, logN, logB, ES, TS, t_fast, Ns, tw);
+    Ns <<= 3;
+    rem -= 3;
+  }
+  if (rem == 2)
+    fft_pass<4>(s, logN, logB, ES, TS, t_fast, Ns, tw);
+  else if (rem == 1)
+    fft_pass<2>(s, logN, logB, ES, TS, t_fast, Ns, tw);
+}
+
+// ---------------------------------------------------------------- launch geometry
+// Row pass: B rows per CTA with blockDim = N*B/8 threads.
+__host__ __device__ inline int row_logB(int logN) {
+  int lb = 11 - logN;  // N*B = 2048 -> 256 threads for small rows
+  return lb < 0 ? 0 : lb;
+}
+// Column pass: strip of W = 2^logW columns, blockDim = Ny*W/8 threads (<= 1024).
+__host__ __device__ inline int col_logW(int logNy, int logNx) {
+  int lw = logNy >= 7 ? 13 - logNy : 11 - logNy;  // <= 1024 threads, >= 256 for short columns
+  if (lw > 4 && logNy >= 7) lw = 4;               // 16 columns = 128 B row segments
+  if (lw < 0) lw = 0;
+  if (lw > logNx) lw = logNx;
+  return lw;
+}
+
+// ---------------------------------------------------------------- row kernels
+// IN: 0 = real ghosted spatial field (copy_to_spectral fused), 1 = complex
+// OUT: 0 = complex, 1 = real ghosted spatial field (copy_to_spatial + update_ghosts fused)
+struct RowArgs {
+  const void* src[8];
+  void* dst[8];
+  float scale[8];
+};
+
+template <int IN, int OUT, bool INV>
+__global__ void __launch_bounds__(1024) k_rows(RowArgs a, Grid g, const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  const int f = blockIdx.y;
+  const int logN = g.log2nx, N = g.nx;
+  const int logB = row_logB(logN);
+  const int row0 = blockIdx.x << logB;
+  const float sc = a.scale[f];
+  for (int i = threadIdx.x; i < (N << logB); i += blockDim.x) {
+    const int t = i >> logN, e = i & (N - 1);
+    const int row = row0 + t;
+    float2 v = make_float2(0.f, 0.f);
+    if (row < g.ny) {
+      if (IN == 0) {
+        const float* src = (const float*)a.src[f];
+        v = make_float2(src[(size_t)(row + 1) * g.W + e + 1] * sc, 0.f * sc);
+      } else {
+        const float2* src = (const float2*)a.src[f];
+        v = src[(size_t)row * N + e];
+      }
+    }
+    sm[(t << logN) + e] = INV ? c_conj(v) : v;
+  }
+  __syncthreads();
+  block_fft(sm, logN, logB, 1, N, false, tw);
+  for (int i = threadIdx.x; i < (N << logB); i += blockDim.x) {
+    const int t = i >> logN, e = i & (N - 1);
+    const int row = row0 + t;
+    if (row >= g.ny) continue;
+    float2 v = sm[(t << logN) + e];
+    if (INV) v = c_conj(v);
+    if (OUT == 0) {
+      float2* dst = (float2*)a.dst[f];
+      dst[(size_t)row * N + e] = INV ? c_scale(v, sc) : v;
+    } else {
+      // spatial = Re(ifft) * (1/(nx ny)); the CTA that owns row r also fills the
+      // ghost columns of row r+1 and, for r == ny-1 / r == 0, the ghost rows.
+      float* dst = (float*)a.dst[f];
+      const float re = v.x * sc;
+      const int W = g.W;
+      const int R = row + 1;  // ghosted row
+      dst[(size_t)R * W + e + 1] = re;
+      if (e == N - 1) dst[(size_t)R * W + 0] = re;        // left ghost <- last column
+      if (e == 0) dst[(size_t)R * W + N + 1] = re;        // right ghost <- first column
+      if (R == g.ny) {                                    // top ghost row <- last row
+        dst[e + 1] = re;
+        if (e == N - 1) dst[0] = re;                      // top-left <- bottom-right
+        if (e == 0) dst[N + 1] = re;                      // top-right <- bottom-left
+      }
+      if (R == 1) {                                       // bottom ghost row <- first row
+        dst[(size_t)(g.ny + 1) * W + e + 1] = re;
+        if (e == N - 1) dst[(size_t)(g.ny + 1) * W + 0] = re;      // bottom-left <- top-right
+        if (e == 0) dst[(size_t)(g.ny + 1) * W + N + 1] = re;      // bottom-right <- top-left
+      }
+    }
+  }
+}
+
+// Column FFTs, in place on complex arrays: CTA = strip of W columns of one field.
+struct ColArgs {
+  float2* data[8];
+};
+template <bool INV>
+__global__ void __launch_bounds__(1024) k_cols(ColArgs a, Grid g, const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  const int f = blockIdx.y;
+  const int logN = g.log2ny, N = g.ny;
+  const int logW = col_logW(g.log2ny, g.log2nx);
+  const int W = 1 << logW;
+  const int x0 = blockIdx.x << logW;
+  float2* d = a.data[f];
+  for (int i = threadIdx.x; i < (N << logW); i += blockDim.x) {
+    const int y = i >> logW, w = i & (W - 1);
+    float2 v = d[(size_t)y * g.nx + x0 + w];
+    sm[i] = INV ? c_conj(v) : v;  // sm[y*W + w]
+  }
+  __syncthreads();
+  block_fft(sm, logN, logW, W, 1, true, tw);
+  for (int i = threadIdx.x; i < (N << logW); i += blockDim.x) {
+    const int y = i >> logW, w = i & (W - 1);
+    float2 v = sm[i];
+    d[(size_t)y * g.nx + x0 + w] = INV ? c_conj(v) : v;
+  }
+}
+
+// ---------------------------------------------------------------- k-space update
+// src/flds/mod.rs:105-278 for one k point; num_complex operation order.
+struct KArgs {
+  float2 *jx, *jy, *jz, *rho, *ex, *ey, *ez, *bwx, *bwy, *bwz, *bax, *bay, *baz;
+  float cdt, ckc;
+};
+__global__ void k_kspace(KArgs a, Grid g) {
+  const size_t n = (size_t)g.nx * g.ny;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(idx >> g.log2nx), j = (int)(idx & (g.nx - 1));
+    const float kx = wave_kx(j, g.nx), ky = wave_kx(i, g.ny);
+    float2 Jx = a.jx[idx], Jy = a.jy[idx], Jz = a.jz[idx], Rho = a.rho[idx];
+    if (idx == 0) {  // mod.rs:106-107 (j_z[0] is not zeroed)
+      Jx = make_float2(0.f, 0.f);
+      Jy = make_float2(0.f, 0.f);
+    }
+    const float2 Bx = a.bwx[idx], By = a.bwy[idx], Bz = a.bwz[idx];  // b_*.spectral <- b_*_wrk (t-1/2)
+    float2 Ex = a.ex[idx], Ey = a.ey[idx], Ez = a.ez[idx];
+    const float cdt = a.cdt, ckc = a.ckc;
+    // Ampere (mod.rs:130-173)
+    Ex = c_add(Ex, c_sub(c_mul(make_float2(0.0f * ky, cdt * ky), Bz), make_float2(ckc * Jx.x, ckc * Jx.y)));
+    Ey = c_add(Ey, c_sub(c_mul(make_float2(0.0f * kx, -cdt * kx), Bz), make_float2(ckc * Jy.x, ckc * Jy.y)));
+    {
+      float2 kb = c_sub(make_float2(kx * By.x, kx * By.y), make_float2(ky * Bx.x, ky * Bx.y));
+      Ez = c_add(Ez, c_mul(make_float2(0.0f, cdt), kb));
+      Ez = c_sub(Ez, make_float2(ckc * Jz.x, ckc * Jz.y));
+    }
+    // divergence correction with k_norm = 1/k^2, k = 0 kept (mod.rs:177-207)
+    if (idx != 0) {
+      const float kn = 1.0f / (kx * kx + ky * ky);
+      float2 t = c_add(c_add(make_float2(kx * Ex.x, kx * Ex.y), make_float2(ky * Ey.x, ky * Ey.y)),
+                       c_mul(make_float2(0.f, 1.f), Rho));
+      t = c_scale(t, kn);
+      Ex = c_sub(Ex, c_scale(t, kx));
+      Ey = c_sub(Ey, c_scale(t, ky));
+    }
+    // Faraday to t+1/2 (mod.rs:211-225)
+    float2 nBx = c_sub(Bx, c_mul(make_float2(0.0f * ky, cdt * ky), Ez));
+    float2 nBy = c_add(By, c_mul(make_float2(0.0f * kx, cdt * kx), Ez));
+    float2 nBz = c_add(Bz, c_mul(make_float2(0.0f, cdt),
+                                 c_sub(make_float2(ky * Ex.x, ky * Ex.y), make_float2(kx * Ey.x, kx * Ey.y))));
+    // Nyquist column kx = nx/2 and row ky = ny/2 (mod.rs:230-266)
+    if (j == g.nx / 2 || i == g.ny / 2) {
+      const float2 z = make_float2(0.f, 0.f);
+      nBx = nBy = nBz = z;
+      Ex = Ey = Ez = z;
+    }
+    a.ex[idx] = Ex;
+    a.ey[idx] = Ey;
+    a.ez[idx] = Ez;
+    a.bwx[idx] = nBx;
+    a.bwy[idx] = nBy;
+    a.bwz[idx] = nBz;
+    // B at integer time (mod.rs:270-278)
+    a.bax[idx] = c_scale(c_add(Bx, nBx), 0.5f);
+    a.bay[idx] = c_scale(c_add(By, nBy), 0.5f);
+    a.baz[idx] = c_scale(c_add(Bz, nBz), 0.5f);
+  }
+}
+
+// ---------------------------------------------------------------- ghost frame kernels
+struct FieldList {
+  float* f[SPX_NUM_FIELDS];
+};
+struct ConstFieldList {
+  const float* f[SPX_NUM_FIELDS];
+};
+
+// Field::deposit_ghosts, one thread per interior cell of the frame; additions in
+// the reference's order (rows, columns, corners), so results are bit-exact.
+__global__ void k_fold(FieldList L, Grid g) {
+  float* F = L.f[blockIdx.y];
+  const int nx = g.nx, ny = g.ny, W = g.W;
+  const int nper = 2 * nx + 2 * (ny - 2);
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nper; p += gridDim.x * blockDim.x) {
+    int r, c;
+    if (p < nx) { r = 1; c = p + 1; }
+    else if (p < 2 * nx) { r = ny; c = p - nx + 1; }
+    else if (p < 2 * nx + ny - 2) { r = p - 2 * nx + 2; c = 1; }
+    else { r = p - 2 * nx - (ny - 2) + 2; c = nx; }
+    float v = F[r * W + c];
+    if (r == ny) v = __fadd_rn(v, F[0 * W + c]);
+    if (r == 1) v = __fadd_rn(v, F[(ny + 1) * W + c]);
+    if (c == nx) v = __fadd_rn(v, F[r * W + 0]);
+    if (c == 1) v = __fadd_rn(v, F[r * W + nx + 1]);
+    if (r == ny && c == nx) v = __fadd_rn(v, F[0]);
+    if (r == ny && c == 1) v = __fadd_rn(v, F[nx + 1]);
+    if (r == 1 && c == nx) v = __fadd_rn(v, F[(ny + 1) * W + 0]);
+    if (r == 1 && c == 1) v = __fadd_rn(v, F[(ny + 1) * W + nx + 1]);
+    F[r * W + c] = v;
+  }
+}
+
+__device__ __forceinline__ int wrap_row(int r, int n) { return r == 0 ? n : (r == n + 1 ? 1 : r); }
+
+// Field::update_ghosts: every ghost cell <- its periodic interior image.
+__global__ void k_update_ghosts(FieldList L, Grid g) {
+  float* F = L.f[blockIdx.y];
+  const int nx = g.nx, ny = g.ny, W = g.W;
+  const int nper = 2 * (nx + 2) + 2 * ny;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nper; p += gridDim.x * blockDim.x) {
+    int r, c;
+    if (p < nx + 2) { r = 0; c = p; }
+    else if (p < 2 * (nx + 2)) { r = ny + 1; c = p - (nx + 2); }
+    else if (p < 2 * (nx + 2) + ny) { r = p - 2 * (nx + 2) + 1; c = 0; }
+    else { r = p - 2 * (nx + 2) - ny + 1; c = nx + 1; }
+    F[r * W + c] = F[wrap_row(r, ny) * W + wrap_row(c, nx)];
+  }
+}
+
+// One binomial_filter_2_d pass for every cell of the ghosted output: interior
+// cells apply the 1-2-1 x 1-2-1 / 16 stencil to the input (whose ghost cells
+// hold whatever the input had, as in the reference); ghost cells receive the
+// filtered value of their periodic image (the update_ghosts that follows in
+// the reference).  Reference summation order, no contraction: bit-exact.
+__global__ void k_filter(ConstFieldList S, FieldList D, Grid g) {
+  const float* in = S.f[blockIdx.z];
+  float* out = D.f[blockIdx.z];
+  const int W = g.W;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y * blockDim.y + threadIdx.y;
+  if (c > g.nx + 1 || r > g.ny + 1) return;
+  const int ri = wrap_row(r, g.ny), ci = wrap_row(c, g.nx);
+  const float* up = in + (ri - 1) * W + ci;
+  const float* md = in + ri * W + ci;
+  const float* dn = in + (ri + 1) * W + ci;
+  float v = __fmul_rn(0.0625f, up[-1]);
+  v = __fadd_rn(v, __fmul_rn(0.125f, up[0]));
+  v = __fadd_rn(v, __fmul_rn(0.0625f, up[1]));
+  v = __fadd_rn(v, __fmul_rn(0.125f, md[-1]));
+  v = __fadd_rn(v, __fmul_rn(0.25f, md[0]));
+  v = __fadd_rn(v, __fmul_rn(0.125f, md[1]));
+  v = __fadd_rn(v, __fmul_rn(0.0625f, dn[-1]));
+  v = __fadd_rn(v, __fmul_rn(0.125f, dn[0]));
+  v = __fadd_rn(v, __fmul_rn(0.0625f, dn[1]));
+  out[r * W + c] = v;
+}
+
+__global__ void k_scale_c(float2* d, size_t n, float s) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    d[i] = c_scale(d[i], s);
+}
+
+// ---------------------------------------------------------------- host launchers
+void launch_fold(const Grid& g, float* const* fields, int nf, cudaStream_t st) {
+  FieldList L{};
+  for (int i = 0; i < nf; ++i) L.f[i] = fields[i];
+  int nper = 2 * g.nx + 2 * (g.ny - 2);
+  int blocks = (nper + 255) / 256;
+  k_fold<<<dim3(blocks, nf), 256, 0, st>>>(L, g);
+}
+
+void launch_update_ghosts(const Grid& g, float* const* fields, int nf, cudaStream_t st) {
+  FieldList L{};
+  for (int i = 0; i < nf; ++i) L.f[i] = fields[i];
+  int nper = 2 * (g.nx + 2) + 2 * g.ny;
+  k_update_ghosts<<<dim3((nper + 255) / 256, nf), 256, 0, st>>>(L, g);
+}
+
+void launch_filter_pass(const Grid& g, float* const* src, float* const* dst, int nf, cudaStream_t st) {
+  ConstFieldList S{};
+  FieldList D{};
+  for (int i = 0; i < nf; ++i) {
+    S.f[i] = src[i];
+    D.f[i] = dst[i];
+  }
+  dim3 blk(64, 4);
+  dim3 grd((g.nx + 2 + 63) / 64, (g.ny + 2 + 3) / 4, nf);
+  k_filter<<<grd, blk, 0, st>>>(S, D, g);
+}
+
+template <int IN, int OUT, bool INV>
+static void launch_rows(const Grid& g, const RowArgs& a, int nf, const float2* tw, cudaStream_t st) {
+  const int logB = row_logB(g.log2nx);
+  const int threads = std::max(1, (g.nx << logB) / 8);
+  const size_t smem = sizeof(float2) * ((size_t)g.nx << logB);
+  const int blocks = (g.ny + (1 << logB) - 1) >> logB;
+  static bool attr_set = false;
+  if (!attr_set) {
+    SPX_CUDA_TRY(cudaFuncSetAttribute(k_rows<IN, OUT, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    attr_set = true;
+  }
+  k_rows<IN, OUT, INV><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
+}
+
+template <bool INV>
+static void launch_cols(const Grid& g, const ColArgs& a, int nf, const float2* tw, cudaStream_t st) {
+  const int logW = col_logW(g.log2ny, g.log2nx);
+  const int threads = std::max(1, (g.ny << logW) / 8);
+  const size_t smem = sizeof(float2) * ((size_t)g.ny << logW);
+  const int blocks = g.nx >> logW;
+  static bool attr_set = false;
+  if (!attr_set) {
+    SPX_CUDA_TRY(cudaFuncSetAttribute(k_cols<INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    attr_set = true;
+  }
+  k_cols<INV><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
+}
+
+void FieldBuffers::allocate(const Grid& grid) {
+  g = grid;
+  const size_t ss = g.spatial_size() * sizeof(float);
+  for (int i = 0; i < SPX_NUM_FIELDS; ++i) {
+    SPX_CUDA_TRY(cudaMalloc(&spatial[i], ss));
+    SPX_CUDA_TRY(cudaMemset(spatial[i], 0, ss));
+  }
+  for (int i = 0; i < 4; ++i) {
+    SPX_CUDA_TRY(cudaMalloc(&filt_tmp[i], ss));
+    SPX_CUDA_TRY(cudaMemset(filt_tmp[i], 0, ss));
+  }
+  const size_t cs = g.spectral_size() * sizeof(float2);
+  for (int i = 0; i < SP_COUNT; ++i) {
+    SPX_CUDA_TRY(cudaMalloc(&spec[i], cs));
+    SPX_CUDA_TRY(cudaMemset(spec[i], 0, cs));
+  }
+  std::vector<float2> t(std::max(g.nx, g.ny));
+  SPX_CUDA_TRY(cudaMalloc(&tw_x, g.nx * sizeof(float2)));
+  SPX_CUDA_TRY(cudaMalloc(&tw_y, g.ny * sizeof(float2)));
+  make_twiddles(g.nx, t.data());
+  SPX_CUDA_TRY(cudaMemcpy(tw_x, t.data(), g.nx * sizeof(float2), cudaMemcpyHostToDevice));
+  make_twiddles(g.ny, t.data());
+  SPX_CUDA_TRY(cudaMemcpy(tw_y, t.data(), g.ny * sizeof(float2), cudaMemcpyHostToDevice));
+}
+
+void FieldBuffers::release() {
+  for (auto& p : spatial) { if (p) cudaFree(p); p = nullptr; }
+  for (auto& p : filt_tmp) { if (p) cudaFree(p); p = nullptr; }
+  for (auto& p : spec) { if (p) cudaFree(p); p = nullptr; }
+  if (tw_x) cudaFree(tw_x);
+  if (tw_y) cudaFree(tw_y);
+  tw_x = tw_y = nullptr;
+}
+
+int field_update(FieldBuffers& fb, cudaStream_t st) {
+  const Grid& g = fb.g;
+  int launches = 0;
+  // 1. n_pass binomial passes on jx, jy, jz, dsty (mod.rs:90-94), ping-pong.
+  float* cur[4] = {fb.spatial[SPX_JX], fb.spatial[SPX_JY], fb.spatial[SPX_JZ], fb.spatial[SPX_DSTY]};
+  float* oth[4] = {fb.filt_tmp[0], fb.filt_tmp[1], fb.filt_tmp[2], fb.filt_tmp[3]};
+  for (uint32_t p = 0; p < fb.n_pass; ++p) {
+    launch_filter_pass(g, cur, oth, 4, st);
+    ++launches;
+    for (int i = 0; i < 4; ++i) std::swap(cur[i], oth[i]);
+  }
+  if (fb.n_pass & 1) {  // keep the filtered result in the field's own buffer
+    for (int i = 0; i < 4; ++i)
+      SPX_CUDA_TRY(cudaMemcpyAsync(oth[i], cur[i], g.spatial_size() * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    launches += 4;
+  }
+  // 2. copy_to_spectral (+ dsty/dens) fused with the row FFTs (mod.rs:66-85, 101-103, 122-124)
+  {
+    RowArgs a{};
+    const int src_ids[7] = {SPX_JX, SPX_JY, SPX_JZ, SPX_DSTY, SPX_EX, SPX_EY, SPX_EZ};
+    const int dst_ids[7] = {SP_JX, SP_JY, SP_JZ, SP_RHO, SP_EX, SP_EY, SP_EZ};
+    for (int i = 0; i < 7; ++i) {
+      a.src[i] = fb.spatial[src_ids[i]];
+      a.dst[i] = fb.spec[dst_ids[i]];
+      a.scale[i] = 1.0f;
+    }
+    a.scale[3] = 1.0f / (float)fb.dens;
+    launch_rows<0, 0, false>(g, a, 7, fb.tw_x, st);
+    ++launches;
+    ColArgs c{};
+    for (int i = 0; i < 7; ++i) c.data[i] = fb.spec[dst_ids[i]];
+    launch_cols<false>(g, c, 7, fb.tw_y, st);
+    ++launches;
+  }
+  // 3. k-space update (mod.rs:105-278)
+  {
+    KArgs k;
+    k.jx = fb.spec[SP_JX]; k.jy = fb.spec[SP_JY]; k.jz = fb.spec[SP_JZ]; k.rho = fb.spec[SP_RHO];
+    k.ex = fb.spec[SP_EX]; k.ey = fb.spec[SP_EY]; k.ez = fb.spec[SP_EZ];
+    k.bwx = fb.spec[SP_BWX]; k.bwy = fb.spec[SP_BWY]; k.bwz = fb.spec[SP_BWZ];
+    k.bax = fb.spec[SP_BAX]; k.bay = fb.spec[SP_BAY]; k.baz = fb.spec[SP_BAZ];
+    k.ckc = fb.dt / (float)fb.dens;  // mod.rs:127
+    k.cdt = fb.dt * fb.c;            // mod.rs:128
+    const size_t n = g.spectral_size();
+    int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+    k_kspace<<<blocks, 256, 0, st>>>(k, g);
+    ++launches;
+  }
+  // 4. inverse transforms of B(t) and E, back to the spatial fields (mod.rs:281-307)
+  {
+    const int spec_ids[6] = {SP_BAX, SP_BAY, SP_BAZ, SP_EX, SP_EY, SP_EZ};
+    const int sp_ids[6] = {SPX_BX, SPX_BY, SPX_BZ, SPX_EX, SPX_EY, SPX_EZ};
+    ColArgs c{};
+    for (int i = 0; i < 6; ++i) c.data[i] = fb.spec[spec_ids[i]];
+    launch_cols<true>(g, c, 6, fb.tw_y, st);
+    ++launches;
+    RowArgs a{};
+    const float norm = 1.0f / (float)((uint64_t)g.nx * (uint64_t)g.ny);  // fft_2d.rs:170
+    for (int i = 0; i < 6; ++i) {
+      a.src[i] = fb.spec[spec_ids[i]];
+      a.dst[i] = fb.spatial[sp_ids[i]];
+      a.scale[i] = norm;
+    }
+    launch_rows<1, 1, true>(g, a, 6, fb.tw_x, st);
+    ++launches;
+  }
+  SPX_CUDA_TRY(cudaGetLastError());
+  return launches;
+}
+
+int fft2d_inplace(const Grid& g, float2* data, const float2* tw_x, const float2* tw_y, bool inverse,
+                  cudaStream_t st) {
+  RowArgs a{};
+  a.src[0] = data;
+  a.dst[0] = data;
+  ColArgs c{};
+  c.data[0] = data;
+  if (!inverse) {
+    a.scale[0] = 1.0f;
+    launch_rows<1, 0, false>(g, a, 1, tw_x, st);
+    launch_cols<false>(g, c, 1, tw_y, st);
+  } else {
+    // reference order: rows then columns, then the 1/(nx ny) scale (fft_2d.rs:132-172)
+    a.scale[0] = 1.0f;
+    launch_rows<1, 0, true>(g, a, 1, tw_x, st);
+    launch_cols<true>(g, c, 1, tw_y, st);
+    const size_t n = g.spectral_size();
+    const float norm = 1.0f / (float)n;
+    k_scale_c<<<(int)std::min<size_t>((n + 255) / 256, 4096), 256, 0, st>>>(data, n, norm);
+  }
+  SPX_CUDA_TRY(cudaGetLastError());
+  return 2;
+}
+
+}  // namespace spx

@@ -1,0 +1,132 @@
+// Particle species storage and kernels of the B200 hot path (src/prtls.rs and
+// the deposition half of src/lib.rs in the reference).
+#pragma once
+#include "common.cuh"
+
+namespace spx {
+
+constexpr int MAX_SPECIES = 4;
+
+// Split-path ("cell-slot") storage of one species.
+//
+// The grid is cut into tiles of TX x TY cells; tile t owns the contiguous
+// block [t*K*TC, (t+1)*K*TC) of every particle array (TC = TX*TY), laid out
+// slot-major: slot s of cell c (c = cell within the tile) is element
+// t*K*TC + s*TC + c.  A particle's cell is implied by where it is stored, so
+// a particle is {dx, dy, px, py, pz, tag} = 24 bytes (tag = its index in the
+// reference's particle order, used only to return data in that order).
+//
+// Two buffers alternate every step.  A cell's particles sit in slots
+// [0, n_low) and [K - n_top, K) of the read buffer.  During a step the thread
+// that owns the cell writes the particles that stay into slots 0, 1, ... of
+// the write buffer; particles that move to another cell are appended from the
+// top (slot K-1 downwards) of the destination cell through an atomic counter.
+// The appender bounds its slot by K - (n_low + n_top of the destination in the
+// read buffer), which the owner's writes can never reach, so the two never
+// collide.  A particle that finds no room goes to the overflow list, which a
+// fallback kernel processes every step until the host repacks with a larger K.
+struct SlotSpecies {
+  float* dx[2] = {};
+  float* dy[2] = {};
+  float* px[2] = {};
+  float* py[2] = {};
+  float* pz[2] = {};
+  uint32_t* tag[2] = {};
+  uint32_t* nlow[2] = {};
+  uint32_t* ntop[2] = {};
+  // overflow lists (double buffered): cell packed as ix | iy << 16 (reference coords)
+  uint32_t* ocell[2] = {};
+  float* odx[2] = {};
+  float* ody[2] = {};
+  float* opx[2] = {};
+  float* opy[2] = {};
+  float* opz[2] = {};
+  uint32_t* otag[2] = {};
+  uint32_t* ocount = nullptr;  // [2]
+  uint32_t ocap = 0;
+  int K = 0;
+  int cur = 0;  // read buffer
+};
+
+// Plain-path storage: global FP32 positions x = ix + dx, y = iy + dy in the
+// reference's particle order.
+struct PlainSpecies {
+  float *x = nullptr, *y = nullptr, *px = nullptr, *py = nullptr, *pz = nullptr;
+};
+
+struct Species {
+  float charge = 0, mass = 1, vth = 0, alpha = 0, beta = 0;
+  uint64_t n = 0;
+  SlotSpecies slot;
+  PlainSpecies plain;
+};
+
+struct ParticleGeom {
+  Grid g;
+  int TX = 16, TY = 16, logTX = 4, logTY = 4, NTX = 1, NTY = 1;
+  int TC() const { return TX * TY; }
+  int ntiles() const { return NTX * NTY; }
+  size_t ncells() const { return (size_t)g.nx * g.ny; }
+};
+
+struct PhysParams {
+  float dt, c, csqinv;
+  int periodic_x, left_wall, wall_loc, delta;
+};
+
+struct FieldPtrs {
+  const float* E[3];
+  const float* B[3];
+  float* J[3];
+  float* dsty;
+  float* dens;
+};
+
+// Device error word bits.
+enum : int { DERR_BOUNDS = 1, DERR_WALL = 2, DERR_OVERFLOW_LOST = 4, DERR_GAMMA = 8 };
+
+// --- split path ---------------------------------------------------------------
+// Upload: pack n particles (device arrays, cell packed ix | iy << 16) into the
+// slot layout with capacity K, in buffer 0.  Returns kernel launch count.
+void slot_allocate(Species& s, const ParticleGeom& pg, int K, uint64_t n);
+void slot_release(Species& s);
+// Count particles per cell (for choosing K).  counts: ncells uint32 (zeroed inside).
+void slot_count(const ParticleGeom& pg, uint64_t n, const uint32_t* cell, uint32_t* counts, cudaStream_t st);
+void slot_scatter(Species& s, const ParticleGeom& pg, uint64_t n, const uint32_t* cell, const float* dx,
+                  const float* dy, const float* px, const float* py, const float* pz, const uint32_t* tag,
+                  uint32_t* cursor, cudaStream_t st);
+// Download in reference order into device arrays indexed by tag.
+void slot_unpack(const Species& s, const ParticleGeom& pg, uint32_t* ix, uint32_t* iy, float* dx, float* dy,
+                 float* px, float* py, float* pz, float* psa, float csqinv, cudaStream_t st);
+// The fused particle kernel over species [s0, s1): PUSH = Boris push
+// (src/prtls.rs:262-443), MOVE = move_and_deposit (src/lib.rs:478-489) with
+// relocation.  Returns the number of launches.
+int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysParams& pp, const FieldPtrs& fp,
+              bool push, bool move, int* derr, cudaStream_t st);
+// Maximum cell occupancy (low + top + arrivals) after the last step, for repack decisions.
+void slot_max_occupancy(const Species& s, const ParticleGeom& pg, uint32_t* d_out, cudaStream_t st);
+
+// --- plain path ---------------------------------------------------------------
+int plain_move_deposit(Species& s, uint64_t n, const ParticleGeom& pg, const PhysParams& pp, const FieldPtrs& fp,
+                       int* derr, cudaStream_t st);
+int plain_push(Species& s, uint64_t n, const ParticleGeom& pg, const PhysParams& pp, const FieldPtrs& fp,
+               int* derr, cudaStream_t st);
+
+// --- diagnostics ----------------------------------------------------------------
+// Adds sum m (gamma-1) c^2 and the particle count into d_acc[0], d_acc[1] (double).
+void kinetic_energy(const Species& s, const ParticleGeom& pg, bool plain, float c, double* d_acc, cudaStream_t st);
+
+// --- device initialisation (seeded) ----------------------------------------------
+struct InitSpec {
+  float charge, mass, vth, gamma_drift, sign_x, c;
+  uint32_t ppc;
+  int x0, x1;  // columns [x0, x1) of the interior (0-based), every row
+  int random_positions;
+  uint64_t seed;
+};
+// Writes particles in the reference's particle order into device arrays
+// (cell packed, dx, dy, px, py, pz); tag = index.
+void init_particles(const InitSpec& is, const Grid& g, uint64_t n, uint32_t* cell, float* dx, float* dy, float* px,
+                    float* py, float* pz, cudaStream_t st);
+
+}  // namespace spx

@@ -1,0 +1,233 @@
+"""Host mirror of the reference's hot-path API over the C ABI.
+
+The reference's types and call sequence (src/lib.rs, src/prtls.rs, src/flds)
+map onto this module as follows:
+
+  Sim::new (src/lib.rs:247-264)                  -> Sim(cfg)
+  Prtl::new (src/prtls.rs:60-84)                 -> Sim.add_species / Prtl
+  Flds::new (src/flds/mod.rs:40-65)              -> created with the Sim (device resident)
+  Sim::move_and_deposit (src/lib.rs:478-489)     -> Sim.move_and_deposit(prtl)
+  Field::deposit_ghosts (src/flds/field.rs:260)  -> Flds.deposit_ghosts(name)
+  Flds::update (src/flds/mod.rs:87-309)          -> Flds.update(sim)
+  Prtl::boris_push (src/prtls.rs:262-443)        -> Prtl.boris_push(sim, flds)
+  run (src/lib.rs:119-202)                       -> run(cfg)
+
+All state lives in device memory; getters copy back in the reference layout.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .config import Config
+from .init import species_arrays
+
+
+class Sim:
+    """Owns one device context (``spx_ctx``)."""
+
+    def __init__(self, cfg: Config, path=None):
+        self.lib = _lib.load()
+        self.config = cfg
+        p = cfg.params
+        self.t = 0
+        self.t_final = cfg.setup.t_final
+        self.size_x, self.size_y, self.delta = p.size_x, p.size_y, p.delta
+        self.dt, self.c, self.dens = p.dt, p.c, p.dens
+        self.gamma_inj, self.n_pass = p.gamma_inj, p.n_pass
+        self.prtl_num = p.dens * (p.size_x - 2 * p.delta) * p.size_y  # src/lib.rs:258-260
+        prm = _lib.SpxParams(
+            size_x=p.size_x, size_y=p.size_y, delta=p.delta, dt=p.dt, c=p.c, dens=p.dens,
+            gamma_inj=p.gamma_inj, n_pass=p.n_pass, periodic_x=1 if p.periodic_x else 0,
+            left_wall=1 if p.left_wall else 0,
+            path=_lib.PATH_PLAIN if (path or p.path) == "plain" else _lib.PATH_SPLIT,
+            tile_x=p.tile_x, tile_y=p.tile_y, slot_capacity=p.slot_capacity, device=0)
+        self._ctx = ctypes.c_void_p()
+        _lib.check(self.lib.spx_create(ctypes.byref(prm), ctypes.byref(self._ctx)))
+        self.flds = Flds(self)
+        self.prtls = []
+
+    # -- lifecycle -------------------------------------------------------------------
+    def close(self):
+        if self._ctx:
+            self.lib.spx_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _chk(self, code):
+        return _lib.check(code, self._ctx)
+
+    # -- species ---------------------------------------------------------------------
+    def add_species(self, charge, mass, vth, ix, iy, dx, dy, px, py, pz, psa=None):
+        """Prtl::new with caller-supplied state (arrays in the reference's order)."""
+        n = len(ix)
+        arrs = [np.ascontiguousarray(ix, dtype=np.uint64), np.ascontiguousarray(iy, dtype=np.uint64)]
+        arrs += [np.ascontiguousarray(a, dtype=np.float32) for a in (dx, dy, px, py, pz)]
+        ps = None if psa is None else np.ascontiguousarray(psa, dtype=np.float32)
+        sid = ctypes.c_int32(-1)
+        self._chk(self.lib.spx_add_species(self._ctx, charge, mass, vth, n, *[_lib.ptr(a) for a in arrs],
+                                           _lib.ptr(ps), ctypes.byref(sid)))
+        pr = Prtl(self, sid.value, charge, mass, vth)
+        self.prtls.append(pr)
+        return pr
+
+    def init_species(self, charge, mass, vth, ppc, x0, x1, gamma_drift=0.0, sign_x=1.0,
+                     random_positions=True, seed=0):
+        """Seeded on-device initialisation (no host arrays)."""
+        sid = ctypes.c_int32(-1)
+        self._chk(self.lib.spx_init_species(self._ctx, charge, mass, vth, ppc, x0, x1, gamma_drift, sign_x,
+                                            1 if random_positions else 0, seed, ctypes.byref(sid)))
+        pr = Prtl(self, sid.value, charge, mass, vth)
+        self.prtls.append(pr)
+        return pr
+
+    def init_from_config(self):
+        """The species of run() (src/lib.rs:121-126), from host arrays drawn with the config's seed."""
+        for k, spec in enumerate(self.config.species_list()):
+            a = species_arrays(self.config.params, spec, seed_offset=k)
+            self.add_species(spec.charge, spec.mass, spec.vth, a["ix"], a["iy"], a["dx"], a["dy"],
+                             a["px"], a["py"], a["pz"], a["psa"])
+        return self.prtls
+
+    # -- the hot path -------------------------------------------------------------------
+    def move_and_deposit(self, prtl):
+        self._chk(self.lib.spx_move_and_deposit(self._ctx, prtl.sid))
+
+    def zero_sources(self):
+        self._chk(self.lib.spx_zero_sources(self._ctx))
+
+    def prepare(self):
+        """The extra move+deposit and ghost fold before the loop (src/lib.rs:130-142)."""
+        self._chk(self.lib.spx_prepare(self._ctx))
+
+    def step(self, n=1):
+        """n iterations of run()'s loop body without output (fused, graph-captured)."""
+        self._chk(self.lib.spx_step(self._ctx, n))
+        self.t += n
+
+    def flush(self):
+        self._chk(self.lib.spx_flush(self._ctx))
+
+    def synchronize(self):
+        self._chk(self.lib.spx_synchronize(self._ctx))
+
+    def diag(self):
+        """FP64 device diagnostics: (E energy, B energy, kinetic energy, net charge, particles)."""
+        out = np.zeros(5, dtype=np.float64)
+        self._chk(self.lib.spx_diag(self._ctx, _lib.ptr(out)))
+        return out
+
+    def set_timing(self, on=True):
+        self._chk(self.lib.spx_set_timing(self._ctx, 1 if on else 0))
+
+    def timing(self):
+        out = np.zeros(4, dtype=np.float32)
+        self._chk(self.lib.spx_get_timing(self._ctx, _lib.ptr(out)))
+        return out
+
+    def last_launch_count(self):
+        return int(self.lib.spx_last_launch_count(self._ctx))
+
+
+class Flds:
+    """Device-resident fields with the reference's names (src/flds/mod.rs:15-37)."""
+
+    NAMES = ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Jx", "Jy", "Jz", "Rho", "Dens")
+
+    def __init__(self, sim):
+        self.sim = sim
+
+    def spatial(self, name, with_ghosts=True):
+        s = self.sim
+        shape = (s.size_y + 2, s.size_x + 2) if with_ghosts else (s.size_y, s.size_x)
+        out = np.empty(shape, dtype=np.float32)
+        s._chk(s.lib.spx_get_field(s._ctx, _lib.FIELD_IDS[name], 1 if with_ghosts else 0, _lib.ptr(out)))
+        return out
+
+    def set_spatial(self, name, arr):
+        s = self.sim
+        a = np.ascontiguousarray(arr, dtype=np.float32)
+        assert a.size == (s.size_y + 2) * (s.size_x + 2)
+        s._chk(s.lib.spx_set_field(s._ctx, _lib.FIELD_IDS[name], _lib.ptr(a)))
+
+    def b_wrk(self, comp):
+        s = self.sim
+        out = np.empty((s.size_y, s.size_x), dtype=np.complex64)
+        s._chk(s.lib.spx_get_bwrk(s._ctx, comp, _lib.ptr(out)))
+        return out
+
+    def set_b_wrk(self, comp, arr):
+        s = self.sim
+        a = np.ascontiguousarray(arr, dtype=np.complex64)
+        s._chk(s.lib.spx_set_bwrk(s._ctx, comp, _lib.ptr(a)))
+
+    def deposit_ghosts(self, name):
+        s = self.sim
+        s._chk(s.lib.spx_deposit_ghosts(s._ctx, _lib.FIELD_IDS[name]))
+
+    def update(self, sim=None):
+        s = self.sim
+        s._chk(s.lib.spx_fields_update(s._ctx))
+
+
+class Prtl:
+    """Handle on one device-resident species (src/prtls.rs:8-23)."""
+
+    def __init__(self, sim, sid, charge, mass, vth):
+        self.sim, self.sid = sim, sid
+        self.charge, self.mass, self.vth = charge, mass, vth
+        f = np.float32
+        self.beta = (f(charge) / f(mass)) * f(0.5) * f(sim.dt)           # src/prtls.rs:61
+        self.alpha = (f(charge) / f(mass)) * f(0.5) * f(sim.dt) / f(sim.c)  # src/prtls.rs:62
+
+    def __len__(self):
+        return int(self.sim.lib.spx_species_count(self.sim._ctx, self.sid))
+
+    def state(self, stride=1):
+        """dict of ix, iy (uint64), dx, dy, px, py, pz, psa (float32) in the reference order."""
+        s = self.sim
+        n = len(self)
+        m = (n + stride - 1) // stride
+        out = {k: np.empty(m, dtype=np.uint64) for k in ("ix", "iy")}
+        out.update({k: np.empty(m, dtype=np.float32) for k in ("dx", "dy", "px", "py", "pz", "psa")})
+        s._chk(s.lib.spx_get_species(s._ctx, self.sid, stride, *[_lib.ptr(out[k]) for k in
+                                                                 ("ix", "iy", "dx", "dy", "px", "py", "pz", "psa")]))
+        return out
+
+    def boris_push(self, sim=None, flds=None):
+        self.sim._chk(self.sim.lib.spx_boris_push(self.sim._ctx, self.sid))
+
+
+def run(cfg: Config, out_dir="output", on_step=None):
+    """run (src/lib.rs:119-202): init, pre-loop move+deposit, then t_final+1
+    iterations; save_output at every output_interval when write_output is set.
+    The fused device step is used between saves."""
+    from .save import save_output
+    with Sim(cfg) as sim:
+        sim.init_from_config()
+        sim.prepare()
+        t = 0
+        while t <= sim.t_final:
+            if cfg.output.write_output and t % cfg.output.output_interval == 0:
+                save_output(t, sim, out_dir)
+            # run until the next save step (or the end) in one fused call
+            nxt = sim.t_final + 1
+            if cfg.output.write_output:
+                nxt = min(nxt, (t // cfg.output.output_interval + 1) * cfg.output.output_interval)
+            sim.step(nxt - t)
+            if on_step:
+                on_step(sim, nxt - 1)
+            t = nxt
+        sim.flush()
+        return sim.diag()

@@ -1,0 +1,46 @@
+"""The C-ABI library loads and exports exactly what include/spectral_gpu.h declares (no GPU needed)."""
+import ctypes
+import os
+import re
+import subprocess
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "spectral_gpu.h")
+
+
+def declared():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"^SPX_API\s+[\w\s\*]+?\b(spx_\w+)\s*\(", txt, flags=re.M)))
+
+
+def test_header_declares_the_binding_list():
+    from spectral_rs_b200 import _lib
+    assert declared() == sorted(_lib.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol():
+    from spectral_rs_b200 import _lib
+    lib = _lib.load()
+    for name in declared():
+        assert hasattr(lib, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = sorted(set(re.findall(r"\bT (spx_\w+)", out)))
+    assert exported == declared()
+
+
+def test_params_struct_layout_matches_header():
+    # the ctypes mirror must have the C struct's size: 3 u64 + 2 f32 + u32 + f32 + u32 + 7 i32 = 72 bytes
+    from spectral_rs_b200 import _lib
+    assert ctypes.sizeof(_lib.SpxParams) == 72
+
+
+def test_errors_without_device_are_reported_not_crashing():
+    # spx_create on a machine without a usable device must fail with a status, not abort
+    from spectral_rs_b200 import _lib
+    lib = _lib.load()
+    prm = _lib.SpxParams(size_x=24, size_y=12, delta=5, dt=0.1, c=3.0, dens=2, gamma_inj=5.0, n_pass=4)
+    ctx = ctypes.c_void_p()
+    code = lib.spx_create(ctypes.byref(prm), ctypes.byref(ctx))
+    assert code == 1  # 24 is not a power of two: rejected before touching a device
+    assert b"power-of-two" in lib.spx_last_error(None)

@@ -1,0 +1,277 @@
+"""GPU particle kernels against the CPU oracle (FP32 reference path and FP64 dprec path).
+
+Bit-exact on identical inputs: cell indices (ix, iy), offsets (dx, dy), momenta
+and Lorentz factors after boris_push and after move_and_deposit (the particle
+TU is built with -fmad=false, IEEE div/sqrt, exactly like the reference's
+Rust arithmetic).  Deposited J / rho / dens differ only by summation order:
+compared with a relative tolerance.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+from conftest import test_params
+
+pytestmark = pytest.mark.gpu
+
+DEP_RTOL = 4e-6  # summation-order tolerance on deposited moments (relative to max |field|)
+
+
+def _cfg(**kw):
+    from spectral_rs_b200.config import Config, Setup, Output
+    return Config(test_params(**kw), Setup(10), Output(False, False, 1, 1, 1, 1))
+
+
+def _species(p, ppc, vth, gamma, sign, seed, random_positions=True, x0=None, x1=None):
+    from spectral_rs_b200.init import positions, draws, velocities
+    rng = np.random.default_rng(seed)
+    ix, iy, dx, dy = positions(p.size_x, p.size_y, p.delta, ppc, x0, x1, random_positions, rng)
+    nrm, uni = draws(len(ix), rng)
+    px, py, pz, psa = velocities(nrm, uni, p.c, vth, gamma, sign)
+    return dict(ix=ix, iy=iy, dx=dx, dy=dy, px=px, py=py, pz=pz, psa=psa)
+
+
+def _pair(cfg, specs, dtype=np.float32, path=None):
+    from spectral_rs_b200 import Sim
+    sim = Sim(cfg, path=path)
+    o = orc.OracleSim.from_params(cfg.params, dtype=dtype)
+    for (q, m, vth, a) in specs:
+        sim.add_species(q, m, vth, a["ix"], a["iy"], a["dx"], a["dy"], a["px"], a["py"], a["pz"], a["psa"])
+        o.add_species(q, m, vth, a["ix"], a["iy"], a["dx"], a["dy"], a["px"], a["py"], a["pz"], a["psa"])
+    return sim, o
+
+
+def _random_fields(sim, o, seed, scale=0.05):
+    rng = np.random.default_rng(seed)
+    for name in ("Ex", "Ey", "Ez", "Bx", "By", "Bz"):
+        f = (rng.standard_normal((sim.size_y + 2, sim.size_x + 2)) * scale).astype(np.float32)
+        sim.flds.set_spatial(name, f)
+        o.set_spatial(name, f.astype(o.dtype))
+
+
+def _assert_state_equal(g, r, keys=("ix", "iy", "dx", "dy", "px", "py", "pz", "psa")):
+    for k in keys:
+        assert np.array_equal(g[k], r[k].astype(g[k].dtype)), (k, np.flatnonzero(g[k] != r[k])[:5])
+
+
+def _assert_moments_close(sim, o, names=("Jx", "Jy", "Jz", "Rho", "Dens"), rtol=DEP_RTOL):
+    dens = np.max(np.abs(o.spatial("Dens")))
+    for name in names:
+        g, r = sim.flds.spatial(name), o.spatial(name).astype(np.float64)
+        # charge of +-1 species cancels: measure its error against the number density
+        scale = max(np.max(np.abs(r)), dens if name == "Rho" else 0.0, 1e-30)
+        err = np.max(np.abs(g - r)) / scale
+        assert err < rtol, (name, err)
+
+
+@pytest.mark.parametrize("periodic", [True, False])
+def test_boris_push_bit_exact(periodic):
+    cfg = _cfg(size_x=64, size_y=32, delta=6, c=4.5, dt=0.1, dens=8, periodic_x=periodic, left_wall=not periodic)
+    p = cfg.params
+    specs = [(1.0, 16.0, 0.1, _species(p, 8, 0.1, 1.0050378, 1.0, 1)),
+             (-1.0, 1.0, 0.1, _species(p, 8, 0.1, 1.0050378, 1.0, 2))]
+    sim, o = _pair(cfg, specs)
+    _random_fields(sim, o, 3)
+    for s in range(2):
+        sim.prtls[s].boris_push()
+        o.boris_push(s)
+        _assert_state_equal(sim.prtls[s].state(), o.state(s))
+    sim.close()
+
+
+@pytest.mark.parametrize("periodic", [True, False])
+def test_move_and_deposit_bit_exact(periodic):
+    cfg = _cfg(size_x=64, size_y=32, delta=6, c=4.5, dt=0.1, dens=8, periodic_x=periodic, left_wall=not periodic)
+    p = cfg.params
+    specs = [(1.0, 16.0, 0.1, _species(p, 8, 0.1, 1.0050378, 1.0, 11)),
+             (-1.0, 1.0, 0.3, _species(p, 8, 0.3, 1.2, 1.0, 12))]
+    sim, o = _pair(cfg, specs)
+    for s in range(2):
+        sim.move_and_deposit(sim.prtls[s])
+        o.move_and_deposit(s)
+        _assert_state_equal(sim.prtls[s].state(), o.state(s))
+    _assert_moments_close(sim, o)
+    for name in ("Jx", "Jy", "Jz", "Rho", "Dens"):
+        sim.flds.deposit_ghosts(name)
+    o.fold_sources()
+    _assert_moments_close(sim, o)
+    sim.close()
+
+
+def test_wall_reflection_bit_exact():
+    # fast particles driven into the reflecting wall (src/prtls.rs:153-188), several moves
+    cfg = _cfg(size_x=32, size_y=16, delta=4, c=4.5, dt=0.1, dens=4, periodic_x=False)
+    p = cfg.params
+    a = _species(p, 4, 0.05, 3.0, 1.0, 21, x0=20, x1=28)
+    sim, o = _pair(cfg, [(-1.0, 1.0, 0.05, a)])
+    for _ in range(12):
+        sim.move_and_deposit(sim.prtls[0])
+        o.move_and_deposit(0)
+    g = sim.prtls[0].state()
+    _assert_state_equal(g, o.state(0))
+    assert np.max(g["ix"]) <= p.size_x + 1 - p.delta + 1
+    sim.close()
+
+
+def test_wall_assertion_like_the_reference():
+    """Without the optional left wall, a particle reaching ix <= delta trips the
+    reference's assertion (src/prtls.rs:163-170): an error status on both sides."""
+    from spectral_rs_b200 import _lib
+    cfg = _cfg(size_x=32, size_y=16, delta=4, c=4.5, dt=0.1, dens=4, periodic_x=False)
+    p = cfg.params
+    a = _species(p, 4, 0.3, 1.0, 1.0, 23, x0=4, x1=8)  # hot plasma next to the left edge
+    sim, o = _pair(cfg, [(-1.0, 1.0, 0.3, a)])
+    with pytest.raises(_lib.SpxError) as ei:
+        for _ in range(10):
+            sim.move_and_deposit(sim.prtls[0])
+    assert ei.value.code == 4  # SPX_ERR_WALL
+    with pytest.raises(RuntimeError):
+        for _ in range(10):
+            o.move_and_deposit(0)
+    sim.close()
+
+
+def test_fused_step_equals_per_phase_sequence():
+    """spx_step (push of step t fused with move+deposit of t+1, CUDA graphs) must
+    equal the reference's sequence of per-phase calls on the same device."""
+    from spectral_rs_b200 import Sim
+    cfg = _cfg(size_x=64, size_y=32, delta=0, c=4.5, dt=0.1, dens=8, periodic_x=True, n_pass=2)
+    p = cfg.params
+    sp = [(1.0, 16.0, 0.1, _species(p, 8, 0.1, 1.0, 1.0, 31)), (-1.0, 1.0, 0.1, _species(p, 8, 0.1, 1.0, 1.0, 32))]
+    fused = Sim(cfg)
+    phased = Sim(cfg)
+    for (q, m, v, a) in sp:
+        for s in (fused, phased):
+            s.add_species(q, m, v, a["ix"], a["iy"], a["dx"], a["dy"], a["px"], a["py"], a["pz"], a["psa"])
+    fused.prepare()
+    phased.prepare()
+    fused.step(5)
+    for _ in range(5):
+        phased.zero_sources()
+        for pr in phased.prtls:
+            phased.move_and_deposit(pr)
+        for name in ("Jx", "Jy", "Jz", "Rho", "Dens"):
+            phased.flds.deposit_ghosts(name)
+        phased.flds.update()
+        for pr in phased.prtls:
+            pr.boris_push()
+    # deposits are summed in a different order on every run, so after the first
+    # field solve the two agree to rounding, not bit for bit
+    for s in range(2):
+        a, b = fused.prtls[s].state(), phased.prtls[s].state()
+        assert np.mean((a["ix"] != b["ix"]) | (a["iy"] != b["iy"])) < 1e-3
+        assert np.max(np.abs(a["px"] - b["px"])) < 1e-4 * np.max(np.abs(b["px"]))
+    for name in ("Ex", "Ey", "Ez", "Bx", "By", "Bz"):
+        a, b = fused.flds.spatial(name), phased.flds.spatial(name)
+        assert np.max(np.abs(a - b)) <= 1e-4 * max(np.max(np.abs(b)), 1e-30), name
+    fused.close()
+    phased.close()
+
+
+@pytest.mark.parametrize("periodic,steps", [(True, 20), (False, 20)])
+def test_run_vs_oracle(periodic, steps):
+    """The full loop (src/lib.rs:130-200) against the FP32 and FP64 oracles."""
+    from spectral_rs_b200 import Sim
+    cfg = _cfg(size_x=64, size_y=32, delta=0 if periodic else 6, c=4.5, dt=0.1, dens=8, periodic_x=periodic,
+               left_wall=not periodic, n_pass=4)
+    p = cfg.params
+    specs = [(1.0, 16.0, 0.1, _species(p, 8, 0.1, 1.0050378, 1.0, 41, random_positions=True)),
+             (-1.0, 1.0, 0.1, _species(p, 8, 0.1, 1.0050378, 1.0, 42, random_positions=True))]
+    sim, o32 = _pair(cfg, specs, np.float32)
+    _, o64 = None, orc.OracleSim.from_params(p, dtype=np.float64)
+    for (q, m, v, a) in specs:
+        o64.add_species(q, m, v, a["ix"], a["iy"], a["dx"], a["dy"], a["px"], a["py"], a["pz"], a["psa"])
+    sim.prepare()
+    o32.prepare()
+    o64.prepare()
+    sim.step(steps)
+    o32.step(steps)
+    o64.step(steps)
+    for name in ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Jx", "Dens"):
+        g, r = sim.flds.spatial(name).astype(np.float64), o64.spatial(name)
+        r32 = o32.spatial(name).astype(np.float64)
+        scale = max(np.max(np.abs(r)), 1e-30)
+        err_gpu, err_ref = np.max(np.abs(g - r)) / scale, np.max(np.abs(r32 - r)) / scale
+        # GPU FP32 error against FP64 within a small factor of the reference FP32 path's own error
+        assert err_gpu < max(10 * err_ref, 1e-5), (name, err_gpu, err_ref)
+    for s in range(2):
+        g, r = sim.prtls[s].state(), o32.state(s)
+        mism = np.mean((g["ix"] != r["ix"]) | (g["iy"] != r["iy"]))
+        assert mism < 1e-3, mism
+        assert np.max(np.abs(g["px"] - r["px"])) < 1e-3 * max(np.max(np.abs(r["px"])), 1e-30)
+    sim.close()
+
+
+def test_plain_path_vs_oracle():
+    """The plain FP32 baseline (global positions, unfused, atomics) stays within tolerance."""
+    cfg = _cfg(size_x=64, size_y=32, delta=0, c=4.5, dt=0.1, dens=8, periodic_x=True, n_pass=4)
+    p = cfg.params
+    specs = [(1.0, 16.0, 0.1, _species(p, 8, 0.1, 1.0, 1.0, 51)), (-1.0, 1.0, 0.1, _species(p, 8, 0.1, 1.0, 1.0, 52))]
+    sim, o = _pair(cfg, specs, np.float64, path="plain")
+    sim.prepare()
+    o.prepare()
+    sim.step(10)
+    o.step(10)
+    for name in ("Ex", "Ey", "Bz", "Jx", "Dens"):
+        g, r = sim.flds.spatial(name), o.spatial(name)
+        assert np.max(np.abs(g - r)) / max(np.max(np.abs(r)), 1e-30) < 1e-3, name
+    for s in range(2):
+        g, r = sim.prtls[s].state(), o.state(s)
+        x_g = g["ix"].astype(np.float64) + g["dx"]
+        x_r = r["ix"].astype(np.float64) + r["dx"]
+        assert np.max(np.abs(x_g - x_r)) < 1e-2
+    sim.close()
+
+
+def test_slot_overflow_and_repack():
+    """Slot capacity equal to the initial occupancy: every arrival overflows into
+    the fallback list, which must give the same particles; spx_step then repacks."""
+    cfg = _cfg(size_x=32, size_y=16, delta=0, c=4.5, dt=0.1, dens=4, periodic_x=True, n_pass=2, slot_capacity=-4)
+    p = cfg.params
+    a = _species(p, 4, 0.2, 1.0, 1.0, 61, random_positions=False)
+    sim, o = _pair(cfg, [(-1.0, 1.0, 0.2, a)])
+    for _ in range(6):
+        sim.move_and_deposit(sim.prtls[0])
+        o.move_and_deposit(0)
+        _assert_state_equal(sim.prtls[0].state(), o.state(0))
+    _assert_moments_close(sim, o)
+    sim.prepare()
+    o.prepare()
+    sim.step(4)
+    o.step(4)
+    g, r = sim.prtls[0].state(), o.state(0)
+    assert np.mean((g["ix"] != r["ix"]) | (g["iy"] != r["iy"])) < 1e-3
+    assert len(g["ix"]) == len(a["ix"])
+    sim.close()
+
+
+def test_diag_counts_and_charge():
+    cfg = _cfg(size_x=64, size_y=32, delta=0, c=4.5, dt=0.1, dens=8, periodic_x=True)
+    p = cfg.params
+    a = _species(p, 8, 0.1, 1.0, 1.0, 71)
+    b = _species(p, 8, 0.1, 1.0, 1.0, 72)
+    sim, o = _pair(cfg, [(1.0, 1.0, 0.1, a), (-1.0, 1.0, 0.1, b)])
+    sim.prepare()
+    d = sim.diag()
+    assert d[4] == len(a["ix"]) + len(b["ix"])
+    # kinetic energy, FP64 sum of m (gamma - 1) c^2
+    o.prepare()
+    ke = sum(np.sum((o.state(s)["psa"].astype(np.float64) - 1.0)) for s in range(2)) * 4.5 ** 2
+    assert abs(d[2] - ke) <= 1e-6 * ke
+    # net deposited charge of a neutral plasma after the fold is ~0
+    assert abs(d[3]) < 1e-2 * len(a["ix"])
+    sim.close()
+
+
+def test_device_init_statistics():
+    from spectral_rs_b200 import Sim
+    cfg = _cfg(size_x=64, size_y=32, delta=0, c=4.5, dt=0.1, dens=16, periodic_x=True)
+    with Sim(cfg) as sim:
+        pr = sim.init_species(-1.0, 1.0, 0.1, 16, 0, 64, gamma_drift=0.0, random_positions=True, seed=5)
+        st = pr.state()
+        assert len(st["ix"]) == 64 * 32 * 16
+        assert np.all((st["dx"] >= -0.5) & (st["dx"] < 0.5))
+        assert abs(np.std(st["px"]) / (0.1 * 4.5) - 1) < 0.02
+        assert abs(np.mean(st["py"])) < 0.01
+        # every cell holds exactly ppc particles, in reference order
+        assert np.all(np.bincount((st["iy"] - 1) * 64 + (st["ix"] - 1)) == 16)
