@@ -1,0 +1,361 @@
+#!/usr/bin/env python
+"""Benchmark of the spectral_rs per-timestep hot path on B200.
+
+Metric: particle-steps/s (particles x steps / device time of the timed steps)
+and the HBM roofline fraction of the fused push + move + deposit kernel.
+
+Workload (one GPU): the plain method at scale -- a 2-D periodic thermal
+electron-proton plasma on a 4096 x 1024 grid, mass ratio 64, 64 particles per
+cell per species (536,870,912 particles), Maxwellian momenta with thermal
+spread 0.05c drawn from a seed, FP32 fields and particles, 4 binomial filter
+passes per step, c = 4.5, dt = 0.1 (Courant number c dt = 0.45).  Synthetic
+data from the build's own seeded generator; a "step" is one iteration of the
+reference's loop (zero sources, move + deposit both species, ghost fold,
+Flds::update, Boris push).  The particle arrays (13 GB) exceed the 126 MB L2,
+so no flush is needed between steps.
+
+Besides `value` (device-resident, split path) the line carries:
+  plain_fp32   the plain single-simulation FP32 GPU path on the same workload
+  roofline     the fused particle kernel: algorithmic bytes / CUDA-event time
+  cpu_baseline the C++ restatement of the reference CPU path (oracle/) on a crop
+  e2e          the same metric through the public API from host buffers
+  clocks       SM clocks sampled during the timed region
+
+--impl reference times the reference's CPU path (the oracle restatement; the
+Rust crate cannot be built here) on all host cores, same metric and workload,
+each step a 512 x 256 crop of it.
+
+Multi-GPU (torchrun): the workload does not shard without exchange steps, so
+N > 1 runs N independent replicas (weak scaling); the time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(name="thermal_ep_4096x1024_ppc64", size_x=4096, size_y=1024, delta=0, dt=0.1, c=4.5, dens=64,
+                n_pass=4, mass_ratio=64.0, vth=0.05, ppc=64)
+CROP = dict(size_x=512, size_y=256)  # CPU sample of the same plasma
+FALLBACK_HBM_GBS = 6650.0
+B_PER_PARTICLE = 48.0  # {cell, dx, dy, px, py, pz} read and written once
+B_PER_CELL = 44.0      # E, B read (24 B); Jx, Jy, Jz, rho, dens written (20 B)
+
+
+def params(w, **over):
+    from spectral_rs_b200.config import Params
+    d = dict(size_x=w["size_x"], size_y=w["size_y"], delta=w["delta"], dt=w["dt"], c=w["c"], dens=w["dens"],
+             gamma_inj=1.0, n_pass=w["n_pass"], mass_ratio=w["mass_ratio"], vth=w["vth"], periodic_x=True)
+    d.update(over)
+    return Params(**d)
+
+
+def make_sim(w, path="split", seed=0):
+    from spectral_rs_b200 import Sim
+    from spectral_rs_b200.config import Config, Setup, Output
+    cfg = Config(params(w), Setup(0), Output(False, False, 1, 1, 1, 1))
+    sim = Sim(cfg, path=path)
+    # ions then electrons, as run() creates them (src/lib.rs:124-126); seeded device init
+    sim.init_species(1.0, w["mass_ratio"], w["vth"], w["ppc"], 0, w["size_x"], 0.0, 1.0, True, seed * 2 + 1)
+    sim.init_species(-1.0, 1.0, w["vth"], w["ppc"], 0, w["size_x"], 0.0, 1.0, True, seed * 2 + 2)
+    return sim
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "100"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        time.sleep(0.15)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        rows = [r for r in self.rows if len(r) >= 7]
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[3 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_per_launch(particles, cells):
+    """dram bytes of the fused kernel from the committed ncu summary, scaled to this launch."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "k_slot_traffic.json")) as f:
+            t = json.load(f)
+        return t["dram_bytes_per_particle"] * particles + t.get("dram_bytes_per_cell", 0.0) * cells
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+# ---------------------------------------------------------------- CPU (oracle) arms
+def oracle_crop_rate(w, seconds_target, steps=None, warmup=1):
+    """The reference CPU path (C++ restatement, all host threads) on a crop of the workload."""
+    from oracle import oracle as orc
+    from spectral_rs_b200.config import SpeciesSpec
+    from spectral_rs_b200.init import species_arrays
+    p = params(w, size_x=CROP["size_x"], size_y=CROP["size_y"], random_positions=True, seed=7)
+    o = orc.OracleSim.from_params(p, dtype=np.float32)
+    n = 0
+    for k, (q, m) in enumerate(((1.0, w["mass_ratio"]), (-1.0, 1.0))):
+        spec = SpeciesSpec(charge=q, mass=m, vth=w["vth"], ppc=w["ppc"], drift_gamma=0.0, x0=0, x1=p.size_x)
+        a = species_arrays(p, spec, seed_offset=k)
+        o.add_species(q, m, w["vth"], a["ix"], a["iy"], a["dx"], a["dy"], a["px"], a["py"], a["pz"], a["psa"])
+        n += len(a["ix"])
+    o.prepare()
+    o.step(warmup)
+    if steps is None:
+        t0 = time.perf_counter()
+        o.step(1)
+        one = time.perf_counter() - t0
+        steps = max(1, int(seconds_target / max(one, 1e-3)))
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    sample = f"{CROP['size_x']}x{CROP['size_y']} crop, {w['ppc']} ppc/species, {n} particles, {steps} steps"
+    return n * steps / dt, orc.num_threads(), sample, dt
+
+
+def run_reference(args, w):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    # bounded sample: the crop is ~1/32 of the workload; each step is one loop iteration of it
+    rate, cores, sample, dt = oracle_crop_rate(w, 0, steps=args.steps, warmup=args.warmup)
+    line = {"metric": "particle-steps/s", "value": rate, "unit": "particle-steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": w["name"], "grid": [w["size_x"], w["size_y"]], "ppc_per_species": w["ppc"],
+                       "sample": sample},
+            "cpu_baseline": {"value": rate, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+                             "sample": sample + " (C++ restatement of the reference CPU path)"},
+            "e2e": {"value": rate, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU arm
+def e2e_run(w, steps, seed):
+    """Same metric through the public API from pinned host buffers: upload both
+    species, prepare, `steps` steps, read the saved fields and diagnostics back."""
+    import torch
+    from spectral_rs_b200 import Sim
+    from spectral_rs_b200.config import Config, Setup, Output, SpeciesSpec
+    from spectral_rs_b200.init import positions, draws, velocities
+    p = params(w, random_positions=True, seed=seed)
+    host = []
+    for k, (q, m) in enumerate(((1.0, w["mass_ratio"]), (-1.0, 1.0))):
+        rng = np.random.default_rng([seed, k])
+        ix, iy, dx, dy = positions(p.size_x, p.size_y, 0, w["ppc"], 0, p.size_x, True, rng)
+        n = len(ix)
+        arrs = {}
+        for name, src in (("ix", ix), ("iy", iy), ("dx", dx), ("dy", dy)):
+            t = torch.empty(n, dtype=torch.int64 if name in ("ix", "iy") else torch.float32, pin_memory=True)
+            t.numpy().view(src.dtype)[:] = src
+            arrs[name] = t.numpy().view(src.dtype)
+        del ix, iy, dx, dy
+        for name in ("px", "py", "pz", "psa"):
+            arrs[name] = torch.empty(n, dtype=torch.float32, pin_memory=True).numpy()
+        chunk = 1 << 25
+        for s0 in range(0, n, chunk):
+            s1 = min(n, s0 + chunk)
+            nrm, uni = draws(s1 - s0, rng)
+            px, py, pz, psa = velocities(nrm, uni, p.c, w["vth"], 0.0)
+            arrs["px"][s0:s1], arrs["py"][s0:s1], arrs["pz"][s0:s1], arrs["psa"][s0:s1] = px, py, pz, psa
+        host.append((q, m, arrs))
+    cfg = Config(p, Setup(steps), Output(False, False, 1, 1, 1, 1))
+    sim = Sim(cfg)
+    h2d = sum(a["ix"].nbytes + a["iy"].nbytes + 6 * a["dx"].nbytes for (_, _, a) in host)
+    t0 = time.perf_counter()
+    for q, m, a in host:
+        sim.add_species(q, m, w["vth"], a["ix"], a["iy"], a["dx"], a["dy"], a["px"], a["py"], a["pz"], a["psa"])
+    sim.prepare()
+    sim.step(steps)
+    out = [sim.flds.spatial(name, with_ghosts=False) for name in
+           ("Jx", "Jy", "Jz", "Ex", "Ey", "Ez", "Bx", "By", "Bz", "Dens")]
+    d = sim.diag()
+    dt = time.perf_counter() - t0
+    d2h = sum(o.nbytes for o in out) + d.nbytes
+    n = sum(len(a["ix"]) for (_, _, a) in host)
+    sim.close()
+    return {"value": n * steps / dt, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d / steps,
+            "d2h_bytes_per_step": d2h / steps, "wall_s": dt,
+            "scope": "host arrays -> spx_add_species x2 -> spx_prepare -> spx_step(K) -> 10 fields + diag to host"}
+
+
+def run_gpu(args, w):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    seed = args.seed + rank
+
+    sim = make_sim(w, "split", seed)
+    n_particles = sum(len(p) for p in sim.prtls)
+    cells = w["size_x"] * w["size_y"]
+    sim.prepare()
+    sim.step(args.warmup)
+    stream = torch.cuda.ExternalStream(sim.stream())
+    sim.set_timing(True)  # per-step CUDA events around each phase, on the library's stream
+    sampler = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    phases = sim.timing()  # [particles, fold, field update, step] summed over the steps
+    launches = sim.last_launch_count()
+    counters = sim.counters()
+    sim.set_timing(False)
+    diag = sim.diag()
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    sim.close()
+    del sim
+    value = n_particles * args.steps * world / (ms / 1e3)
+
+    peak, peak_kind = measured_peak()
+    kern_ms = float(phases[0]) / args.steps
+    alg_bytes = B_PER_PARTICLE * n_particles + B_PER_CELL * cells
+    achieved = alg_bytes / (kern_ms / 1e3) / 1e9
+    traffic = traffic_per_launch(n_particles, cells)
+
+    plain = None
+    if not args.no_plain and rank == 0:
+        ps = make_sim(w, "plain", seed)
+        ps.prepare()
+        ps.step(1)
+        stream_p = torch.cuda.ExternalStream(ps.stream())
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream_p)
+        ps.step(args.plain_steps)
+        a1.record(stream_p)
+        a1.synchronize()
+        pms = a0.elapsed_time(a1)
+        ps.close()
+        plain = {"value": n_particles * args.plain_steps / (pms / 1e3), "unit": "particle-steps/s",
+                 "ms_per_step": pms / args.plain_steps, "steps": args.plain_steps,
+                 "path": "plain FP32 (global x = ix + dx, per-phase kernels, global atomics, no sort)"}
+
+    cpu = None
+    e2e = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, cores, sample, _ = oracle_crop_rate(w, args.cpu_seconds)
+        cpu = {"value": rate, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+               "sample": sample + " (C++ restatement of the reference CPU path, OpenMP push/FFT, serial deposit)"}
+    if rank == 0 and not args.no_e2e:
+        e2e = e2e_run(w, args.steps, seed)
+
+    if rank == 0:
+        line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded device init)",
+                "config": {"workload": w["name"], "grid": [w["size_x"], w["size_y"]], "ppc_per_species": w["ppc"],
+                           "particles_per_gpu": n_particles, "mass_ratio": w["mass_ratio"], "vth": w["vth"],
+                           "n_pass": w["n_pass"], "c": w["c"], "dt": w["dt"], "path": "split",
+                           "parallelism": "replicas" if world > 1 else "single",
+                           "l2": "inputs larger than L2 (13 GB particle state)"},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                             "kernel": "k_slot<push,move> (fused push + move + deposit)",
+                             "kernel_ms": kern_ms, "alg_bytes_per_launch": alg_bytes},
+                "phase_ms_per_step": {"particles": float(phases[0]) / args.steps,
+                                      "fold": float(phases[1]) / args.steps,
+                                      "fields": float(phases[2]) / args.steps,
+                                      "step": float(phases[3]) / args.steps},
+                "plain_fp32": plain, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+                "gpu_launches": launches, "layout": counters,
+                "diag": {"field_energy_E": diag[0], "field_energy_B": diag[1], "kinetic": diag[2]}}
+        if plain:
+            line["split_vs_plain"] = value / world / plain["value"]
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--small", action="store_true", help="1/16 of the workload (quick checks)")
+    args = ap.parse_args()
+    w = dict(WORKLOAD)
+    if args.small:
+        w.update(size_x=1024, size_y=256, name="thermal_ep_1024x256_ppc64")
+    if args.impl == "reference":
+        run_reference(args, w)
+    else:
+        run_gpu(args, w)
+
+
+if __name__ == "__main__":
+    main()

@@ -174,11 +174,21 @@ SPX_API int spx_field_op(uint64_t size_x, uint64_t size_y, int32_t op, uint32_t 
  * Power-of-two sizes only. */
 SPX_API int spx_fft2d(uint64_t size_x, uint64_t size_y, int32_t inverse, float* data_complex);
 
-/* Time of the last spx_step call's kernels on the context stream, in ms,
- * split as [0] push+move+deposit, [1] fold+filter, [2] spectral solve,
- * [3] whole step (CUDA events; filled only when timing is enabled). */
+/* Time of the last spx_step call's work on the context stream, in ms, summed
+ * over its steps: [0] particle phase (fused push + move + deposit and slot
+ * relocation), [1] ghost fold, [2] Flds::update (filter + spectral solve),
+ * [3] whole step.  CUDA events; filled only while timing is enabled (then the
+ * steps run uncaptured, one event set per step). */
 SPX_API int spx_set_timing(spx_ctx* ctx, int32_t enable);
 SPX_API int spx_get_timing(spx_ctx* ctx, float* out4);
+/* The context's CUDA stream (a cudaStream_t), so callers can order their own
+ * work and timing events with the library's. */
+SPX_API void* spx_get_stream(const spx_ctx* ctx);
+/* Layout and overflow counters: out8[0] slot repacks so far, [1] particles in
+ * overflow lists at the last check, [2] largest cell occupancy at the last
+ * check, [3] slot capacity K of species 0, [4] tiles, [5] cells per tile,
+ * [6] kernel launches of the last spx_step call, [7] device bytes held. */
+SPX_API int spx_get_counters(const spx_ctx* ctx, uint64_t* out8);
 /* Number of kernel launches issued by the last spx_step call. */
 SPX_API uint64_t spx_last_launch_count(const spx_ctx* ctx);
 

@@ -971,7 +971,7 @@ template <typename T>
 static void init_velocities(uint64_t n, T c, T vth, T gamma_inj, T beta_sign, const T* normals,
                             const T* uniforms, T* px, T* py, T* pz, T* psa) {
   const T csqinv = T(1.) / (c * c);
-  const T beta_inj = beta_sign * std::sqrt(T(1.) - T(1) / (gamma_inj * gamma_inj));
+  const T beta_inj = gamma_inj > T(1) ? beta_sign * std::sqrt(T(1.) - T(1) / (gamma_inj * gamma_inj)) : T(0);
   for (uint64_t i = 0; i < n; ++i) {
     px[i] = normals[3 * i + 0];
     px[i] *= vth * c;
@@ -981,6 +981,7 @@ static void init_velocities(uint64_t n, T c, T vth, T gamma_inj, T beta_sign, co
     pz[i] *= vth * c;
     psa[i] = T(1.0) + (px[i] * px[i] + py[i] * py[i] + pz[i] * pz[i]) * csqinv;
     psa[i] = std::sqrt(psa[i]);
+    if (!(gamma_inj > T(1))) continue;  // additive: no drift at all (the reference requires gamma_inj > 1)
     T ux = px[i] / c;
     T r = uniforms[i];
     if (-beta_inj * ux > r * psa[i]) ux *= T(-1.);

@@ -31,10 +31,11 @@ struct spx_ctx {
   bool use_graphs = true;
   // timing ring
   bool timing = false;
-  std::vector<cudaEvent_t> ev;  // 4 per step
+  std::vector<cudaEvent_t> ev;  // 5 per step
   int ev_steps = 0;
   float last_timing[4] = {0, 0, 0, 0};
   uint64_t last_launches = 0;
+  uint64_t repacks = 0, last_overflow = 0, last_max_occ = 0;
 };
 
 static std::string g_create_err;
@@ -226,7 +227,9 @@ static int choose_K(spx_ctx* c, uint64_t n) {
   SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
   if (c->prm.slot_capacity < 0) return std::max((int)mx, -c->prm.slot_capacity);  // exact K (tests)
   const double mean = (double)n / (double)c->pg.ncells();
-  int K = (int)std::ceil(std::max(1.5 * mx, mean + 10.0 * std::sqrt(mean))) + 16;
+  // room for Poisson-like fluctuations of the occupancy; the overflow list and
+  // repack handle anything beyond
+  int K = (int)std::ceil(std::max(1.25 * mx, mean + 8.0 * std::sqrt(mean))) + 8;
   if (c->prm.slot_capacity > 0) K = std::max(K, c->prm.slot_capacity);
   return K;
 }
@@ -578,10 +581,12 @@ void pack_cells(uint64_t n, const uint32_t* ix, const uint32_t* iy, uint32_t* ce
   if (n) k_pack_cells<<<148 * 8, 256, 0, st>>>(n, ix, iy, cell);
 }
 
-// Overflow handling: if a species parked particles in its overflow list or a
-// cell is close to its capacity, rebuild its slots with a larger K.
+// Overflow handling: if a species parked particles in its overflow list,
+// rebuild its slots with a larger K (the list keeps results exact meanwhile).
 static void maybe_repack(spx_ctx* c) {
   if (c->plain) return;
+  c->last_overflow = 0;
+  c->last_max_occ = 0;
   for (auto& s : c->species) {
     SlotSpecies& S = s.slot;
     uint32_t h[2] = {0, 0};
@@ -590,7 +595,10 @@ static void maybe_repack(spx_ctx* c) {
     SPX_CUDA_TRY(cudaMemcpyAsync(&h[0], c->d_u32, 4, cudaMemcpyDeviceToHost, c->st));
     SPX_CUDA_TRY(cudaMemcpyAsync(&h[1], S.ocount + S.cur, 4, cudaMemcpyDeviceToHost, c->st));
     SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
-    if (h[1] == 0 && h[0] + 8 < (uint32_t)S.K) continue;
+    c->last_overflow += h[1];
+    c->last_max_occ = std::max<uint64_t>(c->last_max_occ, h[0]);
+    if (h[1] == 0) continue;  // the overflow list is in use: grow the capacity
+    ++c->repacks;
     // unpack (reference order) and pack again with a larger capacity
     const uint64_t n = s.n;
     Staging st;
@@ -618,10 +626,10 @@ static void maybe_repack(spx_ctx* c) {
 static int step_body(spx_ctx* c, bool timed, int slot) {
   int launches = 0;
   const int ns = (int)c->species.size();
-  cudaEvent_t* e = timed ? &c->ev[4 * slot] : nullptr;
+  cudaEvent_t* e = timed ? &c->ev[5 * slot] : nullptr;
+  if (e) SPX_CUDA_TRY(cudaEventRecord(e[4], c->st));
+  zero_sources(c);  // memsets, not kernels
   if (e) SPX_CUDA_TRY(cudaEventRecord(e[0], c->st));
-  zero_sources(c);
-  launches += 5;
   if (c->plain) {
     launches += run_move(c, 0, ns, false);
   } else if (c->pending_push) {
@@ -654,9 +662,9 @@ extern "C" int spx_step(spx_ctx* c, uint32_t n) {
   SPX_GUARD(c, {
     uint64_t launches = 0;
     if (c->timing) {
-      if ((int)c->ev.size() < 4 * (int)n) {
+      if ((int)c->ev.size() < 5 * (int)n) {
         for (auto ev : c->ev) cudaEventDestroy(ev);
-        c->ev.assign(4 * n, nullptr);
+        c->ev.assign(5 * n, nullptr);
         for (auto& ev : c->ev) SPX_CUDA_TRY(cudaEventCreate(&ev));
       }
       for (uint32_t i = 0; i < n; ++i) launches += step_body(c, true, (int)i);
@@ -701,10 +709,10 @@ extern "C" int spx_step(spx_ctx* c, uint32_t n) {
       float acc[4] = {0, 0, 0, 0};
       for (int i = 0; i < c->ev_steps; ++i) {
         float a, b, d, t;
-        SPX_CUDA_TRY(cudaEventElapsedTime(&a, c->ev[4 * i], c->ev[4 * i + 1]));
-        SPX_CUDA_TRY(cudaEventElapsedTime(&b, c->ev[4 * i + 1], c->ev[4 * i + 2]));
-        SPX_CUDA_TRY(cudaEventElapsedTime(&d, c->ev[4 * i + 2], c->ev[4 * i + 3]));
-        SPX_CUDA_TRY(cudaEventElapsedTime(&t, c->ev[4 * i], c->ev[4 * i + 3]));
+        SPX_CUDA_TRY(cudaEventElapsedTime(&a, c->ev[5 * i], c->ev[5 * i + 1]));
+        SPX_CUDA_TRY(cudaEventElapsedTime(&b, c->ev[5 * i + 1], c->ev[5 * i + 2]));
+        SPX_CUDA_TRY(cudaEventElapsedTime(&d, c->ev[5 * i + 2], c->ev[5 * i + 3]));
+        SPX_CUDA_TRY(cudaEventElapsedTime(&t, c->ev[5 * i + 4], c->ev[5 * i + 3]));
         acc[0] += a;
         acc[1] += b;
         acc[2] += d;
@@ -728,6 +736,21 @@ extern "C" int spx_get_timing(spx_ctx* c, float* out4) {
   return SPX_OK;
 }
 extern "C" uint64_t spx_last_launch_count(const spx_ctx* c) { return c ? c->last_launches : 0; }
+extern "C" void* spx_get_stream(const spx_ctx* c) { return c ? (void*)c->st : nullptr; }
+extern "C" int spx_get_counters(const spx_ctx* c, uint64_t* out8) {
+  if (!c || !out8) return SPX_ERR_ARG;
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  out8[0] = c->repacks;
+  out8[1] = c->last_overflow;
+  out8[2] = c->last_max_occ;
+  out8[3] = c->species.empty() ? 0 : (uint64_t)c->species[0].slot.K;
+  out8[4] = (uint64_t)c->pg.ntiles();
+  out8[5] = (uint64_t)c->pg.TC();
+  out8[6] = c->last_launches;
+  out8[7] = (uint64_t)(total_b - free_b);
+  return SPX_OK;
+}
 
 // ---------------------------------------------------------------- field access
 extern "C" int spx_get_field(spx_ctx* c, int32_t field, int32_t with_ghosts, float* out) {

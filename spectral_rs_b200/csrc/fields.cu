@@ -177,7 +177,7 @@ struct RowArgs {
 };
 
 template <int IN, int OUT, bool INV>
-__global__ void __launch_bounds__(1024) k_rows(RowArgs a, Grid g, const float2* __restrict__ tw) {
+__global__ void __launch_bounds__(1024) k_rows(const __grid_constant__ RowArgs a, Grid g, const float2* __restrict__ tw) {
   extern __shared__ float2 sm[];
   const int f = blockIdx.y;
   const int logN = g.log2nx, N = g.nx;
@@ -239,7 +239,7 @@ struct ColArgs {
   float2* data[8];
 };
 template <bool INV>
-__global__ void __launch_bounds__(1024) k_cols(ColArgs a, Grid g, const float2* __restrict__ tw) {
+__global__ void __launch_bounds__(1024) k_cols(const __grid_constant__ ColArgs a, Grid g, const float2* __restrict__ tw) {
   extern __shared__ float2 sm[];
   const int f = blockIdx.y;
   const int logN = g.log2ny, N = g.ny;
@@ -331,7 +331,7 @@ struct ConstFieldList {
 
 // Field::deposit_ghosts, one thread per interior cell of the frame; additions in
 // the reference's order (rows, columns, corners), so results are bit-exact.
-__global__ void k_fold(FieldList L, Grid g) {
+__global__ void k_fold(const __grid_constant__ FieldList L, Grid g) {
   float* F = L.f[blockIdx.y];
   const int nx = g.nx, ny = g.ny, W = g.W;
   const int nper = 2 * nx + 2 * (ny - 2);
@@ -357,7 +357,7 @@ __global__ void k_fold(FieldList L, Grid g) {
 __device__ __forceinline__ int wrap_row(int r, int n) { return r == 0 ? n : (r == n + 1 ? 1 : r); }
 
 // Field::update_ghosts: every ghost cell <- its periodic interior image.
-__global__ void k_update_ghosts(FieldList L, Grid g) {
+__global__ void k_update_ghosts(const __grid_constant__ FieldList L, Grid g) {
   float* F = L.f[blockIdx.y];
   const int nx = g.nx, ny = g.ny, W = g.W;
   const int nper = 2 * (nx + 2) + 2 * ny;
@@ -376,7 +376,7 @@ __global__ void k_update_ghosts(FieldList L, Grid g) {
 // hold whatever the input had, as in the reference); ghost cells receive the
 // filtered value of their periodic image (the update_ghosts that follows in
 // the reference).  Reference summation order, no contraction: bit-exact.
-__global__ void k_filter(ConstFieldList S, FieldList D, Grid g) {
+__global__ void k_filter(const __grid_constant__ ConstFieldList S, const __grid_constant__ FieldList D, Grid g) {
   const float* in = S.f[blockIdx.z];
   float* out = D.f[blockIdx.z];
   const int W = g.W;
@@ -508,7 +508,6 @@ int field_update(FieldBuffers& fb, cudaStream_t st) {
   if (fb.n_pass & 1) {  // keep the filtered result in the field's own buffer
     for (int i = 0; i < 4; ++i)
       SPX_CUDA_TRY(cudaMemcpyAsync(oth[i], cur[i], g.spatial_size() * sizeof(float), cudaMemcpyDeviceToDevice, st));
-    launches += 4;
   }
   // 2. copy_to_spectral (+ dsty/dens) fused with the row FFTs (mod.rs:66-85, 101-103, 122-124)
   {

@@ -207,14 +207,26 @@ __device__ __forceinline__ void relocate(const StepArgs& a, const SpeciesArgs& S
   }
 }
 
+// Shared-memory pitch of the E/B window: the lanes of a warp cover 32/TX tile
+// rows; a pitch congruent to TX modulo 32 puts consecutive rows on disjoint
+// banks, so every gather load of a warp is conflict-free.
+__host__ __device__ inline int eb_pitch(int TX) {
+  if (TX >= 32) return TX + 2;
+  int p = TX;
+  while (p < TX + 2) p += 32;
+  return p;
+}
+
 // One CTA per tile, one thread per cell.  Every particle a thread processes
-// starts in the thread's cell, so the 3x3 E/B neighbourhood (54 values) lives
-// in registers for the whole tile pass and deposits that stay in the cell's
-// stencil accumulate in registers; only particles whose half- or full-step
-// cell differs use shared-memory atomics.
+// starts in the thread's cell: the E/B window of the tile (+1 cell halo) is
+// staged once in shared memory and gathered with conflict-free loads, and
+// deposits that stay in the cell's 3x3 stencil accumulate in registers (36
+// accumulators); only particles whose half- or full-step cell differs use
+// shared-memory atomics.  The next particle's state is loaded while the
+// current one is processed.
 template <bool PUSH, bool MOVE>
-__global__ void __launch_bounds__(256) k_slot(const __grid_constant__ StepArgs a) {
-  extern __shared__ float win[];
+__global__ void __launch_bounds__(256, 2) k_slot(const __grid_constant__ StepArgs a) {
+  extern __shared__ float smem[];
   const int TC = a.TX * a.TY;
   const int tile = blockIdx.x;
   const int tx = tile % a.NTX, ty = tile / a.NTX;
@@ -222,27 +234,31 @@ __global__ void __launch_bounds__(256) k_slot(const __grid_constant__ StepArgs a
   const int lx = c & (a.TX - 1), ly = c >> a.logTX;
   const int ox = tx * a.TX + lx + 1, oy = ty * a.TY + ly + 1;  // owner cell (reference coords)
   const int W = a.g.W, nx = a.g.nx, ny = a.g.ny;
+  // deposit window: tile + 2 cells
   const int WX = a.TX + 4, WY = a.TY + 4, WN = WX * WY;
-  const int wx0 = tx * a.TX + 1 - 2, wy0 = ty * a.TY + 1 - 2;  // window origin
+  const int wx0 = tx * a.TX + 1 - 2, wy0 = ty * a.TY + 1 - 2;
+  float* win = smem;
   float* wjx = win;
   float* wjy = win + WN;
   float* wjz = win + 2 * WN;
   float* wrho = win + 3 * WN;
   float* wdens = win + 4 * WN;
-  if (MOVE) {
+  // E/B window: tile + 1 cell, 6 planes
+  const int PE = eb_pitch(a.TX), EY = a.TY + 2, EN = PE * EY;
+  float* ebw = smem + (MOVE ? 5 * WN : 0);
+  if (MOVE)
     for (int i = c; i < 5 * WN; i += TC) win[i] = 0.f;
-    __syncthreads();
-  }
-  float eb[6][9];
   if (PUSH) {
     const float* src[6] = {a.f.E[0], a.f.E[1], a.f.E[2], a.f.B[0], a.f.B[1], a.f.B[2]};
-#pragma unroll
-    for (int f = 0; f < 6; ++f)
-#pragma unroll
-      for (int r = 0; r < 3; ++r)
-#pragma unroll
-        for (int q = 0; q < 3; ++q) eb[f][r * 3 + q] = __ldg(src[f] + (size_t)(oy - 1 + r) * W + (ox - 1 + q));
+    const int EX = a.TX + 2;
+    for (int i = c; i < 6 * EY * EX; i += TC) {
+      const int f = i / (EY * EX), k = i - f * (EY * EX);
+      const int r = k / EX, q = k - r * EX;
+      ebw[f * EN + r * PE + q] = __ldg(src[f] + (size_t)(ty * a.TY + r) * W + (tx * a.TX + q));
+    }
   }
+  __syncthreads();
+  const float* eb = ebw + ly * PE + lx;  // top-left of this cell's 3x3 neighbourhood
   float accJ[3][9];
 #pragma unroll
   for (int k = 0; k < 9; ++k) accJ[0][k] = accJ[1][k] = accJ[2][k] = 0.f;
@@ -252,18 +268,49 @@ __global__ void __launch_bounds__(256) k_slot(const __grid_constant__ StepArgs a
 
   for (int s = 0; s < a.ns; ++s) {
     const SpeciesArgs& S = a.sp[s];
-    const size_t base = (size_t)tile * S.K * TC + c;
+    const float* __restrict__ rdx = S.dx;
+    const float* __restrict__ rdy = S.dy;
+    const float* __restrict__ rpx = S.px;
+    const float* __restrict__ rpy = S.py;
+    const float* __restrict__ rpz = S.pz;
+    const uint32_t* __restrict__ rtag = S.tag;
+    const int K = S.K;
+    const size_t base = (size_t)tile * K * TC + c;
     const int nlow = (int)S.nlow[gc], ntop = (int)S.ntop[gc];
     const int total = nlow + ntop;
-    const float q = S.charge;
+    const float q = S.charge, beta = S.beta, alpha = S.alpha;
     float accD[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) accD[k] = 0.f;
     int wcur = 0;
+    // software pipeline: state of particle n is loaded during particle n-1
+    float ndx = 0.f, ndy = 0.f, npx = 0.f, npy = 0.f, npz = 0.f;
+    uint32_t ntag = 0;
+    size_t nidx = base;
+    if (total > 0) {
+      nidx = base + (size_t)(nlow > 0 ? 0 : K - 1) * TC;
+      ndx = rdx[nidx];
+      ndy = rdy[nidx];
+      npx = rpx[nidx];
+      npy = rpy[nidx];
+      npz = rpz[nidx];
+      if (MOVE) ntag = rtag[nidx];
+    }
     for (int n = 0; n < total; ++n) {
-      const int slot = n < nlow ? n : S.K - 1 - (n - nlow);
-      const size_t idx = base + (size_t)slot * TC;
-      float dx = S.dx[idx], dy = S.dy[idx], px = S.px[idx], py = S.py[idx], pz = S.pz[idx];
+      const size_t idx = nidx;
+      float dx = ndx, dy = ndy, px = npx, py = npy, pz = npz;
+      const uint32_t tag = ntag;
+      if (n + 1 < total) {
+        const int m = n + 1;
+        const int slot = m < nlow ? m : K - 1 - (m - nlow);
+        nidx = base + (size_t)slot * TC;
+        ndx = rdx[nidx];
+        ndy = rdy[nidx];
+        npx = rpx[nidx];
+        npy = rpy[nidx];
+        npz = rpz[nidx];
+        if (MOVE) ntag = rtag[nidx];
+      }
       float psa;
       if (PUSH) {
         float w[9];
@@ -271,12 +318,19 @@ __global__ void __launch_bounds__(256) k_slot(const __grid_constant__ StepArgs a
         float gth[6];
 #pragma unroll
         for (int f = 0; f < 6; ++f) {
-          float t = w[0] * eb[f][0];
-#pragma unroll
-          for (int k = 1; k < 9; ++k) t += w[k] * eb[f][k];
+          const float* e = eb + f * EN;
+          float t = w[0] * e[0];
+          t += w[1] * e[1];
+          t += w[2] * e[2];
+          t += w[3] * e[PE];
+          t += w[4] * e[PE + 1];
+          t += w[5] * e[PE + 2];
+          t += w[6] * e[2 * PE];
+          t += w[7] * e[2 * PE + 1];
+          t += w[8] * e[2 * PE + 2];
           gth[f] = t;
         }
-        boris(gth, S.beta, S.alpha, csqinv, px, py, pz, psa);
+        boris(gth, beta, alpha, csqinv, px, py, pz, psa);
       } else {
         psa = gamma_of(px, py, pz, csqinv);
       }
@@ -286,7 +340,6 @@ __global__ void __launch_bounds__(256) k_slot(const __grid_constant__ StepArgs a
         S.rpz[idx] = pz;
         continue;
       }
-      const uint32_t tag = S.tag[idx];
       const float inv = 1.0f / psa;
       const float c1 = half_dt * inv;
       int ix = ox, iy = oy;
@@ -526,11 +579,11 @@ int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysPar
       const int w = S.cur ^ 1;
       SPX_CUDA_TRY(cudaMemsetAsync(S.ntop[w], 0, pg.ncells() * sizeof(uint32_t), st));
       SPX_CUDA_TRY(cudaMemsetAsync(S.ocount + w, 0, sizeof(uint32_t), st));
-      launches += 2;
     }
   }
   const int TC = pg.TC();
-  const size_t smem = move ? 5 * (size_t)(pg.TX + 4) * (pg.TY + 4) * sizeof(float) : 0;
+  const size_t smem = ((move ? 5 * (size_t)(pg.TX + 4) * (pg.TY + 4) : 0) +
+                       (push ? 6 * (size_t)eb_pitch(pg.TX) * (pg.TY + 2) : 0)) * sizeof(float);
   if (push && move)
     k_slot<true, true><<<pg.ntiles(), TC, smem, st>>>(a);
   else if (push)

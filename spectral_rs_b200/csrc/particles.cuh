@@ -100,7 +100,7 @@ void slot_unpack(const Species& s, const ParticleGeom& pg, uint32_t* ix, uint32_
                  float* px, float* py, float* pz, float* psa, float csqinv, cudaStream_t st);
 // The fused particle kernel over species [s0, s1): PUSH = Boris push
 // (src/prtls.rs:262-443), MOVE = move_and_deposit (src/lib.rs:478-489) with
-// relocation.  Returns the number of launches.
+// relocation.  Returns the number of kernel launches (memsets not counted).
 int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysParams& pp, const FieldPtrs& fp,
               bool push, bool move, int* derr, cudaStream_t st);
 // Maximum cell occupancy (low + top + arrivals) after the last step, for repack decisions.

@@ -139,6 +139,18 @@ class Sim:
     def last_launch_count(self):
         return int(self.lib.spx_last_launch_count(self._ctx))
 
+    def counters(self):
+        """dict of slot-layout counters (repacks, overflow, occupancy, K, tiles, launches, device bytes)."""
+        out = np.zeros(8, dtype=np.uint64)
+        self._chk(self.lib.spx_get_counters(self._ctx, _lib.ptr(out)))
+        keys = ("repacks", "overflow", "max_occupancy", "slot_capacity", "tiles", "cells_per_tile",
+                "launches", "device_bytes")
+        return {k: int(v) for k, v in zip(keys, out)}
+
+    def stream(self):
+        """The context's cudaStream_t as an integer handle (torch.cuda.ExternalStream accepts it)."""
+        return int(self.lib.spx_get_stream(self._ctx) or 0)
+
 
 class Flds:
     """Device-resident fields with the reference's names (src/flds/mod.rs:15-37)."""
