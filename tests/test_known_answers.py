@@ -113,14 +113,23 @@ def test_walls_conserve_momentum_magnitude():
 
 
 def _light_wave(sim, p, m, steps):
+    """Ey = cos(k x) in vacuum, advanced by Flds::update; `sim` is the oracle or a GPU Sim."""
     x = np.arange(p.size_x + 2) - 1
     k = 2 * np.pi * m / p.size_x
     ey = np.tile(np.cos(k * x), (p.size_y + 2, 1))
-    sim.set_spatial("Ey", ey.astype(sim.dtype if hasattr(sim, "dtype") else np.float32))
+    gpu = hasattr(sim, "flds")
+    if gpu:
+        sim.flds.set_spatial("Ey", ey.astype(np.float32))
+    else:
+        sim.set_spatial("Ey", ey)
     hist = []
     for _ in range(steps):
-        sim.fields_update() if hasattr(sim, "fields_update") else sim.flds.update()
-        f = sim.spatial("Ey") if hasattr(sim, "spatial") else sim.flds.spatial("Ey")
+        if gpu:
+            sim.flds.update()
+            f = sim.flds.spatial("Ey")
+        else:
+            sim.fields_update()
+            f = sim.spatial("Ey")
         hist.append(f[1:-1, 1:-1].astype(np.float64))
     return k, hist
 
