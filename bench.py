@@ -176,6 +176,23 @@ def run_reference(args, w):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- rank plumbing
+def rank_seed(base_seed, rank):
+    """Each replica draws its own plasma."""
+    return base_seed + rank
+
+
+def max_over_ranks(ms, device="cpu"):
+    """The timed region's length is the slowest rank's (every rank calls this once)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(ms)
+    t = torch.tensor([float(ms)], device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ---------------------------------------------------------------- GPU arm
 def e2e_run(w, steps, seed):
     """Same metric through the public API from pinned host buffers: upload both
@@ -236,7 +253,7 @@ def run_gpu(args, w):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    seed = args.seed + rank
+    seed = rank_seed(args.seed, rank)
 
     sim = make_sim(w, "split", seed)
     n_particles = sum(len(p) for p in sim.prtls)
@@ -264,9 +281,7 @@ def run_gpu(args, w):
     sim.set_timing(False)
     diag = sim.diag()
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, device="cuda")
         dist.barrier()
     sim.close()
     del sim
