@@ -28,7 +28,7 @@ EXPORTS = [
     "spx_boris_push", "spx_prepare", "spx_step", "spx_flush", "spx_synchronize",
     "spx_get_field", "spx_set_field", "spx_get_bwrk", "spx_set_bwrk", "spx_diag",
     "spx_field_op", "spx_fft2d", "spx_set_timing", "spx_get_timing", "spx_last_launch_count",
-    "spx_get_stream", "spx_get_counters",
+    "spx_get_stream", "spx_get_counters", "spx_filter_noalloc", "spx_noalloc_last_error",
 ]
 
 
@@ -100,6 +100,8 @@ def load():
         "spx_last_launch_count": (ctypes.c_uint64, [P]),
         "spx_get_stream": (ctypes.c_void_p, [P]),
         "spx_get_counters": (ctypes.c_int, [P, P]),
+        "spx_filter_noalloc": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, P, P, P]),
+        "spx_noalloc_last_error": (ctypes.c_char_p, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
