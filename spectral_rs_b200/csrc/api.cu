@@ -145,6 +145,7 @@ extern "C" int spx_create(const spx_params* p, spx_ctx** out) {
     SPX_CUDA_TRY(cudaMalloc(&c->d_diag, 8 * sizeof(double)));
     SPX_CUDA_TRY(cudaMalloc(&c->d_u32, 8 * sizeof(uint32_t)));
     SPX_CUDA_TRY(cudaMalloc(&c->d_counts, c->pg.ncells() * sizeof(uint32_t)));
+    slot_set_kernel_attributes();
   } catch (const spx::Error& e) {
     spx_destroy(c);
     return fail(nullptr, e.code, e.msg);
@@ -215,12 +216,11 @@ static int choose_K(spx_ctx* c, uint64_t n) {
   SPX_CUDA_TRY(cudaMemsetAsync(c->d_u32, 0, sizeof(uint32_t), c->st));
   // max over the counts array
   Species tmp;
-  tmp.slot.nlow[0] = c->d_counts;
-  tmp.slot.cur = 0;
+  tmp.slot.nlow = c->d_counts;
   uint32_t* zeros = nullptr;
   SPX_CUDA_TRY(cudaMallocAsync(&zeros, c->pg.ncells() * sizeof(uint32_t), c->st));
   SPX_CUDA_TRY(cudaMemsetAsync(zeros, 0, c->pg.ncells() * sizeof(uint32_t), c->st));
-  tmp.slot.ntop[0] = zeros;
+  tmp.slot.top = zeros;
   slot_max_occupancy(tmp, c->pg, c->d_u32, c->st);
   SPX_CUDA_TRY(cudaMemcpyAsync(&mx, c->d_u32, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
   SPX_CUDA_TRY(cudaFreeAsync(zeros, c->st));
@@ -593,7 +593,7 @@ static void maybe_repack(spx_ctx* c) {
     SPX_CUDA_TRY(cudaMemsetAsync(c->d_u32, 0, sizeof(uint32_t), c->st));
     slot_max_occupancy(s, c->pg, c->d_u32, c->st);
     SPX_CUDA_TRY(cudaMemcpyAsync(&h[0], c->d_u32, 4, cudaMemcpyDeviceToHost, c->st));
-    SPX_CUDA_TRY(cudaMemcpyAsync(&h[1], S.ocount + S.cur, 4, cudaMemcpyDeviceToHost, c->st));
+    SPX_CUDA_TRY(cudaMemcpyAsync(&h[1], S.ocount + S.ocur, 4, cudaMemcpyDeviceToHost, c->st));
     SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
     c->last_overflow += h[1];
     c->last_max_occ = std::max<uint64_t>(c->last_max_occ, h[0]);
@@ -652,7 +652,11 @@ static int step_body(spx_ctx* c, bool timed, int slot) {
 
 static uint32_t parity_key(spx_ctx* c) {
   uint32_t k = c->pending_push ? 1u : 0u;
-  for (size_t i = 0; i < c->species.size(); ++i) k |= (uint32_t)c->species[i].slot.cur << (i + 1);
+  for (size_t i = 0; i < c->species.size(); ++i) {
+    const SlotSpecies& S = c->species[i].slot;
+    k |= (uint32_t)S.ocur << (2 * i + 1);
+    k |= (uint32_t)(S.moves_since_compact == S.compact_every - 1) << (2 * i + 2);
+  }
   return k;
 }
 
@@ -682,8 +686,10 @@ extern "C" int spx_step(spx_ctx* c, uint32_t n) {
         const uint32_t key = parity_key(c);
         auto it = c->graphs.find(key);
         if (it == c->graphs.end()) {
-          std::vector<int> cur_before(c->species.size());
-          for (size_t s = 0; s < c->species.size(); ++s) cur_before[s] = c->species[s].slot.cur;
+          // capturing records the work without running it: keep the host-side
+          // slot state as it was, then replay the graph like a cached one
+          std::vector<SlotSpecies> before;
+          for (auto& sp : c->species) before.push_back(sp.slot);
           cudaGraph_t gr;
           SPX_CUDA_TRY(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
           const int l = step_body(c, false, 0);
@@ -691,15 +697,17 @@ extern "C" int spx_step(spx_ctx* c, uint32_t n) {
           cudaGraphExec_t ex;
           SPX_CUDA_TRY(cudaGraphInstantiate(&ex, gr, 0));
           SPX_CUDA_TRY(cudaGraphDestroy(gr));
-          // capturing recorded the work without running it: undo the host-side
-          // parity flips, then execute
-          for (size_t s = 0; s < c->species.size(); ++s) c->species[s].slot.cur = cur_before[s];
+          for (size_t s = 0; s < c->species.size(); ++s) c->species[s].slot = before[s];
           it = c->graphs.emplace(key, ex).first;
           launches += l - 1;
         }
         SPX_CUDA_TRY(cudaGraphLaunch(it->second, c->st));
         if (!c->plain)
-          for (size_t s = 0; s < c->species.size(); ++s) c->species[s].slot.cur ^= 1;
+          for (auto& sp : c->species) {  // what slot_step does to the host-side state
+            SlotSpecies& S = sp.slot;
+            S.ocur ^= 1;
+            if (++S.moves_since_compact >= S.compact_every) S.moves_since_compact = 0;
+          }
         launches += 1;
       }
     }

@@ -116,21 +116,19 @@ __device__ __forceinline__ void apply_bc(const PhysParams& p, int nx, int ny, in
 }
 
 // ---------------------------------------------------------------- split path kernel
+// Slot of a particle that left its cell: dx holds this NaN bit pattern.
+constexpr uint32_t HOLE_BITS = 0xFFFFFFFFu;
+__device__ __forceinline__ bool is_hole(float dx) { return __float_as_uint(dx) == HOLE_BITS; }
+
 struct SpeciesArgs {
-  // read buffer
-  const float *dx, *dy, *px, *py, *pz;
-  const uint32_t* tag;
-  const uint32_t *nlow, *ntop;
-  float *rpx, *rpy, *rpz;  // in-place momentum writes (push-only mode)
-  // write buffer
-  float *wdx, *wdy, *wpx, *wpy, *wpz;
-  uint32_t* wtag;
-  uint32_t *wnlow, *wntop;
+  float *dx, *dy, *px, *py, *pz;
+  uint32_t* tag;
+  const uint32_t *nlow, *top;  // read-only during a step
+  uint32_t* arr;               // arrivals of this step (atomic)
   // overflow lists: read (r*) and write (w*)
   const uint32_t* rocell;
-  const float *rodx, *rody, *ropx, *ropy, *ropz;
+  float *rodx, *rody, *ropx, *ropy, *ropz;
   const uint32_t* rotag;
-  float *ropx_w, *ropy_w, *ropz_w;
   uint32_t* wocell;
   float *wodx, *wody, *wopx, *wopy, *wopz;
   uint32_t* wotag;
@@ -171,8 +169,10 @@ __device__ __forceinline__ void dep9(float* win, int WX, int WY, int wx0, int wy
   }
 }
 
-// Append a particle that left its cell to the destination cell's top slots of
-// the write buffer (or to the overflow list).
+// Append a particle that left its cell to the destination cell: slot
+// K-1-(top+i) below the destination's committed top range, i from the
+// arrivals counter; the bound K - nlow - top keeps it clear of every slot the
+// destination's owner reads or writes this step.  No room: the overflow list.
 __device__ __forceinline__ void relocate(const StepArgs& a, const SpeciesArgs& S, int ix, int iy, float dx, float dy,
                                          float px, float py, float pz, uint32_t tag) {
   const int TC = a.TX * a.TY;
@@ -180,18 +180,19 @@ __device__ __forceinline__ void relocate(const StepArgs& a, const SpeciesArgs& S
   const int dc = (((iy - 1) & (a.TY - 1)) << a.logTX) | ((ix - 1) & (a.TX - 1));
   const size_t dtile = (size_t)dty * a.NTX + dtx;
   const size_t dgc = dtile * TC + dc;
-  const int limit = S.K - (int)(S.nlow[dgc] + S.ntop[dgc]);
-  const int i = (int)atomicAdd(&S.wntop[dgc], 1u);
+  const int top = (int)S.top[dgc];
+  const int limit = S.K - (int)S.nlow[dgc] - top;
+  const int i = (int)atomicAdd(&S.arr[dgc], 1u);
   if (i < limit) {
-    const size_t widx = dtile * (size_t)S.K * TC + (size_t)(S.K - 1 - i) * TC + dc;
-    S.wdx[widx] = dx;
-    S.wdy[widx] = dy;
-    S.wpx[widx] = px;
-    S.wpy[widx] = py;
-    S.wpz[widx] = pz;
-    S.wtag[widx] = tag;
+    const size_t widx = dtile * (size_t)S.K * TC + (size_t)(S.K - 1 - top - i) * TC + dc;
+    S.dx[widx] = dx;
+    S.dy[widx] = dy;
+    S.px[widx] = px;
+    S.py[widx] = py;
+    S.pz[widx] = pz;
+    S.tag[widx] = tag;
   } else {
-    atomicSub(&S.wntop[dgc], 1u);
+    atomicSub(&S.arr[dgc], 1u);
     const uint32_t o = atomicAdd(S.wocount, 1u);
     if (o < S.ocap) {
       S.wocell[o] = (uint32_t)ix | ((uint32_t)iy << 16);
@@ -217,13 +218,29 @@ __host__ __device__ inline int eb_pitch(int TX) {
   return p;
 }
 
+// Per-warp queues of the rare work (a particle whose half-step cell differs
+// from its owner cell deposits J elsewhere; a particle whose full-step cell
+// differs deposits rho elsewhere and moves to another cell).  Lanes append with
+// a ballot; the warp drains a queue cooperatively once it holds >= 32 entries,
+// so the rare paths run converged instead of as divergent branches.
+constexpr int QCAP = 64;     // entries per queue
+constexpr int QWORDS = 7;    // words per entry
+constexpr int QWARP = 2 * QWORDS * QCAP;  // floats per warp (J queue + mover queue)
+
+__host__ __device__ inline size_t slot_smem_floats(int TX, int TY, bool push, bool move) {
+  const size_t win = move ? 5 * (size_t)(TX + 4) * (TY + 4) : 0;
+  const size_t eb = push ? 6 * (size_t)eb_pitch(TX) * (TY + 2) : 0;
+  const size_t q = move ? (size_t)(TX * TY / 32) * QWARP : 0;
+  return win + eb + q;
+}
+
 // One CTA per tile, one thread per cell.  Every particle a thread processes
-// starts in the thread's cell: the E/B window of the tile (+1 cell halo) is
-// staged once in shared memory and gathered with conflict-free loads, and
-// deposits that stay in the cell's 3x3 stencil accumulate in registers (36
-// accumulators); only particles whose half- or full-step cell differs use
-// shared-memory atomics.  The next particle's state is loaded while the
-// current one is processed.
+// starts in the thread's cell: E/B of the tile (+1 halo) is staged once in
+// shared memory and gathered with conflict-free loads; J and rho deposits that
+// stay in the owner cell's stencil accumulate in registers.  The particles stay
+// in their slot (in place); a particle that leaves marks its slot as a hole.
+// The warp walks its cells' slots in lock-step rounds (low range, then the top
+// range of arrivals), so the loads and stores of a round are coalesced.
 template <bool PUSH, bool MOVE>
 __global__ void __launch_bounds__(256, 2) k_slot(const __grid_constant__ StepArgs a) {
   extern __shared__ float smem[];
@@ -231,6 +248,7 @@ __global__ void __launch_bounds__(256, 2) k_slot(const __grid_constant__ StepArg
   const int tile = blockIdx.x;
   const int tx = tile % a.NTX, ty = tile / a.NTX;
   const int c = threadIdx.x;
+  const int lane = c & 31, warp = c >> 5;
   const int lx = c & (a.TX - 1), ly = c >> a.logTX;
   const int ox = tx * a.TX + lx + 1, oy = ty * a.TY + ly + 1;  // owner cell (reference coords)
   const int W = a.g.W, nx = a.g.nx, ny = a.g.ny;
@@ -246,6 +264,9 @@ __global__ void __launch_bounds__(256, 2) k_slot(const __grid_constant__ StepArg
   // E/B window: tile + 1 cell, 6 planes
   const int PE = eb_pitch(a.TX), EY = a.TY + 2, EN = PE * EY;
   float* ebw = smem + (MOVE ? 5 * WN : 0);
+  float* qbase = ebw + (PUSH ? 6 * EN : 0) + warp * QWARP;
+  float* qj = qbase;                   // [QWORDS][QCAP]
+  float* qm = qbase + QWORDS * QCAP;   // [QWORDS][QCAP]
   if (MOVE)
     for (int i = c; i < 5 * WN; i += TC) win[i] = 0.f;
   if (PUSH) {
@@ -265,133 +286,208 @@ __global__ void __launch_bounds__(256, 2) k_slot(const __grid_constant__ StepArg
   const size_t gc = (size_t)tile * TC + c;
   const float half_dt = 0.5f * a.p.dt;
   const float csqinv = a.p.csqinv;
+  const unsigned lt_mask = (1u << lane) - 1u;
 
   for (int s = 0; s < a.ns; ++s) {
     const SpeciesArgs& S = a.sp[s];
-    const float* __restrict__ rdx = S.dx;
-    const float* __restrict__ rdy = S.dy;
-    const float* __restrict__ rpx = S.px;
-    const float* __restrict__ rpy = S.py;
-    const float* __restrict__ rpz = S.pz;
-    const uint32_t* __restrict__ rtag = S.tag;
+    float* __restrict__ sdx = S.dx;
+    float* __restrict__ sdy = S.dy;
+    float* __restrict__ spx = S.px;
+    float* __restrict__ spy = S.py;
+    float* __restrict__ spz = S.pz;
     const int K = S.K;
     const size_t base = (size_t)tile * K * TC + c;
-    const int nlow = (int)S.nlow[gc], ntop = (int)S.ntop[gc];
-    const int total = nlow + ntop;
+    const int nlow = (int)S.nlow[gc], ntop = (int)S.top[gc];
+    const int wl = __reduce_max_sync(0xffffffffu, nlow);
+    const int rounds = wl + __reduce_max_sync(0xffffffffu, ntop);
     const float q = S.charge, beta = S.beta, alpha = S.alpha;
     float accD[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) accD[k] = 0.f;
-    int wcur = 0;
-    // software pipeline: state of particle n is loaded during particle n-1
+    int nq_j = 0, nq_m = 0;  // warp-uniform queue sizes
+
+    auto slot_of = [&](int r, bool& act) -> int {
+      if (r < wl) {
+        act = r < nlow;
+        return r;
+      }
+      act = (r - wl) < ntop;
+      return K - 1 - (r - wl);
+    };
+    // drain the J queue: deposit the stencils whose centre left the owner cell
+    auto drain_j = [&]() {
+      for (int e = lane; e < nq_j; e += 32) {
+        const uint32_t cell = __float_as_uint(qj[0 * QCAP + e]);
+        const int jx = (int)(cell & 0xFFFFu), jy = (int)(cell >> 16);
+        float w[9];
+        tsc_weights(qj[1 * QCAP + e], qj[2 * QCAP + e], w);
+        dep9(wjx, WX, WY, wx0, wy0, a.f.J[0], W, jx, jy, w, qj[3 * QCAP + e]);
+        dep9(wjy, WX, WY, wx0, wy0, a.f.J[1], W, jx, jy, w, qj[4 * QCAP + e]);
+        dep9(wjz, WX, WY, wx0, wy0, a.f.J[2], W, jx, jy, w, qj[5 * QCAP + e]);
+      }
+      __syncwarp();
+      nq_j = 0;
+    };
+    // drain the mover queue: rho/dens at the new cell, then relocation
+    auto drain_m = [&]() {
+      for (int e = lane; e < nq_m; e += 32) {
+        const uint32_t cell = __float_as_uint(qm[0 * QCAP + e]);
+        const int mx = (int)(cell & 0xFFFFu), my = (int)(cell >> 16);
+        const float mdx = qm[1 * QCAP + e], mdy = qm[2 * QCAP + e];
+        float w[9];
+        tsc_weights(mdx, mdy, w);
+        dep9(wrho, WX, WY, wx0, wy0, a.f.dsty, W, mx, my, w, q);
+        dep9(wdens, WX, WY, wx0, wy0, a.f.dens, W, mx, my, w, 1.0f);
+        relocate(a, S, mx, my, mdx, mdy, qm[3 * QCAP + e], qm[4 * QCAP + e], qm[5 * QCAP + e],
+                 __float_as_uint(qm[6 * QCAP + e]));
+      }
+      __syncwarp();
+      nq_m = 0;
+    };
+
+    // software pipeline: the state of round r+1 is loaded during round r
     float ndx = 0.f, ndy = 0.f, npx = 0.f, npy = 0.f, npz = 0.f;
-    uint32_t ntag = 0;
+    bool nact = false;
     size_t nidx = base;
-    if (total > 0) {
-      nidx = base + (size_t)(nlow > 0 ? 0 : K - 1) * TC;
-      ndx = rdx[nidx];
-      ndy = rdy[nidx];
-      npx = rpx[nidx];
-      npy = rpy[nidx];
-      npz = rpz[nidx];
-      if (MOVE) ntag = rtag[nidx];
+    if (rounds > 0) {
+      const int sl = slot_of(0, nact);
+      nidx = base + (size_t)sl * TC;
+      if (nact) {
+        ndx = sdx[nidx];
+        ndy = sdy[nidx];
+        npx = spx[nidx];
+        npy = spy[nidx];
+        npz = spz[nidx];
+      }
     }
-    for (int n = 0; n < total; ++n) {
+    for (int r = 0; r < rounds; ++r) {
       const size_t idx = nidx;
+      const bool act = nact && !is_hole(ndx);
       float dx = ndx, dy = ndy, px = npx, py = npy, pz = npz;
-      const uint32_t tag = ntag;
-      if (n + 1 < total) {
-        const int m = n + 1;
-        const int slot = m < nlow ? m : K - 1 - (m - nlow);
-        nidx = base + (size_t)slot * TC;
-        ndx = rdx[nidx];
-        ndy = rdy[nidx];
-        npx = rpx[nidx];
-        npy = rpy[nidx];
-        npz = rpz[nidx];
-        if (MOVE) ntag = rtag[nidx];
-      }
-      float psa;
-      if (PUSH) {
-        float w[9];
-        tsc_weights(dx, dy, w);
-        float gth[6];
-#pragma unroll
-        for (int f = 0; f < 6; ++f) {
-          const float* e = eb + f * EN;
-          float t = w[0] * e[0];
-          t += w[1] * e[1];
-          t += w[2] * e[2];
-          t += w[3] * e[PE];
-          t += w[4] * e[PE + 1];
-          t += w[5] * e[PE + 2];
-          t += w[6] * e[2 * PE];
-          t += w[7] * e[2 * PE + 1];
-          t += w[8] * e[2 * PE + 2];
-          gth[f] = t;
+      if (r + 1 < rounds) {
+        const int sl = slot_of(r + 1, nact);
+        nidx = base + (size_t)sl * TC;
+        if (nact) {
+          ndx = sdx[nidx];
+          ndy = sdy[nidx];
+          npx = spx[nidx];
+          npy = spy[nidx];
+          npz = spz[nidx];
         }
-        boris(gth, beta, alpha, csqinv, px, py, pz, psa);
-      } else {
-        psa = gamma_of(px, py, pz, csqinv);
       }
-      if (!MOVE) {
-        S.rpx[idx] = px;
-        S.rpy[idx] = py;
-        S.rpz[idx] = pz;
-        continue;
-      }
-      const float inv = 1.0f / psa;
-      const float c1 = half_dt * inv;
-      int ix = ox, iy = oy;
-      // first half: position, boundaries, current (src/lib.rs:480-484)
-      move_half(c1, px, py, ix, iy, dx, dy);
-      apply_bc(a.p, nx, ny, ix, iy, dx, px, a.derr);
-      {
-        const float vx = q * px * inv, vy = q * py * inv, vz = q * pz * inv;
-        float w[9];
-        tsc_weights(dx, dy, w);
-        if (ix == ox && iy == oy) {
+      bool jcross = false, mover = false;
+      int ix = ox, iy = oy, jxc = ox, jyc = oy;
+      float jdx = 0.f, jdy = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
+      if (act) {
+        float psa;
+        if (PUSH) {
+          float w[9];
+          tsc_weights(dx, dy, w);
+          float gth[6];
 #pragma unroll
-          for (int k = 0; k < 9; ++k) {
-            accJ[0][k] += w[k] * vx;
-            accJ[1][k] += w[k] * vy;
-            accJ[2][k] += w[k] * vz;
+          for (int f = 0; f < 6; ++f) {
+            const float* e = eb + f * EN;
+            float t = w[0] * e[0];
+            t += w[1] * e[1];
+            t += w[2] * e[2];
+            t += w[3] * e[PE];
+            t += w[4] * e[PE + 1];
+            t += w[5] * e[PE + 2];
+            t += w[6] * e[2 * PE];
+            t += w[7] * e[2 * PE + 1];
+            t += w[8] * e[2 * PE + 2];
+            gth[f] = t;
           }
+          boris(gth, beta, alpha, csqinv, px, py, pz, psa);
         } else {
-          dep9(wjx, WX, WY, wx0, wy0, a.f.J[0], W, ix, iy, w, vx);
-          dep9(wjy, WX, WY, wx0, wy0, a.f.J[1], W, ix, iy, w, vy);
-          dep9(wjz, WX, WY, wx0, wy0, a.f.J[2], W, ix, iy, w, vz);
+          psa = gamma_of(px, py, pz, csqinv);
         }
-      }
-      // second half: position, boundaries, density (src/lib.rs:486-488)
-      move_half(c1, px, py, ix, iy, dx, dy);
-      apply_bc(a.p, nx, ny, ix, iy, dx, px, a.derr);
-      {
-        float w[9];
-        tsc_weights(dx, dy, w);
-        if (ix == ox && iy == oy) {
+        if (!MOVE) {
+          spx[idx] = px;
+          spy[idx] = py;
+          spz[idx] = pz;
+        } else {
+          const float inv = 1.0f / psa;
+          const float c1 = half_dt * inv;
+          // first half: position, boundaries, current (src/lib.rs:480-484)
+          move_half(c1, px, py, ix, iy, dx, dy);
+          apply_bc(a.p, nx, ny, ix, iy, dx, px, a.derr);
+          vx = q * px * inv;
+          vy = q * py * inv;
+          vz = q * pz * inv;
+          jcross = ix != ox || iy != oy;
+          if (!jcross) {
+            float w[9];
+            tsc_weights(dx, dy, w);
+            // summation order of deposits is not the reference's anyway: fused multiply-add here
 #pragma unroll
-          for (int k = 0; k < 9; ++k) accD[k] += w[k];
-        } else {
-          dep9(wrho, WX, WY, wx0, wy0, a.f.dsty, W, ix, iy, w, q);
-          dep9(wdens, WX, WY, wx0, wy0, a.f.dens, W, ix, iy, w, 1.0f);
+            for (int k = 0; k < 9; ++k) {
+              accJ[0][k] = __fmaf_rn(w[k], vx, accJ[0][k]);
+              accJ[1][k] = __fmaf_rn(w[k], vy, accJ[1][k]);
+              accJ[2][k] = __fmaf_rn(w[k], vz, accJ[2][k]);
+            }
+          } else {
+            jxc = ix;
+            jyc = iy;
+            jdx = dx;
+            jdy = dy;
+          }
+          // second half: position, boundaries, density (src/lib.rs:486-488)
+          move_half(c1, px, py, ix, iy, dx, dy);
+          apply_bc(a.p, nx, ny, ix, iy, dx, px, a.derr);
+          mover = ix != ox || iy != oy;
+          if (!mover) {
+            float w[9];
+            tsc_weights(dx, dy, w);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) accD[k] += w[k];
+            sdx[idx] = dx;
+            sdy[idx] = dy;
+            spx[idx] = px;
+            spy[idx] = py;
+            spz[idx] = pz;
+          } else {
+            sdx[idx] = __uint_as_float(HOLE_BITS);
+          }
         }
       }
-      if (ix == ox && iy == oy) {
-        const size_t widx = base + (size_t)wcur * TC;
-        S.wdx[widx] = dx;
-        S.wdy[widx] = dy;
-        S.wpx[widx] = px;
-        S.wpy[widx] = py;
-        S.wpz[widx] = pz;
-        S.wtag[widx] = tag;
-        ++wcur;
-      } else {
-        relocate(a, S, ix, iy, dx, dy, px, py, pz, tag);
+      if (MOVE) {
+        const unsigned mj = __ballot_sync(0xffffffffu, jcross);
+        if (mj) {
+          if (jcross) {
+            const int e = nq_j + __popc(mj & lt_mask);
+            qj[0 * QCAP + e] = __uint_as_float((uint32_t)jxc | ((uint32_t)jyc << 16));
+            qj[1 * QCAP + e] = jdx;
+            qj[2 * QCAP + e] = jdy;
+            qj[3 * QCAP + e] = vx;
+            qj[4 * QCAP + e] = vy;
+            qj[5 * QCAP + e] = vz;
+          }
+          nq_j += __popc(mj);
+          __syncwarp();
+          if (nq_j >= 32) drain_j();
+        }
+        const unsigned mm = __ballot_sync(0xffffffffu, mover);
+        if (mm) {
+          if (mover) {
+            const int e = nq_m + __popc(mm & lt_mask);
+            qm[0 * QCAP + e] = __uint_as_float((uint32_t)ix | ((uint32_t)iy << 16));
+            qm[1 * QCAP + e] = dx;
+            qm[2 * QCAP + e] = dy;
+            qm[3 * QCAP + e] = px;
+            qm[4 * QCAP + e] = py;
+            qm[5 * QCAP + e] = pz;
+            qm[6 * QCAP + e] = __uint_as_float(S.tag[idx]);
+          }
+          nq_m += __popc(mm);
+          __syncwarp();
+          if (nq_m >= 32) drain_m();
+        }
       }
     }
     if (MOVE) {
-      S.wnlow[gc] = (uint32_t)wcur;
+      if (nq_j) drain_j();
+      if (nq_m) drain_m();
       // this species' density stencil of the owner cell -> window
       const int bl = (oy - 1 - wy0) * WX + (ox - 1 - wx0);
 #pragma unroll
@@ -420,7 +516,6 @@ __global__ void __launch_bounds__(256, 2) k_slot(const __grid_constant__ StepArg
   }
   __syncthreads();
   // window -> global (clipped to the ghosted grid)
-  float* dst[5] = {a.f.J[0], a.f.J[1], a.f.J[2], a.f.dsty, a.f.dens};
   for (int i = c; i < 5 * WN; i += TC) {
     const float v = win[i];
     if (v == 0.f) continue;
@@ -428,7 +523,8 @@ __global__ void __launch_bounds__(256, 2) k_slot(const __grid_constant__ StepArg
     const int wy = k / WX, wx = k - wy * WX;
     const int gx = wx0 + wx, gy = wy0 + wy;
     if (gx < 0 || gx > nx + 1 || gy < 0 || gy > ny + 1) continue;
-    atomicAdd(dst[plane] + (size_t)gy * W + gx, v);
+    float* d = plane == 0 ? a.f.J[0] : plane == 1 ? a.f.J[1] : plane == 2 ? a.f.J[2] : plane == 3 ? a.f.dsty : a.f.dens;
+    atomicAdd(d + (size_t)gy * W + gx, v);
   }
 }
 
@@ -449,11 +545,12 @@ __global__ void k_slot_overflow(const __grid_constant__ StepArgs a, int s) {
     if (PUSH) {
       float w[9];
       tsc_weights(dx, dy, w);
-      const float* src[6] = {a.f.E[0], a.f.E[1], a.f.E[2], a.f.B[0], a.f.B[1], a.f.B[2]};
       float gth[6];
 #pragma unroll
       for (int f = 0; f < 6; ++f) {
-        const float* b = src[f] + (size_t)(iy - 1) * W + (ix - 1);
+        const float* src = f == 0 ? a.f.E[0] : f == 1 ? a.f.E[1] : f == 2 ? a.f.E[2] : f == 3 ? a.f.B[0]
+                           : f == 4 ? a.f.B[1] : a.f.B[2];
+        const float* b = src + (size_t)(iy - 1) * W + (ix - 1);
         float t = w[0] * b[0];
         t += w[1] * b[1];
         t += w[2] * b[2];
@@ -470,9 +567,9 @@ __global__ void k_slot_overflow(const __grid_constant__ StepArgs a, int s) {
       psa = gamma_of(px, py, pz, csqinv);
     }
     if (!MOVE) {
-      S.ropx_w[i] = px;
-      S.ropy_w[i] = py;
-      S.ropz_w[i] = pz;
+      S.ropx[i] = px;
+      S.ropy[i] = py;
+      S.ropz[i] = pz;
       continue;
     }
     const float q = S.charge;
@@ -508,29 +605,62 @@ __global__ void k_slot_overflow(const __grid_constant__ StepArgs a, int s) {
   }
 }
 
+// After a moving step: the arrivals become part of the committed top range.
+__global__ void k_commit(uint32_t* top, uint32_t* arr, size_t ncells) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < ncells; i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t a = arr[i];
+    if (a) {
+      top[i] += a;
+      arr[i] = 0;
+    }
+  }
+}
+
+// Remove the holes: each thread packs its cell's particles into slots
+// 0..n-1, the low range in place first, then the top range in ascending slot
+// order (a destination never lies above its source, so nothing unread is overwritten).
+__global__ void k_compact(float* dx, float* dy, float* px, float* py, float* pz, uint32_t* tag, uint32_t* nlow,
+                          uint32_t* top, int K, int TC, size_t ncells) {
+  for (size_t gc = blockIdx.x * (size_t)blockDim.x + threadIdx.x; gc < ncells; gc += (size_t)gridDim.x * blockDim.x) {
+    const size_t tile = gc / TC;
+    const int c = (int)(gc - tile * TC);
+    const size_t base = tile * (size_t)K * TC + c;
+    const int nl = (int)nlow[gc], nt = (int)top[gc];
+    int w = 0;
+    for (int n = 0; n < nl + nt; ++n) {
+      const int slot = n < nl ? n : K - nt + (n - nl);
+      const size_t i = base + (size_t)slot * TC;
+      const float x = dx[i];
+      if (is_hole(x)) continue;
+      if (slot != w) {
+        const size_t o = base + (size_t)w * TC;
+        dx[o] = x;
+        dy[o] = dy[i];
+        px[o] = px[i];
+        py[o] = py[i];
+        pz[o] = pz[i];
+        tag[o] = tag[i];
+      }
+      ++w;
+    }
+    nlow[gc] = (uint32_t)w;
+    top[gc] = 0;
+  }
+}
+
 static SpeciesArgs species_args(Species& sp) {
   SlotSpecies& s = sp.slot;
-  const int r = s.cur, w = s.cur ^ 1;
+  const int r = s.ocur, w = s.ocur ^ 1;
   SpeciesArgs A;
-  A.dx = s.dx[r];
-  A.dy = s.dy[r];
-  A.px = s.px[r];
-  A.py = s.py[r];
-  A.pz = s.pz[r];
-  A.tag = s.tag[r];
-  A.nlow = s.nlow[r];
-  A.ntop = s.ntop[r];
-  A.rpx = s.px[r];
-  A.rpy = s.py[r];
-  A.rpz = s.pz[r];
-  A.wdx = s.dx[w];
-  A.wdy = s.dy[w];
-  A.wpx = s.px[w];
-  A.wpy = s.py[w];
-  A.wpz = s.pz[w];
-  A.wtag = s.tag[w];
-  A.wnlow = s.nlow[w];
-  A.wntop = s.ntop[w];
+  A.dx = s.dx;
+  A.dy = s.dy;
+  A.px = s.px;
+  A.py = s.py;
+  A.pz = s.pz;
+  A.tag = s.tag;
+  A.nlow = s.nlow;
+  A.top = s.top;
+  A.arr = s.arr;
   A.rocell = s.ocell[r];
   A.rodx = s.odx[r];
   A.rody = s.ody[r];
@@ -538,9 +668,6 @@ static SpeciesArgs species_args(Species& sp) {
   A.ropy = s.opy[r];
   A.ropz = s.opz[r];
   A.rotag = s.otag[r];
-  A.ropx_w = s.opx[r];
-  A.ropy_w = s.opy[r];
-  A.ropz_w = s.opz[r];
   A.wocell = s.ocell[w];
   A.wodx = s.odx[w];
   A.wody = s.ody[w];
@@ -556,6 +683,12 @@ static SpeciesArgs species_args(Species& sp) {
   A.beta = sp.beta;
   A.K = s.K;
   return A;
+}
+
+void slot_set_kernel_attributes() {
+  for (const void* f : {(const void*)k_slot<true, true>, (const void*)k_slot<true, false>,
+                        (const void*)k_slot<false, true>})
+    SPX_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
 }
 
 int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysParams& pp, const FieldPtrs& fp,
@@ -574,16 +707,10 @@ int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysPar
   int launches = 0;
   for (int s = s0; s < s1; ++s) {
     a.sp[s - s0] = species_args(sp[s]);
-    if (move) {
-      SlotSpecies& S = sp[s].slot;
-      const int w = S.cur ^ 1;
-      SPX_CUDA_TRY(cudaMemsetAsync(S.ntop[w], 0, pg.ncells() * sizeof(uint32_t), st));
-      SPX_CUDA_TRY(cudaMemsetAsync(S.ocount + w, 0, sizeof(uint32_t), st));
-    }
+    if (move) SPX_CUDA_TRY(cudaMemsetAsync(sp[s].slot.ocount + (sp[s].slot.ocur ^ 1), 0, sizeof(uint32_t), st));
   }
   const int TC = pg.TC();
-  const size_t smem = ((move ? 5 * (size_t)(pg.TX + 4) * (pg.TY + 4) : 0) +
-                       (push ? 6 * (size_t)eb_pitch(pg.TX) * (pg.TY + 2) : 0)) * sizeof(float);
+  const size_t smem = slot_smem_floats(pg.TX, pg.TY, push, move) * sizeof(float);
   if (push && move)
     k_slot<true, true><<<pg.ntiles(), TC, smem, st>>>(a);
   else if (push)
@@ -601,9 +728,21 @@ int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysPar
       k_slot_overflow<false, true><<<64, 256, 0, st>>>(a, s);
     ++launches;
   }
+  if (move) {
+    for (int s = s0; s < s1; ++s) {
+      SlotSpecies& S = sp[s].slot;
+      k_commit<<<148 * 8, 256, 0, st>>>(S.top, S.arr, pg.ncells());
+      ++launches;
+      S.ocur ^= 1;
+      if (++S.moves_since_compact >= S.compact_every) {
+        k_compact<<<(int)((pg.ncells() + 255) / 256), 256, 0, st>>>(S.dx, S.dy, S.px, S.py, S.pz, S.tag, S.nlow, S.top,
+                                                                   S.K, TC, pg.ncells());
+        ++launches;
+        S.moves_since_compact = 0;
+      }
+    }
+  }
   SPX_CUDA_TRY(cudaGetLastError());
-  if (move)
-    for (int s = s0; s < s1; ++s) sp[s].slot.cur ^= 1;
   return launches;
 }
 
@@ -651,13 +790,15 @@ void slot_scatter(Species& s, const ParticleGeom& pg, uint64_t n, const uint32_t
                   const float* dy, const float* px, const float* py, const float* pz, const uint32_t* tag,
                   uint32_t* cursor, cudaStream_t st) {
   SlotSpecies& S = s.slot;
-  S.cur = 0;
+  S.ocur = 0;
+  S.moves_since_compact = 0;
   SPX_CUDA_TRY(cudaMemsetAsync(cursor, 0, pg.ncells() * sizeof(uint32_t), st));
   if (n)
-    k_scatter<<<148 * 8, 256, 0, st>>>(n, cell, dx, dy, px, py, pz, tag, cursor, S.dx[0], S.dy[0], S.px[0], S.py[0],
-                                       S.pz[0], S.tag[0], S.K, pg.TX, pg.TY, pg.logTX, pg.logTY, pg.NTX);
-  SPX_CUDA_TRY(cudaMemcpyAsync(S.nlow[0], cursor, pg.ncells() * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-  SPX_CUDA_TRY(cudaMemsetAsync(S.ntop[0], 0, pg.ncells() * sizeof(uint32_t), st));
+    k_scatter<<<148 * 8, 256, 0, st>>>(n, cell, dx, dy, px, py, pz, tag, cursor, S.dx, S.dy, S.px, S.py, S.pz, S.tag,
+                                       S.K, pg.TX, pg.TY, pg.logTX, pg.logTY, pg.NTX);
+  SPX_CUDA_TRY(cudaMemcpyAsync(S.nlow, cursor, pg.ncells() * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+  SPX_CUDA_TRY(cudaMemsetAsync(S.top, 0, pg.ncells() * sizeof(uint32_t), st));
+  SPX_CUDA_TRY(cudaMemsetAsync(S.arr, 0, pg.ncells() * sizeof(uint32_t), st));
   SPX_CUDA_TRY(cudaMemsetAsync(S.ocount, 0, 2 * sizeof(uint32_t), st));
   SPX_CUDA_TRY(cudaGetLastError());
 }
@@ -671,11 +812,12 @@ __global__ void k_unpack(SpeciesArgs S, int TX, int TY, int logTX, int NTX, size
     const int c = (int)(gc - tile * TC);
     const int tx = (int)(tile % NTX), ty = (int)(tile / NTX);
     const uint32_t cx = tx * TX + (c & (TX - 1)) + 1, cy = ty * TY + (c >> logTX) + 1;
-    const int nlow = (int)S.nlow[gc], ntop = (int)S.ntop[gc];
+    const int nlow = (int)S.nlow[gc], ntop = (int)S.top[gc];
     const size_t base = tile * (size_t)S.K * TC + c;
     for (int n = 0; n < nlow + ntop; ++n) {
       const int slot = n < nlow ? n : S.K - 1 - (n - nlow);
       const size_t i = base + (size_t)slot * TC;
+      if (is_hole(S.dx[i])) continue;
       const uint32_t t = S.tag[i];
       if (ix) ix[t] = cx;
       if (iy) iy[t] = cy;
@@ -715,17 +857,17 @@ void slot_unpack(const Species& s, const ParticleGeom& pg, uint32_t* ix, uint32_
   SPX_CUDA_TRY(cudaGetLastError());
 }
 
-__global__ void k_max_occ(const uint32_t* nlow, const uint32_t* ntop, size_t n, uint32_t* out) {
+__global__ void k_max_occ(const uint32_t* nlow, const uint32_t* top, size_t n, uint32_t* out) {
   uint32_t m = 0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    m = max(m, nlow[i] + ntop[i]);
+    m = max(m, nlow[i] + top[i]);
   for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
 void slot_max_occupancy(const Species& s, const ParticleGeom& pg, uint32_t* d_out, cudaStream_t st) {
   const SlotSpecies& S = s.slot;
-  k_max_occ<<<148 * 4, 256, 0, st>>>(S.nlow[S.cur], S.ntop[S.cur], pg.ncells(), d_out);
+  k_max_occ<<<148 * 4, 256, 0, st>>>(S.nlow, S.top, pg.ncells(), d_out);
   SPX_CUDA_TRY(cudaGetLastError());
 }
 
@@ -733,17 +875,15 @@ void slot_allocate(Species& s, const ParticleGeom& pg, int K, uint64_t n) {
   SlotSpecies& S = s.slot;
   const size_t cap = pg.ncells() * (size_t)K;
   S.K = K;
-  for (int b = 0; b < 2; ++b) {
-    SPX_CUDA_TRY(cudaMalloc(&S.dx[b], cap * sizeof(float)));
-    SPX_CUDA_TRY(cudaMalloc(&S.dy[b], cap * sizeof(float)));
-    SPX_CUDA_TRY(cudaMalloc(&S.px[b], cap * sizeof(float)));
-    SPX_CUDA_TRY(cudaMalloc(&S.py[b], cap * sizeof(float)));
-    SPX_CUDA_TRY(cudaMalloc(&S.pz[b], cap * sizeof(float)));
-    SPX_CUDA_TRY(cudaMalloc(&S.tag[b], cap * sizeof(uint32_t)));
-    SPX_CUDA_TRY(cudaMalloc(&S.nlow[b], pg.ncells() * sizeof(uint32_t)));
-    SPX_CUDA_TRY(cudaMalloc(&S.ntop[b], pg.ncells() * sizeof(uint32_t)));
-    SPX_CUDA_TRY(cudaMemset(S.nlow[b], 0, pg.ncells() * sizeof(uint32_t)));
-    SPX_CUDA_TRY(cudaMemset(S.ntop[b], 0, pg.ncells() * sizeof(uint32_t)));
+  SPX_CUDA_TRY(cudaMalloc(&S.dx, cap * sizeof(float)));
+  SPX_CUDA_TRY(cudaMalloc(&S.dy, cap * sizeof(float)));
+  SPX_CUDA_TRY(cudaMalloc(&S.px, cap * sizeof(float)));
+  SPX_CUDA_TRY(cudaMalloc(&S.py, cap * sizeof(float)));
+  SPX_CUDA_TRY(cudaMalloc(&S.pz, cap * sizeof(float)));
+  SPX_CUDA_TRY(cudaMalloc(&S.tag, cap * sizeof(uint32_t)));
+  for (uint32_t** p : {&S.nlow, &S.top, &S.arr}) {
+    SPX_CUDA_TRY(cudaMalloc(p, pg.ncells() * sizeof(uint32_t)));
+    SPX_CUDA_TRY(cudaMemset(*p, 0, pg.ncells() * sizeof(uint32_t)));
   }
   S.ocap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(1u << 16, n / 32), 1u << 28);
   for (int b = 0; b < 2; ++b) {
@@ -761,14 +901,18 @@ void slot_allocate(Species& s, const ParticleGeom& pg, int K, uint64_t n) {
 
 void slot_release(Species& s) {
   SlotSpecies& S = s.slot;
+  for (void* p : {(void*)S.dx, (void*)S.dy, (void*)S.px, (void*)S.py, (void*)S.pz, (void*)S.tag, (void*)S.nlow,
+                  (void*)S.top, (void*)S.arr})
+    if (p) cudaFree(p);
   for (int b = 0; b < 2; ++b) {
-    for (void* p : {(void*)S.dx[b], (void*)S.dy[b], (void*)S.px[b], (void*)S.py[b], (void*)S.pz[b], (void*)S.tag[b],
-                    (void*)S.nlow[b], (void*)S.ntop[b], (void*)S.ocell[b], (void*)S.odx[b], (void*)S.ody[b],
-                    (void*)S.opx[b], (void*)S.opy[b], (void*)S.opz[b], (void*)S.otag[b]})
+    for (void* p : {(void*)S.ocell[b], (void*)S.odx[b], (void*)S.ody[b], (void*)S.opx[b], (void*)S.opy[b],
+                    (void*)S.opz[b], (void*)S.otag[b]})
       if (p) cudaFree(p);
   }
   if (S.ocount) cudaFree(S.ocount);
+  const int ce = S.compact_every;
   S = SlotSpecies();
+  S.compact_every = ce;
 }
 
 // ---------------------------------------------------------------- plain FP32 path
@@ -907,11 +1051,12 @@ __global__ void k_kinetic_slot(SpeciesArgs S, int TC, size_t ncells, float mass,
   for (size_t gc = blockIdx.x * (size_t)blockDim.x + threadIdx.x; gc < ncells; gc += (size_t)gridDim.x * blockDim.x) {
     const size_t tile = gc / TC;
     const int cc = (int)(gc - tile * TC);
-    const int nlow = (int)S.nlow[gc], ntop = (int)S.ntop[gc];
+    const int nlow = (int)S.nlow[gc], ntop = (int)S.top[gc];
     const size_t base = tile * (size_t)S.K * TC + cc;
     for (int n = 0; n < nlow + ntop; ++n) {
       const int slot = n < nlow ? n : S.K - 1 - (n - nlow);
       const size_t i = base + (size_t)slot * TC;
+      if (is_hole(S.dx[i])) continue;
       const double g = (double)gamma_of(S.px[i], S.py[i], S.pz[i], csqinv);
       e += (double)mass * (g - 1.0) * csq;
       cnt += 1.0;

@@ -16,24 +16,26 @@ constexpr int MAX_SPECIES = 4;
 // a particle is {dx, dy, px, py, pz, tag} = 24 bytes (tag = its index in the
 // reference's particle order, used only to return data in that order).
 //
-// Two buffers alternate every step.  A cell's particles sit in slots
-// [0, n_low) and [K - n_top, K) of the read buffer.  During a step the thread
-// that owns the cell writes the particles that stay into slots 0, 1, ... of
-// the write buffer; particles that move to another cell are appended from the
-// top (slot K-1 downwards) of the destination cell through an atomic counter.
-// The appender bounds its slot by K - (n_low + n_top of the destination in the
-// read buffer), which the owner's writes can never reach, so the two never
-// collide.  A particle that finds no room goes to the overflow list, which a
-// fallback kernel processes every step until the host repacks with a larger K.
+// Particles stay in their slot: a cell's particles occupy slots [0, nlow) and
+// [K - top, K).  During a step the thread that owns the cell updates every
+// particle in place; a particle that moves to another cell marks its old slot
+// as a hole and is appended below the destination's top range (slot
+// K-1-(top+i), i from an atomic arrivals counter); the bound i < K - nlow - top
+// keeps appends clear of every slot the destination's owner touches.  After
+// the step the arrivals join the top range; every `compact_every` moving steps
+// a compaction pass removes the holes.  A particle that finds no room goes to
+// the overflow list, which a fallback kernel processes every step until the
+// host repacks with a larger K.
 struct SlotSpecies {
-  float* dx[2] = {};
-  float* dy[2] = {};
-  float* px[2] = {};
-  float* py[2] = {};
-  float* pz[2] = {};
-  uint32_t* tag[2] = {};
-  uint32_t* nlow[2] = {};
-  uint32_t* ntop[2] = {};
+  float* dx = nullptr;
+  float* dy = nullptr;
+  float* px = nullptr;
+  float* py = nullptr;
+  float* pz = nullptr;
+  uint32_t* tag = nullptr;
+  uint32_t* nlow = nullptr;  // low range extent per cell (holes included)
+  uint32_t* top = nullptr;   // committed top range extent per cell
+  uint32_t* arr = nullptr;   // arrivals of the running step per cell
   // overflow lists (double buffered): cell packed as ix | iy << 16 (reference coords)
   uint32_t* ocell[2] = {};
   float* odx[2] = {};
@@ -45,7 +47,9 @@ struct SlotSpecies {
   uint32_t* ocount = nullptr;  // [2]
   uint32_t ocap = 0;
   int K = 0;
-  int cur = 0;  // read buffer
+  int ocur = 0;  // overflow list read by the next step
+  int moves_since_compact = 0;
+  int compact_every = 8;
 };
 
 // Plain-path storage: global FP32 positions x = ix + dx, y = iy + dy in the
@@ -103,7 +107,8 @@ void slot_unpack(const Species& s, const ParticleGeom& pg, uint32_t* ix, uint32_
 // relocation.  Returns the number of kernel launches (memsets not counted).
 int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysParams& pp, const FieldPtrs& fp,
               bool push, bool move, int* derr, cudaStream_t st);
-// Maximum cell occupancy (low + top + arrivals) after the last step, for repack decisions.
+// Maximum cell occupancy (low + top range, holes included), for repack decisions.
+void slot_set_kernel_attributes();
 void slot_max_occupancy(const Species& s, const ParticleGeom& pg, uint32_t* d_out, cudaStream_t st);
 
 // --- plain path ---------------------------------------------------------------
