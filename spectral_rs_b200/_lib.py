@@ -10,7 +10,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libspectral_gpu.so")
+# SPX_LIB_PATH selects another build of the same library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("SPX_LIB_PATH") or os.path.join(HERE, "libspectral_gpu.so")
 
 SPX_OK = 0
 ERRORS = {1: "SPX_ERR_ARG", 2: "SPX_ERR_CUDA", 3: "SPX_ERR_BOUNDS", 4: "SPX_ERR_WALL",

@@ -64,6 +64,7 @@ static int check_device_error(spx_ctx* c) {
   if (h & DERR_WALL) return fail(c, SPX_ERR_WALL, "reflecting wall assertion: a particle is beyond wall_loc+1 or at ix <= delta");
   if (h & DERR_BOUNDS) return fail(c, SPX_ERR_BOUNDS, "particle cell index out of the grid");
   if (h & DERR_OVERFLOW_LOST) return fail(c, SPX_ERR_STATE, "particle overflow list full: slot capacity too small");
+  if (h & DERR_TIMEOUT) return fail(c, SPX_ERR_TIMEOUT, "a bounded wait for staged particle data gave up");
   return fail(c, SPX_ERR_STATE, "device error word " + std::to_string(h));
 }
 

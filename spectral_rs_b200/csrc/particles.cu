@@ -28,6 +28,75 @@ __device__ __forceinline__ void tsc_weights(float dx, float dy, float (&w)[9]) {
   w[8] = 0.5f * (0.5f + dy) * (0.5f + dy) * 0.5f * (0.5f + dx) * (0.5f + dx);
 }
 
+// ---------------------------------------------------------------- packed FP32x2
+// sm_100a executes two FP32 operations per instruction (add/sub/mul/fma .f32x2).
+// A lone packed mul, add or sub rounds each element exactly like the scalar
+// .rn operation, but the code generator fuses a packed multiply feeding a
+// packed add into a fused multiply-add even with contraction disabled (measured:
+// ~26% of random mul+add pairs differ from the scalar result).  So packed ops
+// appear here only in multiply-only chains, constant-offset subtractions, and
+// the deposit sums (whose order and rounding are not the reference's anyway);
+// every multiply feeding an add on the exact path stays scalar.
+__device__ __forceinline__ unsigned long long pk2(float2 a) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+  return r;
+}
+__device__ __forceinline__ float2 up2(unsigned long long r) {
+  float2 a;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+  return a;
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
+  return up2(r);
+}
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
+  return up2(r);
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
+  return up2(r);
+}
+// fused multiply-add: only for sums whose rounding is not the reference's anyway (deposits)
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)), "l"(pk2(c)));
+  return up2(r);
+}
+__device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
+
+// tsc_weights restated pairwise: w00/w02, w20/w22 and w10/w12 share their
+// left factors and differ only in (0.5 - dx) vs (0.5 + dx), so each pair is
+// one packed product chain with the reference's association order.  The two
+// 0.75 - d*d terms (a multiply feeding a subtraction) stay scalar.
+__device__ __forceinline__ void tsc_weights_x2(float dx, float dy, float (&w)[9]) {
+  const float2 ab = sub2(bc2(0.5f), make_float2(dy, -dy));  // (0.5 - dy, 0.5 + dy)
+  const float2 cd = sub2(bc2(0.5f), make_float2(dx, -dx));  // (0.5 - dx, 0.5 + dx)
+  const float2 p1 = mul2(bc2(0.5f), ab);
+  const float2 p2 = mul2(p1, ab);                             // (0.5 a a, 0.5 b b)
+  const float2 p3 = mul2(p2, bc2(0.5f));
+  const float2 fh = make_float2(0.75f - dy * dy, 0.75f - dx * dx);
+  const float f05 = fh.x * 0.5f;
+  const float2 r0 = mul2(mul2(bc2(p3.x), cd), cd);  // w00, w02
+  const float2 r1 = mul2(mul2(bc2(f05), cd), cd);   // w10, w12
+  const float2 r2 = mul2(mul2(bc2(p3.y), cd), cd);  // w20, w22
+  const float2 m = mul2(p2, bc2(fh.y));             // w01, w21
+  w[0] = r0.x;
+  w[1] = m.x;
+  w[2] = r0.y;
+  w[3] = r1.x;
+  w[4] = fh.x * fh.y;
+  w[5] = r1.y;
+  w[6] = r2.x;
+  w[7] = m.y;
+  w[8] = r2.y;
+}
+
 // Boris push of src/prtls.rs:412-440 given the gathered fields g[0..5] = E, B.
 __device__ __forceinline__ void boris(const float (&g)[6], float beta, float alpha, float csqinv, float& px,
                                       float& py, float& pz, float& psa) {
@@ -208,15 +277,12 @@ __device__ __forceinline__ void relocate(const StepArgs& a, const SpeciesArgs& S
   }
 }
 
-// Shared-memory pitch of the E/B window: the lanes of a warp cover 32/TX tile
-// rows; a pitch congruent to TX modulo 32 puts consecutive rows on disjoint
-// banks, so every gather load of a warp is conflict-free.
-__host__ __device__ inline int eb_pitch(int TX) {
-  if (TX >= 32) return TX + 2;
-  int p = TX;
-  while (p < TX + 2) p += 32;
-  return p;
-}
+// E/B window of a tile in shared memory: (TY+2) x (TX+2) cells, one float4
+// {Ex, Ey, Ez, Bx} and one float2 {By, Bz} per cell, so a gather of one
+// neighbour cell is two vector loads.  A 128-bit load is served 8 lanes per
+// wavefront and a 64-bit load 16 lanes per wavefront; the lanes of a warp own
+// consecutive cells of a tile row, so both are conflict-free.
+__host__ __device__ inline size_t eb_floats(int TX, int TY) { return (size_t)6 * (TX + 2) * (TY + 2); }
 
 // Per-warp queues of the rare work (a particle whose half-step cell differs
 // from its owner cell deposits J elsewhere; a particle whose full-step cell
@@ -226,10 +292,9 @@ __host__ __device__ inline int eb_pitch(int TX) {
 constexpr int QCAP = 64;     // entries per queue
 constexpr int QWORDS = 7;    // words per entry
 constexpr int QWARP = 2 * QWORDS * QCAP;  // floats per warp (J queue + mover queue)
-
 __host__ __device__ inline size_t slot_smem_floats(int TX, int TY, bool push, bool move) {
   const size_t win = move ? 5 * (size_t)(TX + 4) * (TY + 4) : 0;
-  const size_t eb = push ? 6 * (size_t)eb_pitch(TX) * (TY + 2) : 0;
+  const size_t eb = push ? eb_floats(TX, TY) : 0;
   const size_t q = move ? (size_t)(TX * TY / 32) * QWARP : 0;
   return win + eb + q;
 }
@@ -241,8 +306,11 @@ __host__ __device__ inline size_t slot_smem_floats(int TX, int TY, bool push, bo
 // in their slot (in place); a particle that leaves marks its slot as a hole.
 // The warp walks its cells' slots in lock-step rounds (low range, then the top
 // range of arrivals), so the loads and stores of a round are coalesced.
+#ifndef SPX_SLOT_MIN_BLOCKS
+#define SPX_SLOT_MIN_BLOCKS 2  // resident 256-thread CTAs per SM the register budget is sized for
+#endif
 template <bool PUSH, bool MOVE>
-__global__ void __launch_bounds__(256, 2) k_slot(const __grid_constant__ StepArgs a) {
+__global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS) k_slot(const __grid_constant__ StepArgs a) {
   extern __shared__ float smem[];
   const int TC = a.TX * a.TY;
   const int tile = blockIdx.x;
@@ -261,28 +329,33 @@ __global__ void __launch_bounds__(256, 2) k_slot(const __grid_constant__ StepArg
   float* wjz = win + 2 * WN;
   float* wrho = win + 3 * WN;
   float* wdens = win + 4 * WN;
-  // E/B window: tile + 1 cell, 6 planes
-  const int PE = eb_pitch(a.TX), EY = a.TY + 2, EN = PE * EY;
-  float* ebw = smem + (MOVE ? 5 * WN : 0);
-  float* qbase = ebw + (PUSH ? 6 * EN : 0) + warp * QWARP;
+  // E/B window: tile + 1 cell
+  const int EX = a.TX + 2, EY = a.TY + 2;
+  float4* eb4 = reinterpret_cast<float4*>(smem + (MOVE ? 5 * WN : 0));  // 16-byte aligned: 5*WN is a multiple of 4
+  float2* eb2 = reinterpret_cast<float2*>(eb4 + EX * EY);
+  float* after_eb = smem + (MOVE ? 5 * WN : 0) + (PUSH ? 6 * EX * EY : 0);
+  float* qbase = after_eb + warp * QWARP;
   float* qj = qbase;                   // [QWORDS][QCAP]
   float* qm = qbase + QWORDS * QCAP;   // [QWORDS][QCAP]
   if (MOVE)
     for (int i = c; i < 5 * WN; i += TC) win[i] = 0.f;
   if (PUSH) {
-    const float* src[6] = {a.f.E[0], a.f.E[1], a.f.E[2], a.f.B[0], a.f.B[1], a.f.B[2]};
-    const int EX = a.TX + 2;
-    for (int i = c; i < 6 * EY * EX; i += TC) {
-      const int f = i / (EY * EX), k = i - f * (EY * EX);
-      const int r = k / EX, q = k - r * EX;
-      ebw[f * EN + r * PE + q] = __ldg(src[f] + (size_t)(ty * a.TY + r) * W + (tx * a.TX + q));
+    for (int i = c; i < EY * EX; i += TC) {
+      const int r = i / EX, q = i - r * EX;
+      const size_t g = (size_t)(ty * a.TY + r) * W + (tx * a.TX + q);
+      eb4[i] = make_float4(__ldg(a.f.E[0] + g), __ldg(a.f.E[1] + g), __ldg(a.f.E[2] + g), __ldg(a.f.B[0] + g));
+      eb2[i] = make_float2(__ldg(a.f.B[1] + g), __ldg(a.f.B[2] + g));
     }
   }
   __syncthreads();
-  const float* eb = ebw + ly * PE + lx;  // top-left of this cell's 3x3 neighbourhood
-  float accJ[3][9];
+  const int ebo = ly * EX + lx;  // top-left of this cell's 3x3 neighbourhood
+  float2 accJxy[9];
+  float accJz[9];
 #pragma unroll
-  for (int k = 0; k < 9; ++k) accJ[0][k] = accJ[1][k] = accJ[2][k] = 0.f;
+  for (int k = 0; k < 9; ++k) {
+    accJxy[k] = make_float2(0.f, 0.f);
+    accJz[k] = 0.f;
+  }
   const size_t gc = (size_t)tile * TC + c;
   const float half_dt = 0.5f * a.p.dt;
   const float csqinv = a.p.csqinv;
@@ -290,13 +363,13 @@ __global__ void __launch_bounds__(256, 2) k_slot(const __grid_constant__ StepArg
 
   for (int s = 0; s < a.ns; ++s) {
     const SpeciesArgs& S = a.sp[s];
-    float* __restrict__ sdx = S.dx;
-    float* __restrict__ sdy = S.dy;
-    float* __restrict__ spx = S.px;
-    float* __restrict__ spy = S.py;
-    float* __restrict__ spz = S.pz;
     const int K = S.K;
-    const size_t base = (size_t)tile * K * TC + c;
+    const size_t tb = (size_t)tile * K * TC;  // this tile's block of slots
+    float* __restrict__ sdx = S.dx + tb;
+    float* __restrict__ sdy = S.dy + tb;
+    float* __restrict__ spx = S.px + tb;
+    float* __restrict__ spy = S.py + tb;
+    float* __restrict__ spz = S.pz + tb;
     const int nlow = (int)S.nlow[gc], ntop = (int)S.top[gc];
     const int wl = __reduce_max_sync(0xffffffffu, nlow);
     const int rounds = wl + __reduce_max_sync(0xffffffffu, ntop);
@@ -348,10 +421,10 @@ __global__ void __launch_bounds__(256, 2) k_slot(const __grid_constant__ StepArg
     // software pipeline: the state of round r+1 is loaded during round r
     float ndx = 0.f, ndy = 0.f, npx = 0.f, npy = 0.f, npz = 0.f;
     bool nact = false;
-    size_t nidx = base;
+    int nidx = c;
     if (rounds > 0) {
       const int sl = slot_of(0, nact);
-      nidx = base + (size_t)sl * TC;
+      nidx = sl * TC + c;
       if (nact) {
         ndx = sdx[nidx];
         ndy = sdy[nidx];
@@ -361,12 +434,12 @@ __global__ void __launch_bounds__(256, 2) k_slot(const __grid_constant__ StepArg
       }
     }
     for (int r = 0; r < rounds; ++r) {
-      const size_t idx = nidx;
+      const int idx = nidx;
       const bool act = nact && !is_hole(ndx);
       float dx = ndx, dy = ndy, px = npx, py = npy, pz = npz;
       if (r + 1 < rounds) {
         const int sl = slot_of(r + 1, nact);
-        nidx = base + (size_t)sl * TC;
+        nidx = sl * TC + c;
         if (nact) {
           ndx = sdx[nidx];
           ndy = sdy[nidx];
@@ -382,21 +455,29 @@ __global__ void __launch_bounds__(256, 2) k_slot(const __grid_constant__ StepArg
         float psa;
         if (PUSH) {
           float w[9];
-          tsc_weights(dx, dy, w);
+          tsc_weights_x2(dx, dy, w);
+          // six running sums, neighbour cells in the reference's order w00 .. w22
           float gth[6];
 #pragma unroll
-          for (int f = 0; f < 6; ++f) {
-            const float* e = eb + f * EN;
-            float t = w[0] * e[0];
-            t += w[1] * e[1];
-            t += w[2] * e[2];
-            t += w[3] * e[PE];
-            t += w[4] * e[PE + 1];
-            t += w[5] * e[PE + 2];
-            t += w[6] * e[2 * PE];
-            t += w[7] * e[2 * PE + 1];
-            t += w[8] * e[2 * PE + 2];
-            gth[f] = t;
+          for (int k = 0; k < 9; ++k) {
+            const int o = ebo + (k / 3) * EX + (k % 3);
+            const float4 e4 = eb4[o];
+            const float2 e2 = eb2[o];
+            if (k == 0) {
+              gth[0] = w[0] * e4.x;
+              gth[1] = w[0] * e4.y;
+              gth[2] = w[0] * e4.z;
+              gth[3] = w[0] * e4.w;
+              gth[4] = w[0] * e2.x;
+              gth[5] = w[0] * e2.y;
+            } else {
+              gth[0] += w[k] * e4.x;
+              gth[1] += w[k] * e4.y;
+              gth[2] += w[k] * e4.z;
+              gth[3] += w[k] * e4.w;
+              gth[4] += w[k] * e2.x;
+              gth[5] += w[k] * e2.y;
+            }
           }
           boris(gth, beta, alpha, csqinv, px, py, pz, psa);
         } else {
@@ -412,19 +493,22 @@ __global__ void __launch_bounds__(256, 2) k_slot(const __grid_constant__ StepArg
           // first half: position, boundaries, current (src/lib.rs:480-484)
           move_half(c1, px, py, ix, iy, dx, dy);
           apply_bc(a.p, nx, ny, ix, iy, dx, px, a.derr);
-          vx = q * px * inv;
-          vy = q * py * inv;
+          {
+            const float2 vxy = mul2(mul2(bc2(q), make_float2(px, py)), bc2(inv));
+            vx = vxy.x;
+            vy = vxy.y;
+          }
           vz = q * pz * inv;
           jcross = ix != ox || iy != oy;
           if (!jcross) {
             float w[9];
-            tsc_weights(dx, dy, w);
+            tsc_weights_x2(dx, dy, w);
             // summation order of deposits is not the reference's anyway: fused multiply-add here
+            const float2 vxy = make_float2(vx, vy);
 #pragma unroll
             for (int k = 0; k < 9; ++k) {
-              accJ[0][k] = __fmaf_rn(w[k], vx, accJ[0][k]);
-              accJ[1][k] = __fmaf_rn(w[k], vy, accJ[1][k]);
-              accJ[2][k] = __fmaf_rn(w[k], vz, accJ[2][k]);
+              accJxy[k] = fma2(bc2(w[k]), vxy, accJxy[k]);
+              accJz[k] = __fmaf_rn(w[k], vz, accJz[k]);
             }
           } else {
             jxc = ix;
@@ -438,7 +522,7 @@ __global__ void __launch_bounds__(256, 2) k_slot(const __grid_constant__ StepArg
           mover = ix != ox || iy != oy;
           if (!mover) {
             float w[9];
-            tsc_weights(dx, dy, w);
+            tsc_weights_x2(dx, dy, w);
 #pragma unroll
             for (int k = 0; k < 9; ++k) accD[k] += w[k];
             sdx[idx] = dx;
@@ -477,7 +561,7 @@ __global__ void __launch_bounds__(256, 2) k_slot(const __grid_constant__ StepArg
             qm[3 * QCAP + e] = px;
             qm[4 * QCAP + e] = py;
             qm[5 * QCAP + e] = pz;
-            qm[6 * QCAP + e] = __uint_as_float(S.tag[idx]);
+            qm[6 * QCAP + e] = __uint_as_float(S.tag[tb + idx]);
           }
           nq_m += __popc(mm);
           __syncwarp();
@@ -509,9 +593,9 @@ __global__ void __launch_bounds__(256, 2) k_slot(const __grid_constant__ StepArg
     for (int r = 0; r < 3; ++r)
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        atomicAdd(wjx + bl + r * WX + k, accJ[0][r * 3 + k]);
-        atomicAdd(wjy + bl + r * WX + k, accJ[1][r * 3 + k]);
-        atomicAdd(wjz + bl + r * WX + k, accJ[2][r * 3 + k]);
+        atomicAdd(wjx + bl + r * WX + k, accJxy[r * 3 + k].x);
+        atomicAdd(wjy + bl + r * WX + k, accJxy[r * 3 + k].y);
+        atomicAdd(wjz + bl + r * WX + k, accJz[r * 3 + k]);
       }
   }
   __syncthreads();
@@ -616,36 +700,54 @@ __global__ void k_commit(uint32_t* top, uint32_t* arr, size_t ncells) {
   }
 }
 
-// Remove the holes: each thread packs its cell's particles into slots
-// 0..n-1, the low range in place first, then the top range in ascending slot
-// order (a destination never lies above its source, so nothing unread is overwritten).
-__global__ void k_compact(float* dx, float* dy, float* px, float* py, float* pz, uint32_t* tag, uint32_t* nlow,
-                          uint32_t* top, int K, int TC, size_t ncells) {
-  for (size_t gc = blockIdx.x * (size_t)blockDim.x + threadIdx.x; gc < ncells; gc += (size_t)gridDim.x * blockDim.x) {
-    const size_t tile = gc / TC;
-    const int c = (int)(gc - tile * TC);
-    const size_t base = tile * (size_t)K * TC + c;
-    const int nl = (int)nlow[gc], nt = (int)top[gc];
-    int w = 0;
-    for (int n = 0; n < nl + nt; ++n) {
-      const int slot = n < nl ? n : K - nt + (n - nl);
-      const size_t i = base + (size_t)slot * TC;
-      const float x = dx[i];
-      if (is_hole(x)) continue;
-      if (slot != w) {
-        const size_t o = base + (size_t)w * TC;
-        dx[o] = x;
-        dy[o] = dy[i];
-        px[o] = px[i];
-        py[o] = py[i];
-        pz[o] = pz[i];
-        tag[o] = tag[i];
-      }
-      ++w;
+// Remove the holes: one CTA per tile, one thread per cell, packing the cell's
+// particles into slots 0..n-1 in place: the low range in rounds shared by the
+// warp, then the top range in ascending slot order (a destination never lies
+// above its source, so nothing unread is overwritten).
+__global__ void __launch_bounds__(256) k_compact(float* dx, float* dy, float* px, float* py, float* pz,
+                                                 uint32_t* tag, uint32_t* nlow, uint32_t* top, int K) {
+  const int TC = blockDim.x, c = threadIdx.x;
+  const size_t gc = (size_t)blockIdx.x * TC + c;
+  const size_t tb = (size_t)blockIdx.x * K * TC;
+  dx += tb;
+  dy += tb;
+  px += tb;
+  py += tb;
+  pz += tb;
+  tag += tb;
+  const int nl = (int)nlow[gc], nt = (int)top[gc];
+  const int wl = __reduce_max_sync(0xffffffffu, nl);
+  const int rounds = wl + __reduce_max_sync(0xffffffffu, nt);
+  int w = 0;
+  for (int r = 0; r < rounds; ++r) {
+    bool act;
+    int slot;
+    if (r < wl) {
+      act = r < nl;
+      slot = r;
+    } else {
+      act = (r - wl) < nt;
+      slot = K - nt + (r - wl);
     }
-    nlow[gc] = (uint32_t)w;
-    top[gc] = 0;
+    if (!act) continue;
+    const int i = slot * TC + c;
+    const float x = dx[i];
+    if (is_hole(x)) continue;
+    if (slot != w) {
+      const int o = w * TC + c;
+      const float y = dy[i], u = px[i], v = py[i], z = pz[i];
+      const uint32_t t = tag[i];
+      dx[o] = x;
+      dy[o] = y;
+      px[o] = u;
+      py[o] = v;
+      pz[o] = z;
+      tag[o] = t;
+    }
+    ++w;
   }
+  nlow[gc] = (uint32_t)w;
+  top[gc] = 0;
 }
 
 static SpeciesArgs species_args(Species& sp) {
@@ -735,8 +837,7 @@ int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysPar
       ++launches;
       S.ocur ^= 1;
       if (++S.moves_since_compact >= S.compact_every) {
-        k_compact<<<(int)((pg.ncells() + 255) / 256), 256, 0, st>>>(S.dx, S.dy, S.px, S.py, S.pz, S.tag, S.nlow, S.top,
-                                                                   S.K, TC, pg.ncells());
+        k_compact<<<pg.ntiles(), TC, 0, st>>>(S.dx, S.dy, S.px, S.py, S.pz, S.tag, S.nlow, S.top, S.K);
         ++launches;
         S.moves_since_compact = 0;
       }

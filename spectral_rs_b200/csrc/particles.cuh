@@ -87,7 +87,7 @@ struct FieldPtrs {
 };
 
 // Device error word bits.
-enum : int { DERR_BOUNDS = 1, DERR_WALL = 2, DERR_OVERFLOW_LOST = 4, DERR_GAMMA = 8 };
+enum : int { DERR_BOUNDS = 1, DERR_WALL = 2, DERR_OVERFLOW_LOST = 4, DERR_GAMMA = 8, DERR_TIMEOUT = 16 };
 
 // --- split path ---------------------------------------------------------------
 // Upload: pack n particles (device arrays, cell packed ix | iy << 16) into the
