@@ -8,7 +8,8 @@ Workload (one GPU): the plain method at scale -- a 2-D periodic thermal
 electron-proton plasma on a 4096 x 1024 grid, mass ratio 64, 64 particles per
 cell per species (536,870,912 particles), Maxwellian momenta with thermal
 spread 0.05c drawn from a seed, FP32 fields and particles, 4 binomial filter
-passes per step, c = 4.5, dt = 0.1 (Courant number c dt = 0.45).  Synthetic
+passes per step, c = 3.0, dt = 0.1 (Courant number c dt = 0.3; the reference
+algorithm is numerically unstable for this plasma at c dt = 0.45).  Synthetic
 data from the build's own seeded generator; a "step" is one iteration of the
 reference's loop (zero sources, move + deposit both species, ghost fold,
 Flds::update, Boris push).  The particle arrays (13 GB) exceed the 126 MB L2,
@@ -42,7 +43,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = dict(name="thermal_ep_4096x1024_ppc64", size_x=4096, size_y=1024, delta=0, dt=0.1, c=4.5, dens=64,
+WORKLOAD = dict(name="thermal_ep_4096x1024_ppc64", size_x=4096, size_y=1024, delta=0, dt=0.1, c=3.0, dens=64,
                 n_pass=4, mass_ratio=64.0, vth=0.05, ppc=64)
 CROP = dict(size_x=512, size_y=256)  # CPU sample of the same plasma
 FALLBACK_HBM_GBS = 6650.0
@@ -349,6 +350,97 @@ def run_gpu(args, w):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------- batched uneven ensemble
+ENSEMBLE_SEED = 4242
+ENSEMBLE_GRIDS = ((128, 128), (256, 128), (512, 256), (1024, 256))
+
+
+def ensemble_members(n=64, seed=ENSEMBLE_SEED):
+    """BASELINE configuration 4, drawn from a fixed seed: shocks against the
+    reflecting wall, grids from ENSEMBLE_GRIDS, ppc in [4, 32], mass ratio in
+    {1, 16, 64}, upstream drift uniform in [0.05c, 0.3c], thermal spread 0.1c."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        nx, ny = ENSEMBLE_GRIDS[rng.integers(len(ENSEMBLE_GRIDS))]
+        beta = float(rng.uniform(0.05, 0.3))
+        out.append(dict(size_x=nx, size_y=ny, ppc=int(rng.integers(4, 33)),
+                        mass_ratio=float(rng.choice([1.0, 16.0, 64.0])), beta=beta,
+                        gamma=1.0 / np.sqrt(1.0 - beta * beta)))
+    return out
+
+
+def ensemble_config(m):
+    from spectral_rs_b200.config import Config, Params, Setup, Output
+    p = Params(size_x=m["size_x"], size_y=m["size_y"], delta=8, dt=0.1, c=3.0, dens=m["ppc"],
+               gamma_inj=m["gamma"], n_pass=4, mass_ratio=m["mass_ratio"], vth=0.1, periodic_x=False,
+               left_wall=True)
+    return Config(p, Setup(0), Output(False, False, 1, 1, 1, 1))
+
+
+def run_ensemble(args):
+    import torch
+    from spectral_rs_b200 import Batch, Sim
+    members = ensemble_members(args.ensemble)
+    cfgs = [ensemble_config(m) for m in members]
+    b = Batch(cfgs)
+    for k, (sim, m) in enumerate(zip(b.sims, members)):
+        x0, x1 = 8, m["size_x"] - 8
+        sim.init_species(1.0, m["mass_ratio"], 0.1, m["ppc"], x0, x1, m["gamma"], 1.0, True, 2 * k + 1)
+        sim.init_species(-1.0, 1.0, 0.1, m["ppc"], x0, x1, m["gamma"], 1.0, True, 2 * k + 2)
+    n_particles = sum(len(p) for s in b.sims for p in s.prtls)
+    b.prepare()
+    b.step(args.warmup)
+    stream = torch.cuda.ExternalStream(b.stream())
+    torch.cuda.synchronize()
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    launches = b.last_launch_count()
+    b.set_timing(True)
+    b.step(3)
+    part_ms, step_ms = (float(x) / 3 for x in b.timing())
+    b.close()
+    value = n_particles * args.steps / (ms / 1e3)
+    # the plain single-simulation FP32 path on the same members, one after the other
+    plain_ms = 0.0
+    if not args.no_plain:
+        for k, (cfg, m) in enumerate(zip(cfgs, members)):
+            s = Sim(cfg, path="plain")
+            x0, x1 = 8, m["size_x"] - 8
+            s.init_species(1.0, m["mass_ratio"], 0.1, m["ppc"], x0, x1, m["gamma"], 1.0, True, 2 * k + 1)
+            s.init_species(-1.0, 1.0, 0.1, m["ppc"], x0, x1, m["gamma"], 1.0, True, 2 * k + 2)
+            s.prepare()
+            s.step(1)
+            st = torch.cuda.ExternalStream(s.stream())
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(st)
+            s.step(args.plain_steps)
+            a1.record(st)
+            a1.synchronize()
+            plain_ms += a0.elapsed_time(a1) / args.plain_steps
+            s.close()
+    line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded device init)",
+            "config": {"workload": f"ensemble_{args.ensemble}_shocks", "seed": ENSEMBLE_SEED,
+                       "particles": n_particles, "grids": [[m["size_x"], m["size_y"]] for m in members],
+                       "path": "split, batched (persistent work-queue particle kernel, one graph per step)"},
+            "phase_ms_per_step": {"particles": part_ms, "step": step_ms}, "gpu_launches": launches,
+            "clocks": clocks}
+    if plain_ms:
+        line["plain_fp32"] = {"value": n_particles / (plain_ms / 1e3), "unit": "particle-steps/s",
+                              "ms_per_step": plain_ms, "path": "plain FP32, one simulation after another"}
+        line["split_vs_plain"] = value / line["plain_fp32"]["value"]
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -362,7 +454,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--small", action="store_true", help="1/16 of the workload (quick checks)")
+    ap.add_argument("--workload", default="thermal", choices=["thermal", "ensemble"])
+    ap.add_argument("--ensemble", type=int, default=64, help="members of the batched ensemble")
     args = ap.parse_args()
+    if args.workload == "ensemble":
+        run_ensemble(args)
+        return
     w = dict(WORKLOAD)
     if args.small:
         w.update(size_x=1024, size_y=256, name="thermal_ep_1024x256_ppc64")

@@ -192,6 +192,31 @@ SPX_API int spx_get_counters(const spx_ctx* ctx, uint64_t* out8);
 /* Number of kernel launches issued by the last spx_step call. */
 SPX_API uint64_t spx_last_launch_count(const spx_ctx* ctx);
 
+/* ---- Batches of independent simulations ------------------------------------
+ * Many simulations with their own grids, species and parameters (BASELINE
+ * configuration 4: uneven ensembles) advance together: the particle phase of
+ * all of them is one persistent kernel over a work queue of (simulation, tile)
+ * items ordered by decreasing work, the field phase of each runs on its own
+ * stream, and one step of the batch is one CUDA graph launch.  There is no
+ * counterpart in the reference (one simulation per process).
+ * spx_batch_sim returns the context of simulation i, used as any spx_ctx for
+ * species set-up (spx_add_species / spx_init_species) and for getters; after
+ * spx_batch_prepare the simulations must only be stepped through the batch.
+ * All simulations use the same tile shape (16 x 16 unless params set one). */
+typedef struct spx_batch spx_batch;
+SPX_API int spx_batch_create(int32_t n_sims, const spx_params* params, spx_batch** out);
+SPX_API int spx_batch_destroy(spx_batch* batch);
+SPX_API const char* spx_batch_last_error(const spx_batch* batch);
+SPX_API spx_ctx* spx_batch_sim(spx_batch* batch, int32_t sim);
+SPX_API int spx_batch_prepare(spx_batch* batch);
+SPX_API int spx_batch_step(spx_batch* batch, uint32_t n);
+/* Timing (CUDA events, uncaptured steps when enabled): out2[0] particle phase,
+ * out2[1] whole steps, ms summed over the last spx_batch_step call. */
+SPX_API int spx_batch_set_timing(spx_batch* batch, int32_t enable);
+SPX_API int spx_batch_get_timing(spx_batch* batch, float* out2);
+SPX_API void* spx_batch_get_stream(const spx_batch* batch);
+SPX_API uint64_t spx_batch_last_launch_count(const spx_batch* batch);
+
 /* Allocation-free binomial filter, for callers that cannot call cudaMalloc:
  * a host loop that must not synchronize the device (cudaMalloc/cudaFree do),
  * a framework that hands out memory only from its own pool, or a driver that

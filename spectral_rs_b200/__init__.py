@@ -6,8 +6,8 @@ reference's Sim / Prtl / Flds API, its config.toml schema and its save layout.
 """
 from . import _lib
 from .config import Config, ConfigError, Params, Setup, Output, SpeciesSpec
-from .sim import Sim, Flds, Prtl, run
+from .sim import Sim, Flds, Prtl, Batch, run
 from .save import save_output
 
-__all__ = ["Config", "ConfigError", "Params", "Setup", "Output", "SpeciesSpec", "Sim", "Flds", "Prtl", "run",
+__all__ = ["Config", "ConfigError", "Params", "Setup", "Output", "SpeciesSpec", "Sim", "Flds", "Prtl", "Batch", "run",
            "save_output", "_lib"]

@@ -30,6 +30,9 @@ EXPORTS = [
     "spx_get_field", "spx_set_field", "spx_get_bwrk", "spx_set_bwrk", "spx_diag",
     "spx_field_op", "spx_fft2d", "spx_set_timing", "spx_get_timing", "spx_last_launch_count",
     "spx_get_stream", "spx_get_counters", "spx_filter_noalloc", "spx_noalloc_last_error",
+    "spx_batch_create", "spx_batch_destroy", "spx_batch_last_error", "spx_batch_sim", "spx_batch_prepare",
+    "spx_batch_step", "spx_batch_set_timing", "spx_batch_get_timing", "spx_batch_get_stream",
+    "spx_batch_last_launch_count",
 ]
 
 
@@ -103,6 +106,16 @@ def load():
         "spx_get_counters": (ctypes.c_int, [P, P]),
         "spx_filter_noalloc": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, P, P, P]),
         "spx_noalloc_last_error": (ctypes.c_char_p, []),
+        "spx_batch_create": (ctypes.c_int, [ctypes.c_int32, P, ctypes.POINTER(P)]),
+        "spx_batch_destroy": (ctypes.c_int, [P]),
+        "spx_batch_last_error": (ctypes.c_char_p, [P]),
+        "spx_batch_sim": (ctypes.c_void_p, [P, ctypes.c_int32]),
+        "spx_batch_prepare": (ctypes.c_int, [P]),
+        "spx_batch_step": (ctypes.c_int, [P, ctypes.c_uint32]),
+        "spx_batch_set_timing": (ctypes.c_int, [P, ctypes.c_int32]),
+        "spx_batch_get_timing": (ctypes.c_int, [P, P]),
+        "spx_batch_get_stream": (ctypes.c_void_p, [P]),
+        "spx_batch_last_launch_count": (ctypes.c_uint64, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

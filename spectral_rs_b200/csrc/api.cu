@@ -147,6 +147,7 @@ extern "C" int spx_create(const spx_params* p, spx_ctx** out) {
     SPX_CUDA_TRY(cudaMalloc(&c->d_u32, 8 * sizeof(uint32_t)));
     SPX_CUDA_TRY(cudaMalloc(&c->d_counts, c->pg.ncells() * sizeof(uint32_t)));
     slot_set_kernel_attributes();
+    fields_set_kernel_attributes();
   } catch (const spx::Error& e) {
     spx_destroy(c);
     return fail(nullptr, e.code, e.msg);
@@ -231,6 +232,9 @@ static int choose_K(spx_ctx* c, uint64_t n) {
   // room for Poisson-like fluctuations of the occupancy; the overflow list and
   // repack handle anything beyond
   int K = (int)std::ceil(std::max(1.25 * mx, mean + 8.0 * std::sqrt(mean))) + 8;
+  // a reflecting wall piles incoming and reflected particles up (a shock
+  // compresses the plasma about fourfold): leave room for that from the start
+  if (!c->prm.periodic_x) K = std::max(K, (int)std::ceil(4.0 * mx + 8.0 * std::sqrt(4.0 * mx)) + 8);
   if (c->prm.slot_capacity > 0) K = std::max(K, c->prm.slot_capacity);
   return K;
 }
@@ -894,6 +898,7 @@ extern "C" int spx_fft2d(uint64_t nx, uint64_t ny, int32_t inverse, float* data)
     make_twiddles((int)ny, t.data());
     SPX_CUDA_TRY(cudaMemcpy(ty, t.data(), ny * 8, cudaMemcpyHostToDevice));
     SPX_CUDA_TRY(cudaMemcpy(d, data, bytes, cudaMemcpyHostToDevice));
+    fields_set_kernel_attributes();
     fft2d_inplace(g, d, tx, ty, inverse != 0, 0);
     SPX_CUDA_TRY(cudaMemcpy(data, d, bytes, cudaMemcpyDeviceToHost));
     cudaFree(d);
@@ -904,3 +909,256 @@ extern "C" int spx_fft2d(uint64_t nx, uint64_t ny, int32_t inverse, float* data)
   }
   return SPX_OK;
 }
+
+// ======================================================================
+// Batches of independent simulations (uneven grids and particle counts).
+// The particle phase of every simulation is one persistent launch over a
+// work queue of (simulation, tile) items; the field phase of each simulation
+// runs on its own stream; one step of the whole batch is one CUDA graph.
+// ======================================================================
+struct spx_batch {
+  std::vector<spx_ctx*> sims;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_join;
+  SlotBatch sb;
+  bool built = false;
+  std::map<uint32_t, cudaGraphExec_t> graphs;
+  std::string err;
+  bool timing = false;
+  cudaEvent_t t0 = nullptr, t1 = nullptr, t2 = nullptr;
+  float last_ms[2] = {0, 0};  // particle phase, whole step (summed over the last call)
+  uint64_t last_launches = 0;
+};
+
+static int bfail(spx_batch* b, int code, const std::string& m) {
+  if (b) b->err = m;
+  else g_create_err = m;
+  return code;
+}
+
+static std::vector<SlotBatchSim> batch_sims(spx_batch* b) {
+  std::vector<SlotBatchSim> v;
+  for (spx_ctx* c : b->sims) {
+    SlotBatchSim m;
+    m.sp = c->species.data();
+    m.ns = (int)c->species.size();
+    m.pg = c->pg;
+    m.pp = c->pp;
+    m.fp = field_ptrs(c);
+    m.derr = c->d_err;
+    v.push_back(m);
+  }
+  return v;
+}
+
+extern "C" int spx_batch_create(int32_t n, const spx_params* params, spx_batch** out) {
+  if (!out || !params || n <= 0) return bfail(nullptr, SPX_ERR_ARG, "bad batch arguments");
+  *out = nullptr;
+  spx_batch* b = new spx_batch();
+  try {
+    for (int i = 0; i < n; ++i) {
+      spx_params p = params[i];
+      if (p.path == SPX_PATH_PLAIN) throw spx::Error(SPX_ERR_ARG, "a batch runs the split path");
+      if (p.tile_x <= 0 && p.tile_y <= 0) p.tile_x = p.tile_y = 16;  // one tile shape for the whole batch
+      spx_ctx* c = nullptr;
+      int rc = spx_create(&p, &c);
+      if (rc) throw spx::Error(rc, std::string("simulation ") + std::to_string(i) + ": " + g_create_err);
+      b->sims.push_back(c);
+      if (c->pg.TX != b->sims[0]->pg.TX || c->pg.TY != b->sims[0]->pg.TY)
+        throw spx::Error(SPX_ERR_ARG, "all simulations of a batch need the same tile shape");
+    }
+    SPX_CUDA_TRY(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
+    SPX_CUDA_TRY(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+    b->ev_join.resize(n);
+    for (auto& e : b->ev_join) SPX_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    SPX_CUDA_TRY(cudaEventCreate(&b->t0));
+    SPX_CUDA_TRY(cudaEventCreate(&b->t1));
+    SPX_CUDA_TRY(cudaEventCreate(&b->t2));
+  } catch (const spx::Error& e) {
+    spx_batch_destroy(b);
+    return bfail(nullptr, e.code, e.msg);
+  }
+  *out = b;
+  return SPX_OK;
+}
+
+extern "C" int spx_batch_destroy(spx_batch* b) {
+  if (!b) return SPX_OK;
+  if (b->st) cudaStreamSynchronize(b->st);
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->sb.release();
+  for (spx_ctx* c : b->sims) spx_destroy(c);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  for (auto e : b->ev_join) cudaEventDestroy(e);
+  for (auto e : {b->t0, b->t1, b->t2})
+    if (e) cudaEventDestroy(e);
+  if (b->st) cudaStreamDestroy(b->st);
+  delete b;
+  return SPX_OK;
+}
+
+extern "C" const char* spx_batch_last_error(const spx_batch* b) { return b ? b->err.c_str() : g_create_err.c_str(); }
+
+extern "C" spx_ctx* spx_batch_sim(spx_batch* b, int32_t i) {
+  if (!b || i < 0 || i >= (int)b->sims.size()) return nullptr;
+  return b->sims[i];
+}
+
+extern "C" int spx_batch_prepare(spx_batch* b) {
+  if (!b) return SPX_ERR_ARG;
+  for (size_t i = 0; i < b->sims.size(); ++i) {
+    spx_ctx* c = b->sims[i];
+    if (c->species.empty()) return bfail(b, SPX_ERR_STATE, "simulation " + std::to_string(i) + " has no species");
+    if (int rc = spx_prepare(c)) return bfail(b, rc, "simulation " + std::to_string(i) + ": " + c->err);
+  }
+  try {
+    b->sb.release();
+    slot_batch_build(b->sb, batch_sims(b));
+    b->built = true;
+  } catch (const spx::Error& e) {
+    return bfail(b, e.code, e.msg);
+  }
+  return SPX_OK;
+}
+
+// One step of every simulation.  Returns kernel launches.
+static int batch_step_body(spx_batch* b, bool timed) {
+  int launches = 0;
+  const int n = (int)b->sims.size();
+  auto fork = [&]() {
+    SPX_CUDA_TRY(cudaEventRecord(b->ev_fork, b->st));
+    for (spx_ctx* c : b->sims) SPX_CUDA_TRY(cudaStreamWaitEvent(c->st, b->ev_fork, 0));
+  };
+  auto join = [&]() {
+    for (int i = 0; i < n; ++i) {
+      SPX_CUDA_TRY(cudaEventRecord(b->ev_join[i], b->sims[i]->st));
+      SPX_CUDA_TRY(cudaStreamWaitEvent(b->st, b->ev_join[i], 0));
+    }
+  };
+  if (timed) SPX_CUDA_TRY(cudaEventRecord(b->t0, b->st));
+  fork();
+  for (spx_ctx* c : b->sims) zero_sources(c);
+  join();
+  std::vector<SlotBatchSim> sims = batch_sims(b);
+  const SlotSpecies& S0 = b->sims[0]->species[0].slot;
+  const bool compact = S0.moves_since_compact + 1 >= S0.compact_every;
+  const bool pending = b->sims[0]->pending_push;
+  launches += slot_batch_step(b->sb, sims, pending, true, compact, b->st);
+  if (timed) SPX_CUDA_TRY(cudaEventRecord(b->t1, b->st));
+  fork();
+  for (spx_ctx* c : b->sims) {
+    launches += fold_all(c);
+    launches += field_update(c->fb, c->st);
+    c->pending_push = true;
+  }
+  join();
+  if (timed) SPX_CUDA_TRY(cudaEventRecord(b->t2, b->st));
+  return launches;
+}
+
+extern "C" int spx_batch_step(spx_batch* b, uint32_t steps) {
+  if (!b) return SPX_ERR_ARG;
+  if (!b->built) return bfail(b, SPX_ERR_STATE, "spx_batch_prepare first");
+  try {
+    // the batch advances in lock-step: same overflow parity, compaction phase and pending push
+    for (spx_ctx* c : b->sims)
+      for (auto& sp : c->species)
+        if (sp.slot.ocur != b->sims[0]->species[0].slot.ocur ||
+            sp.slot.moves_since_compact != b->sims[0]->species[0].slot.moves_since_compact ||
+            c->pending_push != b->sims[0]->pending_push)
+          return bfail(b, SPX_ERR_STATE, "simulations of the batch were stepped separately");
+    uint64_t launches = 0;
+    float acc[2] = {0, 0};
+    for (uint32_t k = 0; k < steps; ++k) {
+      if (b->timing) {
+        launches += batch_step_body(b, true);
+        SPX_CUDA_TRY(cudaEventSynchronize(b->t2));
+        float p = 0, t = 0;
+        SPX_CUDA_TRY(cudaEventElapsedTime(&p, b->t0, b->t1));
+        SPX_CUDA_TRY(cudaEventElapsedTime(&t, b->t0, b->t2));
+        acc[0] += p;
+        acc[1] += t;
+        continue;
+      }
+      const SlotSpecies& S0 = b->sims[0]->species[0].slot;
+      const uint32_t key = (uint32_t)S0.ocur | ((uint32_t)(S0.moves_since_compact + 1 >= S0.compact_every) << 1) |
+                           ((uint32_t)b->sims[0]->pending_push << 2);
+      auto it = b->graphs.find(key);
+      if (it == b->graphs.end()) {
+        std::vector<std::vector<SlotSpecies>> before;
+        std::vector<bool> pend;
+        for (spx_ctx* c : b->sims) {
+          std::vector<SlotSpecies> v;
+          for (auto& sp : c->species) v.push_back(sp.slot);
+          before.push_back(v);
+          pend.push_back(c->pending_push);
+        }
+        cudaGraph_t gr;
+        SPX_CUDA_TRY(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+        const int l = batch_step_body(b, false);
+        SPX_CUDA_TRY(cudaStreamEndCapture(b->st, &gr));
+        cudaGraphExec_t ex;
+        SPX_CUDA_TRY(cudaGraphInstantiate(&ex, gr, 0));
+        SPX_CUDA_TRY(cudaGraphDestroy(gr));
+        for (size_t i = 0; i < b->sims.size(); ++i) {
+          for (size_t s = 0; s < b->sims[i]->species.size(); ++s) b->sims[i]->species[s].slot = before[i][s];
+          b->sims[i]->pending_push = pend[i];
+        }
+        it = b->graphs.emplace(key, ex).first;
+        launches += l - 1;
+      }
+      SPX_CUDA_TRY(cudaGraphLaunch(it->second, b->st));
+      ++launches;
+      // what the captured step does to the host-side state
+      const bool compact = b->sims[0]->species[0].slot.moves_since_compact + 1 >=
+                           b->sims[0]->species[0].slot.compact_every;
+      for (spx_ctx* c : b->sims) {
+        for (auto& sp : c->species) {
+          sp.slot.ocur ^= 1;
+          sp.slot.moves_since_compact = compact ? 0 : sp.slot.moves_since_compact + 1;
+        }
+        c->pending_push = true;
+      }
+    }
+    SPX_CUDA_TRY(cudaStreamSynchronize(b->st));
+    b->last_launches = launches;
+    if (b->timing) {
+      b->last_ms[0] = acc[0];
+      b->last_ms[1] = acc[1];
+    }
+    bool repacked = false;
+    for (size_t i = 0; i < b->sims.size(); ++i) {
+      spx_ctx* c = b->sims[i];
+      if (int rc = check_device_error(c)) return bfail(b, rc, "simulation " + std::to_string(i) + ": " + c->err);
+      const uint64_t before = c->repacks;
+      maybe_repack(c);
+      repacked |= c->repacks != before;
+    }
+    if (repacked) {  // slot arrays moved: new argument tables, new graphs
+      for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+      b->graphs.clear();
+      b->sb.release();
+      slot_batch_build(b->sb, batch_sims(b));
+    }
+  } catch (const spx::Error& e) {
+    return bfail(b, e.code, e.msg);
+  }
+  return SPX_OK;
+}
+
+extern "C" int spx_batch_set_timing(spx_batch* b, int32_t enable) {
+  if (!b) return SPX_ERR_ARG;
+  b->timing = enable != 0;
+  return SPX_OK;
+}
+
+extern "C" int spx_batch_get_timing(spx_batch* b, float* out2) {
+  if (!b || !out2) return SPX_ERR_ARG;
+  out2[0] = b->last_ms[0];
+  out2[1] = b->last_ms[1];
+  return SPX_OK;
+}
+
+extern "C" void* spx_batch_get_stream(const spx_batch* b) { return b ? (void*)b->st : nullptr; }
+extern "C" uint64_t spx_batch_last_launch_count(const spx_batch* b) { return b ? b->last_launches : 0; }

@@ -432,17 +432,22 @@ void launch_filter_pass(const Grid& g, float* const* src, float* const* dst, int
   k_filter<<<grd, blk, 0, st>>>(S, D, g);
 }
 
+// Dynamic shared memory above 48 KB must be opted into once per kernel (on
+// every device that runs it; done when a context is created, never while a
+// stream is being captured).
+void fields_set_kernel_attributes() {
+  for (const void* f : {(const void*)k_rows<0, 0, false>, (const void*)k_rows<1, 0, false>,
+                        (const void*)k_rows<1, 0, true>, (const void*)k_rows<1, 1, true>, (const void*)k_cols<false>,
+                        (const void*)k_cols<true>})
+    SPX_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+}
+
 template <int IN, int OUT, bool INV>
 static void launch_rows(const Grid& g, const RowArgs& a, int nf, const float2* tw, cudaStream_t st) {
   const int logB = row_logB(g.log2nx);
   const int threads = std::max(1, (g.nx << logB) / 8);
   const size_t smem = sizeof(float2) * ((size_t)g.nx << logB);
   const int blocks = (g.ny + (1 << logB) - 1) >> logB;
-  static bool attr_set = false;
-  if (!attr_set) {
-    SPX_CUDA_TRY(cudaFuncSetAttribute(k_rows<IN, OUT, INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
-    attr_set = true;
-  }
   k_rows<IN, OUT, INV><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
 }
 
@@ -452,11 +457,6 @@ static void launch_cols(const Grid& g, const ColArgs& a, int nf, const float2* t
   const int threads = std::max(1, (g.ny << logW) / 8);
   const size_t smem = sizeof(float2) * ((size_t)g.ny << logW);
   const int blocks = g.nx >> logW;
-  static bool attr_set = false;
-  if (!attr_set) {
-    SPX_CUDA_TRY(cudaFuncSetAttribute(k_cols<INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
-    attr_set = true;
-  }
   k_cols<INV><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
 }
 

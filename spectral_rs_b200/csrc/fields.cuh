@@ -38,6 +38,7 @@ int field_update(FieldBuffers& fb, cudaStream_t st);
 // Fft2D::fft / inv_fft on one complex array in place (tests).
 int fft2d_inplace(const Grid& g, float2* data, const float2* tw_x, const float2* tw_y, bool inverse,
                   cudaStream_t st);
+void fields_set_kernel_attributes();
 // Host generation of the FP64 twiddle table exp(-2 pi i m / n), m in [0, n).
 void make_twiddles(int n, float2* host_out);
 bool is_pow2(uint64_t v);

@@ -310,10 +310,8 @@ __host__ __device__ inline size_t slot_smem_floats(int TX, int TY, bool push, bo
 #define SPX_SLOT_MIN_BLOCKS 2  // resident 256-thread CTAs per SM the register budget is sized for
 #endif
 template <bool PUSH, bool MOVE>
-__global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS) k_slot(const __grid_constant__ StepArgs a) {
-  extern __shared__ float smem[];
+__device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, float* smem) {
   const int TC = a.TX * a.TY;
-  const int tile = blockIdx.x;
   const int tx = tile % a.NTX, ty = tile / a.NTX;
   const int c = threadIdx.x;
   const int lane = c & 31, warp = c >> 5;
@@ -612,11 +610,53 @@ __global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS) k_slot(const __grid_
   }
 }
 
+// One simulation: one CTA per tile.
+template <bool PUSH, bool MOVE>
+__global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS) k_slot(const __grid_constant__ StepArgs a) {
+  extern __shared__ float smem[];
+  slot_tile<PUSH, MOVE>(a, blockIdx.x, smem);
+}
+
+// Many simulations: persistent CTAs take (simulation, tile) items from a work
+// queue (an atomic counter over a list sorted by decreasing work), so uneven
+// grids and particle counts share one launch and balance across the SMs.
+template <bool PUSH, bool MOVE>
+__global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS)
+    k_slot_batch(const StepArgs* __restrict__ args, const int2* __restrict__ items, int nitems, int* counter) {
+  extern __shared__ float smem[];
+  __shared__ int s_item;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int it = s_item;
+    __syncthreads();
+    if (it >= nitems) break;
+    const int2 item = items[it];
+    slot_tile<PUSH, MOVE>(args[item.x], item.y, smem);
+    __syncthreads();  // the shared windows are reused by the next item
+  }
+}
+
 // Overflow fallback: particles parked in the overflow list (no free slot in
 // their cell) get the same per-particle work with global gathers and global
 // atomic deposits.
 template <bool PUSH, bool MOVE>
+__device__ __forceinline__ void slot_overflow(const StepArgs& a, int s);
+
+template <bool PUSH, bool MOVE>
 __global__ void k_slot_overflow(const __grid_constant__ StepArgs a, int s) {
+  slot_overflow<PUSH, MOVE>(a, s);
+}
+
+// batch form: blockIdx.y = simulation, every species of it
+template <bool PUSH, bool MOVE>
+__global__ void k_slot_overflow_batch(const StepArgs* __restrict__ args) {
+  const StepArgs& a = args[blockIdx.y];
+  for (int s = 0; s < a.ns; ++s) slot_overflow<PUSH, MOVE>(a, s);
+}
+
+template <bool PUSH, bool MOVE>
+__device__ __forceinline__ void slot_overflow(const StepArgs& a, int s) {
   const SpeciesArgs& S = a.sp[s];
   const uint32_t n = min(*S.rocount, S.ocap);
   const int W = a.g.W, nx = a.g.nx, ny = a.g.ny;
@@ -704,11 +744,11 @@ __global__ void k_commit(uint32_t* top, uint32_t* arr, size_t ncells) {
 // particles into slots 0..n-1 in place: the low range in rounds shared by the
 // warp, then the top range in ascending slot order (a destination never lies
 // above its source, so nothing unread is overwritten).
-__global__ void __launch_bounds__(256) k_compact(float* dx, float* dy, float* px, float* py, float* pz,
-                                                 uint32_t* tag, uint32_t* nlow, uint32_t* top, int K) {
+__device__ __forceinline__ void compact_tile(float* dx, float* dy, float* px, float* py, float* pz, uint32_t* tag,
+                                             uint32_t* nlow, uint32_t* top, int K, int tile) {
   const int TC = blockDim.x, c = threadIdx.x;
-  const size_t gc = (size_t)blockIdx.x * TC + c;
-  const size_t tb = (size_t)blockIdx.x * K * TC;
+  const size_t gc = (size_t)tile * TC + c;
+  const size_t tb = (size_t)tile * K * TC;
   dx += tb;
   dy += tb;
   px += tb;
@@ -750,6 +790,48 @@ __global__ void __launch_bounds__(256) k_compact(float* dx, float* dy, float* px
   top[gc] = 0;
 }
 
+__global__ void __launch_bounds__(256) k_compact(float* dx, float* dy, float* px, float* py, float* pz,
+                                                 uint32_t* tag, uint32_t* nlow, uint32_t* top, int K) {
+  compact_tile(dx, dy, px, py, pz, tag, nlow, top, K, blockIdx.x);
+}
+
+// batch: one CTA per (simulation, tile) item, every species of the simulation
+__global__ void __launch_bounds__(256) k_compact_batch(const StepArgs* __restrict__ args,
+                                                       const int2* __restrict__ items) {
+  const int2 item = items[blockIdx.x];
+  const StepArgs& a = args[item.x];
+  for (int s = 0; s < a.ns; ++s) {
+    const SpeciesArgs& S = a.sp[s];
+    compact_tile(S.dx, S.dy, S.px, S.py, S.pz, S.tag, const_cast<uint32_t*>(S.nlow), const_cast<uint32_t*>(S.top),
+                 S.K, item.y);
+  }
+}
+
+// batch: arrivals join the top ranges (blockIdx.y = simulation)
+__global__ void k_commit_batch(const StepArgs* __restrict__ args) {
+  const StepArgs& a = args[blockIdx.y];
+  const size_t n = (size_t)a.g.nx * a.g.ny;
+  for (int s = 0; s < a.ns; ++s) {
+    uint32_t* top = const_cast<uint32_t*>(a.sp[s].top);
+    uint32_t* arr = a.sp[s].arr;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+      const uint32_t v = arr[i];
+      if (v) {
+        top[i] += v;
+        arr[i] = 0;
+      }
+    }
+  }
+}
+
+// batch: clear the overflow lists the coming step writes, and the work-queue counter
+__global__ void k_batch_reset(const StepArgs* __restrict__ args, int nsims, int* counter) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *counter = 0;
+  if (i < nsims)
+    for (int s = 0; s < args[i].ns; ++s) *args[i].sp[s].wocount = 0;
+}
+
 static SpeciesArgs species_args(Species& sp) {
   SlotSpecies& s = sp.slot;
   const int r = s.ocur, w = s.ocur ^ 1;
@@ -789,7 +871,8 @@ static SpeciesArgs species_args(Species& sp) {
 
 void slot_set_kernel_attributes() {
   for (const void* f : {(const void*)k_slot<true, true>, (const void*)k_slot<true, false>,
-                        (const void*)k_slot<false, true>})
+                        (const void*)k_slot<false, true>, (const void*)k_slot_batch<true, true>,
+                        (const void*)k_slot_batch<true, false>, (const void*)k_slot_batch<false, true>})
     SPX_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
 }
 
@@ -842,6 +925,111 @@ int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysPar
         S.moves_since_compact = 0;
       }
     }
+  }
+  SPX_CUDA_TRY(cudaGetLastError());
+  return launches;
+}
+
+// ---------------------------------------------------------------- batches of simulations
+void SlotBatch::release() {
+  for (auto& p : d_args)
+    if (p) cudaFree(p), p = nullptr;
+  if (d_items) cudaFree(d_items);
+  if (d_counter) cudaFree(d_counter);
+  d_items = nullptr;
+  d_counter = nullptr;
+  nitems = 0;
+}
+
+void slot_batch_build(SlotBatch& b, const std::vector<SlotBatchSim>& sims) {
+  b.release();
+  b.nsims = (int)sims.size();
+  // work items, heaviest tiles first (particles of the simulation per tile)
+  std::vector<std::pair<double, int2>> w;
+  for (int i = 0; i < b.nsims; ++i) {
+    const SlotBatchSim& m = sims[i];
+    double per_tile = 0;
+    for (int s = 0; s < m.ns; ++s) per_tile += (double)m.sp[s].n / m.pg.ntiles();
+    for (int t = 0; t < m.pg.ntiles(); ++t) w.push_back({per_tile, make_int2(i, t)});
+  }
+  std::stable_sort(w.begin(), w.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+  std::vector<int2> items;
+  for (auto& x : w) items.push_back(x.second);
+  b.nitems = (int)items.size();
+  SPX_CUDA_TRY(cudaMalloc(&b.d_items, items.size() * sizeof(int2)));
+  SPX_CUDA_TRY(cudaMemcpy(b.d_items, items.data(), items.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  SPX_CUDA_TRY(cudaMalloc(&b.d_counter, sizeof(int)));
+  // argument tables for the two overflow-list parities (all species advance together)
+  for (int par = 0; par < 2; ++par) {
+    std::vector<StepArgs> h(b.nsims);
+    for (int i = 0; i < b.nsims; ++i) {
+      const SlotBatchSim& m = sims[i];
+      StepArgs& a = h[i];
+      a.ns = m.ns;
+      a.f = m.fp;
+      a.g = m.pg.g;
+      a.TX = m.pg.TX;
+      a.TY = m.pg.TY;
+      a.logTX = m.pg.logTX;
+      a.logTY = m.pg.logTY;
+      a.NTX = m.pg.NTX;
+      a.p = m.pp;
+      a.derr = m.derr;
+      for (int s = 0; s < m.ns; ++s) {
+        Species sp = m.sp[s];
+        sp.slot.ocur = par;
+        a.sp[s] = species_args(sp);
+      }
+    }
+    SPX_CUDA_TRY(cudaMalloc(&b.d_args[par], h.size() * sizeof(StepArgs)));
+    SPX_CUDA_TRY(cudaMemcpy(b.d_args[par], h.data(), h.size() * sizeof(StepArgs), cudaMemcpyHostToDevice));
+  }
+  const size_t smem = slot_smem_floats(sims[0].pg.TX, sims[0].pg.TY, true, true) * sizeof(float);
+  int per_sm = 0;
+  SPX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_slot_batch<true, true>, sims[0].pg.TC(), smem));
+  int dev = 0, nsm = 0;
+  SPX_CUDA_TRY(cudaGetDevice(&dev));
+  SPX_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  b.grid = std::max(1, std::min(b.nitems, std::max(per_sm, 1) * nsm));
+}
+
+int slot_batch_step(SlotBatch& b, std::vector<SlotBatchSim>& sims, bool push, bool move, bool compact,
+                    cudaStream_t st) {
+  const int par = sims[0].sp[0].slot.ocur;
+  const StepArgs* args = b.d_args[par];
+  const int TC = sims[0].pg.TC();
+  const size_t smem = slot_smem_floats(sims[0].pg.TX, sims[0].pg.TY, push, move) * sizeof(float);
+  int launches = 0;
+  k_batch_reset<<<(b.nsims + 255) / 256, 256, 0, st>>>(args, b.nsims, b.d_counter);
+  ++launches;
+  if (push && move)
+    k_slot_batch<true, true><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
+  else if (push)
+    k_slot_batch<true, false><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
+  else
+    k_slot_batch<false, true><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
+  ++launches;
+  const dim3 og(16, b.nsims);
+  if (push && move)
+    k_slot_overflow_batch<true, true><<<og, 256, 0, st>>>(args);
+  else if (push)
+    k_slot_overflow_batch<true, false><<<og, 256, 0, st>>>(args);
+  else
+    k_slot_overflow_batch<false, true><<<og, 256, 0, st>>>(args);
+  ++launches;
+  if (move) {
+    k_commit_batch<<<dim3(64, b.nsims), 256, 0, st>>>(args);
+    ++launches;
+    if (compact) {
+      k_compact_batch<<<b.nitems, TC, 0, st>>>(args, b.d_items);
+      ++launches;
+    }
+    for (auto& m : sims)
+      for (int s = 0; s < m.ns; ++s) {
+        SlotSpecies& S = m.sp[s].slot;
+        S.ocur ^= 1;
+        S.moves_since_compact = compact ? 0 : S.moves_since_compact + 1;
+      }
   }
   SPX_CUDA_TRY(cudaGetLastError());
   return launches;

@@ -1,6 +1,8 @@
 // Particle species storage and kernels of the B200 hot path (src/prtls.rs and
 // the deposition half of src/lib.rs in the reference).
 #pragma once
+#include <vector>
+
 #include "common.cuh"
 
 namespace spx {
@@ -110,6 +112,32 @@ int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysPar
 // Maximum cell occupancy (low + top range, holes included), for repack decisions.
 void slot_set_kernel_attributes();
 void slot_max_occupancy(const Species& s, const ParticleGeom& pg, uint32_t* d_out, cudaStream_t st);
+
+// --- batches of simulations (one persistent launch over a work queue) -----------
+struct StepArgs;
+struct SlotBatchSim {
+  Species* sp;  // the simulation's species array
+  int ns;
+  ParticleGeom pg;
+  PhysParams pp;
+  FieldPtrs fp;
+  int* derr;
+};
+struct SlotBatch {
+  StepArgs* d_args[2] = {nullptr, nullptr};  // per overflow-list parity
+  int2* d_items = nullptr;                   // (simulation, tile), heaviest first
+  int nitems = 0, nsims = 0, grid = 0;
+  int* d_counter = nullptr;
+  void release();
+};
+// Build the work list and argument tables (again after any repack).  All
+// simulations must share the tile shape.
+void slot_batch_build(SlotBatch& b, const std::vector<SlotBatchSim>& sims);
+// One particle phase for every simulation: reset, persistent particle kernel,
+// overflow fallback, commit and (when `compact`) compaction.  Advances the
+// host-side slot state.  Returns kernel launches.
+int slot_batch_step(SlotBatch& b, std::vector<SlotBatchSim>& sims, bool push, bool move, bool compact,
+                    cudaStream_t st);
 
 // --- plain path ---------------------------------------------------------------
 int plain_move_deposit(Species& s, uint64_t n, const ParticleGeom& pg, const PhysParams& pp, const FieldPtrs& fp,

@@ -243,3 +243,91 @@ def run(cfg: Config, out_dir="output", on_step=None):
             t = nxt
         sim.flush()
         return sim.diag()
+
+
+class _BorrowedSim(Sim):
+    """A simulation owned by a Batch: same accessors as Sim, no ownership of the context."""
+
+    def __init__(self, batch, index, cfg, ctx):
+        self.lib = _lib.load()
+        self.config = cfg
+        p = cfg.params
+        self.t = 0
+        self.t_final = cfg.setup.t_final
+        self.size_x, self.size_y, self.delta = p.size_x, p.size_y, p.delta
+        self.dt, self.c, self.dens = p.dt, p.c, p.dens
+        self.gamma_inj, self.n_pass = p.gamma_inj, p.n_pass
+        self.prtl_num = p.dens * (p.size_x - 2 * p.delta) * p.size_y
+        self._ctx = ctypes.c_void_p(ctx)
+        self.flds = Flds(self)
+        self.prtls = []
+        self.batch, self.index = batch, index
+
+    def close(self):  # the batch owns the context
+        self._ctx = ctypes.c_void_p()
+
+
+class Batch:
+    """Independent simulations advanced together (spx_batch_*): one persistent
+    particle launch over all (simulation, tile) items and one CUDA graph per step."""
+
+    def __init__(self, cfgs):
+        self.lib = _lib.load()
+        prms = (_lib.SpxParams * len(cfgs))()
+        for i, cfg in enumerate(cfgs):
+            p = cfg.params
+            prms[i] = _lib.SpxParams(
+                size_x=p.size_x, size_y=p.size_y, delta=p.delta, dt=p.dt, c=p.c, dens=p.dens,
+                gamma_inj=p.gamma_inj, n_pass=p.n_pass, periodic_x=1 if p.periodic_x else 0,
+                left_wall=1 if p.left_wall else 0, path=_lib.PATH_SPLIT, tile_x=p.tile_x, tile_y=p.tile_y,
+                slot_capacity=p.slot_capacity, device=0)
+        self._b = ctypes.c_void_p()
+        code = self.lib.spx_batch_create(len(cfgs), prms, ctypes.byref(self._b))
+        if code:
+            raise _lib.SpxError(code, self.lib.spx_batch_last_error(None).decode())
+        self.sims = [_BorrowedSim(self, i, cfg, self.lib.spx_batch_sim(self._b, i)) for i, cfg in enumerate(cfgs)]
+
+    def _chk(self, code):
+        if code:
+            raise _lib.SpxError(code, self.lib.spx_batch_last_error(self._b).decode())
+
+    def prepare(self):
+        self._chk(self.lib.spx_batch_prepare(self._b))
+
+    def step(self, n=1):
+        self._chk(self.lib.spx_batch_step(self._b, n))
+        for s in self.sims:
+            s.t += n
+
+    def set_timing(self, on=True):
+        self._chk(self.lib.spx_batch_set_timing(self._b, 1 if on else 0))
+
+    def timing(self):
+        out = np.zeros(2, dtype=np.float32)
+        self._chk(self.lib.spx_batch_get_timing(self._b, _lib.ptr(out)))
+        return out
+
+    def stream(self):
+        return int(self.lib.spx_batch_get_stream(self._b) or 0)
+
+    def last_launch_count(self):
+        return int(self.lib.spx_batch_last_launch_count(self._b))
+
+    def close(self):
+        if self._b:
+            for s in self.sims:
+                s.close()
+            self.lib.spx_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

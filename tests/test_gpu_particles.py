@@ -172,7 +172,7 @@ def test_fused_step_equals_per_phase_sequence():
 def test_run_vs_oracle(periodic, steps):
     """The full loop (src/lib.rs:130-200) against the FP32 and FP64 oracles."""
     from spectral_rs_b200 import Sim
-    cfg = _cfg(size_x=64, size_y=32, delta=0 if periodic else 6, c=4.5, dt=0.1, dens=8, periodic_x=periodic,
+    cfg = _cfg(size_x=64, size_y=32, delta=0 if periodic else 6, c=3.0, dt=0.1, dens=8, periodic_x=periodic,
                left_wall=not periodic, n_pass=4)
     p = cfg.params
     specs = [(1.0, 16.0, 0.1, _species(p, 8, 0.1, 1.0050378, 1.0, 41, random_positions=True)),

@@ -216,3 +216,31 @@ def test_gpu_deposit_sums():
         rho = sim.flds.spatial("Rho")[1:-1, 1:-1].astype(np.float64).sum()
         assert abs(dens - n) < 2e-5 * n
         assert abs(rho - (len(a["ix"]) - len(b["ix"]))) < 2e-5 * n
+
+
+def _thermal_energy_growth(c, steps):
+    """E-field energy after `steps` of a 32 x 32 thermal e-p plasma (FP64 oracle)."""
+    from spectral_rs_b200.config import Params, SpeciesSpec
+    from spectral_rs_b200.init import species_arrays
+    p = Params(size_x=32, size_y=32, delta=0, dt=0.1, c=c, dens=16, gamma_inj=1.0, n_pass=4, periodic_x=True,
+               random_positions=True, seed=3)
+    o = orc.OracleSim.from_params(p, dtype=np.float64)
+    for k, (q, m) in enumerate(((1.0, 64.0), (-1.0, 1.0))):
+        a = species_arrays(p, SpeciesSpec(charge=q, mass=m, vth=0.05, ppc=16, drift_gamma=0.0, x0=0, x1=32),
+                           seed_offset=k)
+        _add(o, q, m, 0.05, a)
+    o.prepare()
+    o.step(10)
+    e0 = sum(float(np.sum(o.spatial(n)[1:-1, 1:-1] ** 2)) for n in ("Ex", "Ey", "Ez"))
+    o.step(steps)
+    e1 = sum(float(np.sum(o.spatial(n)[1:-1, 1:-1] ** 2)) for n in ("Ex", "Ey", "Ez"))
+    return e1 / e0
+
+
+def test_courant_stability_boundary():
+    """The reference algorithm is stable at c dt = 0.3 (its own config.toml: c = 3,
+    dt = 0.1) and blows up at c dt = 0.45 (c = 4.5, dt = 0.1): with omega_pe dt =
+    0.1 the highest resolved k of the leapfrog solver leaves the stable region.
+    The benchmark workloads therefore use c = 3, dt = 0.1."""
+    assert _thermal_energy_growth(3.0, 150) < 10.0
+    assert _thermal_energy_growth(4.5, 150) > 1e6
