@@ -356,7 +356,7 @@ ENSEMBLE_GRIDS = ((128, 128), (256, 128), (512, 256), (1024, 256))
 
 
 def ensemble_members(n=64, seed=ENSEMBLE_SEED):
-    """BASELINE configuration 4, drawn from a fixed seed: shocks against the
+    """The uneven shock ensemble, drawn from a fixed seed: shocks against the
     reflecting wall, grids from ENSEMBLE_GRIDS, ppc in [4, 32], mass ratio in
     {1, 16, 64}, upstream drift uniform in [0.05c, 0.3c], thermal spread 0.1c."""
     rng = np.random.default_rng(seed)

@@ -193,8 +193,8 @@ SPX_API int spx_get_counters(const spx_ctx* ctx, uint64_t* out8);
 SPX_API uint64_t spx_last_launch_count(const spx_ctx* ctx);
 
 /* ---- Batches of independent simulations ------------------------------------
- * Many simulations with their own grids, species and parameters (BASELINE
- * configuration 4: uneven ensembles) advance together: the particle phase of
+ * Many simulations with their own grids, species and parameters (uneven
+ * ensembles, e.g. parameter scans of shocks) advance together: the particle phase of
  * all of them is one persistent kernel over a work queue of (simulation, tile)
  * items ordered by decreasing work, the field phase of each runs on its own
  * stream, and one step of the batch is one CUDA graph launch.  There is no

@@ -11,6 +11,11 @@
 
 using namespace spx;
 
+struct StepGraph {
+  cudaGraphExec_t exec;
+  int launches;  // kernel launches it holds
+};
+
 struct spx_ctx {
   spx_params prm{};
   Grid g{};
@@ -27,7 +32,7 @@ struct spx_ctx {
   bool plain = false;
   std::string err;
   // graphs of one fused step, keyed by the species' buffer parities
-  std::map<uint32_t, cudaGraphExec_t> graphs;
+  std::map<uint32_t, StepGraph> graphs;
   bool use_graphs = true;
   // timing ring
   bool timing = false;
@@ -69,7 +74,7 @@ static int check_device_error(spx_ctx* c) {
 }
 
 static void invalidate_graphs(spx_ctx* c) {
-  for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+  for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second.exec);
   c->graphs.clear();
 }
 
@@ -566,6 +571,8 @@ extern "C" int spx_fields_update(spx_ctx* c) {
   return SPX_OK;
 }
 
+static void capture_steady_state(spx_ctx* c);
+
 extern "C" int spx_prepare(spx_ctx* c) {
   if (!c) return SPX_ERR_ARG;
   SPX_GUARD(c, {
@@ -573,7 +580,8 @@ extern "C" int spx_prepare(spx_ctx* c) {
     run_move(c, 0, (int)c->species.size(), false);  // src/lib.rs:130-132
     fold_all(c);                                      // src/lib.rs:134-142
     invalidate_graphs(c);
-    return check_device_error(c);
+    if (int e = check_device_error(c)) return e;
+    capture_steady_state(c);
   });
   return SPX_OK;
 }
@@ -623,6 +631,7 @@ static void maybe_repack(spx_ctx* c) {
     SPX_CUDA_TRY(cudaFreeAsync(d_iy, c->st));
     SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
     invalidate_graphs(c);
+    capture_steady_state(c);
   }
 }
 
@@ -665,6 +674,44 @@ static uint32_t parity_key(spx_ctx* c) {
   return k;
 }
 
+// Capturing records the work of one step without running it: the host-side
+// slot state is kept as it was, and the graph is then replayed like a cached one.
+static std::map<uint32_t, StepGraph>::iterator capture_step(spx_ctx* c, uint32_t key) {
+  std::vector<SlotSpecies> before;
+  for (auto& sp : c->species) before.push_back(sp.slot);
+  cudaGraph_t gr;
+  SPX_CUDA_TRY(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+  const int l = step_body(c, false, 0);
+  SPX_CUDA_TRY(cudaStreamEndCapture(c->st, &gr));
+  cudaGraphExec_t ex;
+  SPX_CUDA_TRY(cudaGraphInstantiate(&ex, gr, 0));
+  SPX_CUDA_TRY(cudaGraphDestroy(gr));
+  for (size_t s = 0; s < c->species.size(); ++s) c->species[s].slot = before[s];
+  return c->graphs.emplace(key, StepGraph{ex, l}).first;
+}
+
+// The steady state of the split path cycles through four graphs (overflow-list
+// parity x compaction step, push pending).  Capturing all of them up front keeps
+// graph instantiation out of every later run of steps.
+static void capture_steady_state(spx_ctx* c) {
+  if (c->plain || !c->use_graphs || c->species.empty()) return;
+  std::vector<SlotSpecies> before;
+  for (auto& sp : c->species) before.push_back(sp.slot);
+  const bool pend = c->pending_push;
+  for (uint32_t oc = 0; oc < 2; ++oc)
+    for (uint32_t cp = 0; cp < 2; ++cp) {
+      for (auto& sp : c->species) {
+        sp.slot.ocur = oc;
+        sp.slot.moves_since_compact = cp ? sp.slot.compact_every - 1 : 0;
+      }
+      c->pending_push = true;
+      const uint32_t key = parity_key(c);
+      if (!c->graphs.count(key)) capture_step(c, key);
+    }
+  for (size_t s = 0; s < c->species.size(); ++s) c->species[s].slot = before[s];
+  c->pending_push = pend;
+}
+
 extern "C" int spx_step(spx_ctx* c, uint32_t n) {
   if (!c) return SPX_ERR_ARG;
   if (c->species.empty()) return fail(c, SPX_ERR_STATE, "no species");
@@ -691,22 +738,10 @@ extern "C" int spx_step(spx_ctx* c, uint32_t n) {
         const uint32_t key = parity_key(c);
         auto it = c->graphs.find(key);
         if (it == c->graphs.end()) {
-          // capturing records the work without running it: keep the host-side
-          // slot state as it was, then replay the graph like a cached one
-          std::vector<SlotSpecies> before;
-          for (auto& sp : c->species) before.push_back(sp.slot);
-          cudaGraph_t gr;
-          SPX_CUDA_TRY(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
-          const int l = step_body(c, false, 0);
-          SPX_CUDA_TRY(cudaStreamEndCapture(c->st, &gr));
-          cudaGraphExec_t ex;
-          SPX_CUDA_TRY(cudaGraphInstantiate(&ex, gr, 0));
-          SPX_CUDA_TRY(cudaGraphDestroy(gr));
-          for (size_t s = 0; s < c->species.size(); ++s) c->species[s].slot = before[s];
-          it = c->graphs.emplace(key, ex).first;
-          launches += l - 1;
+          it = capture_step(c, key);
+          launches += it->second.launches - 1;
         }
-        SPX_CUDA_TRY(cudaGraphLaunch(it->second, c->st));
+        SPX_CUDA_TRY(cudaGraphLaunch(it->second.exec, c->st));
         if (!c->plain)
           for (auto& sp : c->species) {  // what slot_step does to the host-side state
             SlotSpecies& S = sp.slot;
@@ -923,7 +958,7 @@ struct spx_batch {
   std::vector<cudaEvent_t> ev_join;
   SlotBatch sb;
   bool built = false;
-  std::map<uint32_t, cudaGraphExec_t> graphs;
+  std::map<uint32_t, StepGraph> graphs;
   std::string err;
   bool timing = false;
   cudaEvent_t t0 = nullptr, t1 = nullptr, t2 = nullptr;
@@ -964,6 +999,7 @@ extern "C" int spx_batch_create(int32_t n, const spx_params* params, spx_batch**
       spx_ctx* c = nullptr;
       int rc = spx_create(&p, &c);
       if (rc) throw spx::Error(rc, std::string("simulation ") + std::to_string(i) + ": " + g_create_err);
+      c->use_graphs = false;  // members advance through the batch's own graphs
       b->sims.push_back(c);
       if (c->pg.TX != b->sims[0]->pg.TX || c->pg.TY != b->sims[0]->pg.TY)
         throw spx::Error(SPX_ERR_ARG, "all simulations of a batch need the same tile shape");
@@ -986,7 +1022,7 @@ extern "C" int spx_batch_create(int32_t n, const spx_params* params, spx_batch**
 extern "C" int spx_batch_destroy(spx_batch* b) {
   if (!b) return SPX_OK;
   if (b->st) cudaStreamSynchronize(b->st);
-  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second.exec);
   b->sb.release();
   for (spx_ctx* c : b->sims) spx_destroy(c);
   if (b->ev_fork) cudaEventDestroy(b->ev_fork);
@@ -1005,6 +1041,8 @@ extern "C" spx_ctx* spx_batch_sim(spx_batch* b, int32_t i) {
   return b->sims[i];
 }
 
+static void capture_batch_steady_state(spx_batch* b);
+
 extern "C" int spx_batch_prepare(spx_batch* b) {
   if (!b) return SPX_ERR_ARG;
   for (size_t i = 0; i < b->sims.size(); ++i) {
@@ -1015,6 +1053,9 @@ extern "C" int spx_batch_prepare(spx_batch* b) {
   try {
     b->sb.release();
     slot_batch_build(b->sb, batch_sims(b));
+    for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second.exec);
+    b->graphs.clear();
+    capture_batch_steady_state(b);
     b->built = true;
   } catch (const spx::Error& e) {
     return bfail(b, e.code, e.msg);
@@ -1057,6 +1098,64 @@ static int batch_step_body(spx_batch* b, bool timed) {
   return launches;
 }
 
+static uint32_t batch_key(spx_batch* b) {
+  const SlotSpecies& S0 = b->sims[0]->species[0].slot;
+  return (uint32_t)S0.ocur | ((uint32_t)(S0.moves_since_compact + 1 >= S0.compact_every) << 1) |
+         ((uint32_t)b->sims[0]->pending_push << 2);
+}
+
+// As capture_step, for one step of the whole batch.
+static std::map<uint32_t, StepGraph>::iterator capture_batch_step(spx_batch* b, uint32_t key) {
+  std::vector<std::vector<SlotSpecies>> before;
+  std::vector<bool> pend;
+  for (spx_ctx* c : b->sims) {
+    std::vector<SlotSpecies> v;
+    for (auto& sp : c->species) v.push_back(sp.slot);
+    before.push_back(v);
+    pend.push_back(c->pending_push);
+  }
+  cudaGraph_t gr;
+  SPX_CUDA_TRY(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+  const int l = batch_step_body(b, false);
+  SPX_CUDA_TRY(cudaStreamEndCapture(b->st, &gr));
+  cudaGraphExec_t ex;
+  SPX_CUDA_TRY(cudaGraphInstantiate(&ex, gr, 0));
+  SPX_CUDA_TRY(cudaGraphDestroy(gr));
+  for (size_t i = 0; i < b->sims.size(); ++i) {
+    for (size_t s = 0; s < b->sims[i]->species.size(); ++s) b->sims[i]->species[s].slot = before[i][s];
+    b->sims[i]->pending_push = pend[i];
+  }
+  return b->graphs.emplace(key, StepGraph{ex, l}).first;
+}
+
+// As capture_steady_state: the four graphs of the batch's steady state.
+static void capture_batch_steady_state(spx_batch* b) {
+  std::vector<std::vector<SlotSpecies>> before;
+  std::vector<bool> pend;
+  for (spx_ctx* c : b->sims) {
+    std::vector<SlotSpecies> v;
+    for (auto& sp : c->species) v.push_back(sp.slot);
+    before.push_back(v);
+    pend.push_back(c->pending_push);
+  }
+  for (uint32_t oc = 0; oc < 2; ++oc)
+    for (uint32_t cp = 0; cp < 2; ++cp) {
+      for (spx_ctx* c : b->sims) {
+        for (auto& sp : c->species) {
+          sp.slot.ocur = oc;
+          sp.slot.moves_since_compact = cp ? sp.slot.compact_every - 1 : 0;
+        }
+        c->pending_push = true;
+      }
+      const uint32_t key = batch_key(b);
+      if (!b->graphs.count(key)) capture_batch_step(b, key);
+    }
+  for (size_t i = 0; i < b->sims.size(); ++i) {
+    for (size_t s = 0; s < b->sims[i]->species.size(); ++s) b->sims[i]->species[s].slot = before[i][s];
+    b->sims[i]->pending_push = pend[i];
+  }
+}
+
 extern "C" int spx_batch_step(spx_batch* b, uint32_t steps) {
   if (!b) return SPX_ERR_ARG;
   if (!b->built) return bfail(b, SPX_ERR_STATE, "spx_batch_prepare first");
@@ -1081,34 +1180,13 @@ extern "C" int spx_batch_step(spx_batch* b, uint32_t steps) {
         acc[1] += t;
         continue;
       }
-      const SlotSpecies& S0 = b->sims[0]->species[0].slot;
-      const uint32_t key = (uint32_t)S0.ocur | ((uint32_t)(S0.moves_since_compact + 1 >= S0.compact_every) << 1) |
-                           ((uint32_t)b->sims[0]->pending_push << 2);
+      const uint32_t key = batch_key(b);
       auto it = b->graphs.find(key);
       if (it == b->graphs.end()) {
-        std::vector<std::vector<SlotSpecies>> before;
-        std::vector<bool> pend;
-        for (spx_ctx* c : b->sims) {
-          std::vector<SlotSpecies> v;
-          for (auto& sp : c->species) v.push_back(sp.slot);
-          before.push_back(v);
-          pend.push_back(c->pending_push);
-        }
-        cudaGraph_t gr;
-        SPX_CUDA_TRY(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
-        const int l = batch_step_body(b, false);
-        SPX_CUDA_TRY(cudaStreamEndCapture(b->st, &gr));
-        cudaGraphExec_t ex;
-        SPX_CUDA_TRY(cudaGraphInstantiate(&ex, gr, 0));
-        SPX_CUDA_TRY(cudaGraphDestroy(gr));
-        for (size_t i = 0; i < b->sims.size(); ++i) {
-          for (size_t s = 0; s < b->sims[i]->species.size(); ++s) b->sims[i]->species[s].slot = before[i][s];
-          b->sims[i]->pending_push = pend[i];
-        }
-        it = b->graphs.emplace(key, ex).first;
-        launches += l - 1;
+        it = capture_batch_step(b, key);
+        launches += it->second.launches - 1;
       }
-      SPX_CUDA_TRY(cudaGraphLaunch(it->second, b->st));
+      SPX_CUDA_TRY(cudaGraphLaunch(it->second.exec, b->st));
       ++launches;
       // what the captured step does to the host-side state
       const bool compact = b->sims[0]->species[0].slot.moves_since_compact + 1 >=
@@ -1136,10 +1214,11 @@ extern "C" int spx_batch_step(spx_batch* b, uint32_t steps) {
       repacked |= c->repacks != before;
     }
     if (repacked) {  // slot arrays moved: new argument tables, new graphs
-      for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+      for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second.exec);
       b->graphs.clear();
       b->sb.release();
       slot_batch_build(b->sb, batch_sims(b));
+      capture_batch_steady_state(b);
     }
   } catch (const spx::Error& e) {
     return bfail(b, e.code, e.msg);

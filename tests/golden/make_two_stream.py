@@ -1,6 +1,6 @@
 """Field-energy histories of the two-stream precision study, FP64 and FP32 oracle.
 
-BASELINE configuration 3 (symmetric two-stream electron beams, +-0.2c along x,
+The two-stream precision workload (symmetric two-stream electron beams, +-0.2c along x,
 thermal spread 0.01c, 32 particles per cell per beam, immobile neutralizing ions
 left out: a uniform background only touches k = 0, which the solver ignores) on
 a crop small enough for the CPU oracle: 128 x 128 cells, 2000 steps, c = 3.0,
