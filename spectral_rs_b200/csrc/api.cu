@@ -218,30 +218,34 @@ __global__ void k_plain_from_cells(uint64_t n, const uint32_t* cell, const float
   }
 }
 
-static int choose_K(spx_ctx* c, uint64_t n) {
+// Slot capacity per cell: the low range KL and the arrival regions H.
+struct Capacity {
+  int KL, H;
+};
+
+static Capacity choose_capacity(spx_ctx* c, uint64_t n) {
   uint32_t mx = 0;
   SPX_CUDA_TRY(cudaMemsetAsync(c->d_u32, 0, sizeof(uint32_t), c->st));
   // max over the counts array
   Species tmp;
   tmp.slot.nlow = c->d_counts;
-  uint32_t* zeros = nullptr;
-  SPX_CUDA_TRY(cudaMallocAsync(&zeros, c->pg.ncells() * sizeof(uint32_t), c->st));
-  SPX_CUDA_TRY(cudaMemsetAsync(zeros, 0, c->pg.ncells() * sizeof(uint32_t), c->st));
-  tmp.slot.top = zeros;
   slot_max_occupancy(tmp, c->pg, c->d_u32, c->st);
   SPX_CUDA_TRY(cudaMemcpyAsync(&mx, c->d_u32, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
-  SPX_CUDA_TRY(cudaFreeAsync(zeros, c->st));
   SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
-  if (c->prm.slot_capacity < 0) return std::max((int)mx, -c->prm.slot_capacity);  // exact K (tests)
+  // exact low range and one arrival slot (tests: every step overflows)
+  if (c->prm.slot_capacity < 0) return {std::max((int)mx, -c->prm.slot_capacity), 1};
   const double mean = (double)n / (double)c->pg.ncells();
   // room for Poisson-like fluctuations of the occupancy; the overflow list and
   // repack handle anything beyond
-  int K = (int)std::ceil(std::max(1.25 * mx, mean + 8.0 * std::sqrt(mean))) + 8;
+  int KL = (int)std::ceil(std::max(1.25 * mx, mean + 8.0 * std::sqrt(mean))) + 8;
   // a reflecting wall piles incoming and reflected particles up (a shock
   // compresses the plasma about fourfold): leave room for that from the start
-  if (!c->prm.periodic_x) K = std::max(K, (int)std::ceil(4.0 * mx + 8.0 * std::sqrt(4.0 * mx)) + 8);
-  if (c->prm.slot_capacity > 0) K = std::max(K, c->prm.slot_capacity);
-  return K;
+  if (!c->prm.periodic_x) KL = std::max(KL, (int)std::ceil(4.0 * mx + 8.0 * std::sqrt(4.0 * mx)) + 8);
+  if (c->prm.slot_capacity > 0) KL = std::max(KL, c->prm.slot_capacity);
+  // arrivals of one step: a few per cent of the occupancy in a thermal plasma,
+  // a few tens in a fast flow
+  const int H = std::max(16, (KL + 3) / 4);
+  return {KL, H};
 }
 
 static int finish_species(spx_ctx* c, Species& s, Staging& st, uint64_t n, const uint32_t* d_tag) {
@@ -254,8 +258,8 @@ static int finish_species(spx_ctx* c, Species& s, Staging& st, uint64_t n, const
     SPX_CUDA_TRY(cudaMemcpyAsync(s.plain.pz, st.pz, n * 4, cudaMemcpyDeviceToDevice, c->st));
   } else {
     slot_count(c->pg, n, st.cell, c->d_counts, c->st);
-    const int K = choose_K(c, n);
-    slot_allocate(s, c->pg, K, n);
+    const Capacity cap = choose_capacity(c, n);
+    slot_allocate(s, c->pg, cap.KL, cap.H, n);
     slot_scatter(s, c->pg, n, st.cell, st.dx, st.dy, st.px, st.py, st.pz, d_tag, c->d_counts, c->st);
   }
   SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
@@ -622,10 +626,11 @@ static void maybe_repack(spx_ctx* c) {
     slot_unpack(s, c->pg, d_ix, d_iy, st.dx, st.dy, st.px, st.py, st.pz, nullptr, c->pp.csqinv, c->st);
     pack_cells(n, d_ix, d_iy, st.cell, c->st);  // cell = ix | iy << 16
     slot_count(c->pg, n, st.cell, c->d_counts, c->st);
-    int K = choose_K(c, n);
-    K = std::max(K, S.K + std::max(S.K / 2, 4));
+    Capacity cap = choose_capacity(c, n);
+    cap.KL = std::max(cap.KL, S.KL + std::max(S.KL / 2, 4));
+    cap.H = std::max(cap.H, S.H + std::max(S.H / 2, 4));
     slot_release(s);
-    slot_allocate(s, c->pg, K, n);
+    slot_allocate(s, c->pg, cap.KL, cap.H, n);
     slot_scatter(s, c->pg, n, st.cell, st.dx, st.dy, st.px, st.py, st.pz, nullptr, c->d_counts, c->st);
     SPX_CUDA_TRY(cudaFreeAsync(d_ix, c->st));
     SPX_CUDA_TRY(cudaFreeAsync(d_iy, c->st));
@@ -666,11 +671,7 @@ static int step_body(spx_ctx* c, bool timed, int slot) {
 
 static uint32_t parity_key(spx_ctx* c) {
   uint32_t k = c->pending_push ? 1u : 0u;
-  for (size_t i = 0; i < c->species.size(); ++i) {
-    const SlotSpecies& S = c->species[i].slot;
-    k |= (uint32_t)S.ocur << (2 * i + 1);
-    k |= (uint32_t)(S.moves_since_compact == S.compact_every - 1) << (2 * i + 2);
-  }
+  for (size_t i = 0; i < c->species.size(); ++i) k |= (uint32_t)c->species[i].slot.ocur << (i + 1);
   return k;
 }
 
@@ -690,24 +691,20 @@ static std::map<uint32_t, StepGraph>::iterator capture_step(spx_ctx* c, uint32_t
   return c->graphs.emplace(key, StepGraph{ex, l}).first;
 }
 
-// The steady state of the split path cycles through four graphs (overflow-list
-// parity x compaction step, push pending).  Capturing all of them up front keeps
-// graph instantiation out of every later run of steps.
+// The steady state of the split path alternates between two graphs (arrival
+// region and overflow-list parity, push pending).  Capturing both up front
+// keeps graph instantiation out of every later run of steps.
 static void capture_steady_state(spx_ctx* c) {
   if (c->plain || !c->use_graphs || c->species.empty()) return;
   std::vector<SlotSpecies> before;
   for (auto& sp : c->species) before.push_back(sp.slot);
   const bool pend = c->pending_push;
-  for (uint32_t oc = 0; oc < 2; ++oc)
-    for (uint32_t cp = 0; cp < 2; ++cp) {
-      for (auto& sp : c->species) {
-        sp.slot.ocur = oc;
-        sp.slot.moves_since_compact = cp ? sp.slot.compact_every - 1 : 0;
-      }
-      c->pending_push = true;
-      const uint32_t key = parity_key(c);
-      if (!c->graphs.count(key)) capture_step(c, key);
-    }
+  for (uint32_t oc = 0; oc < 2; ++oc) {
+    for (auto& sp : c->species) sp.slot.ocur = oc;
+    c->pending_push = true;
+    const uint32_t key = parity_key(c);
+    if (!c->graphs.count(key)) capture_step(c, key);
+  }
   for (size_t s = 0; s < c->species.size(); ++s) c->species[s].slot = before[s];
   c->pending_push = pend;
 }
@@ -743,11 +740,7 @@ extern "C" int spx_step(spx_ctx* c, uint32_t n) {
         }
         SPX_CUDA_TRY(cudaGraphLaunch(it->second.exec, c->st));
         if (!c->plain)
-          for (auto& sp : c->species) {  // what slot_step does to the host-side state
-            SlotSpecies& S = sp.slot;
-            S.ocur ^= 1;
-            if (++S.moves_since_compact >= S.compact_every) S.moves_since_compact = 0;
-          }
+          for (auto& sp : c->species) sp.slot.ocur ^= 1;  // what slot_step does to the host-side state
         launches += 1;
       }
     }
@@ -1082,10 +1075,8 @@ static int batch_step_body(spx_batch* b, bool timed) {
   for (spx_ctx* c : b->sims) zero_sources(c);
   join();
   std::vector<SlotBatchSim> sims = batch_sims(b);
-  const SlotSpecies& S0 = b->sims[0]->species[0].slot;
-  const bool compact = S0.moves_since_compact + 1 >= S0.compact_every;
   const bool pending = b->sims[0]->pending_push;
-  launches += slot_batch_step(b->sb, sims, pending, true, compact, b->st);
+  launches += slot_batch_step(b->sb, sims, pending, true, b->st);
   if (timed) SPX_CUDA_TRY(cudaEventRecord(b->t1, b->st));
   fork();
   for (spx_ctx* c : b->sims) {
@@ -1099,9 +1090,7 @@ static int batch_step_body(spx_batch* b, bool timed) {
 }
 
 static uint32_t batch_key(spx_batch* b) {
-  const SlotSpecies& S0 = b->sims[0]->species[0].slot;
-  return (uint32_t)S0.ocur | ((uint32_t)(S0.moves_since_compact + 1 >= S0.compact_every) << 1) |
-         ((uint32_t)b->sims[0]->pending_push << 2);
+  return (uint32_t)b->sims[0]->species[0].slot.ocur | ((uint32_t)b->sims[0]->pending_push << 1);
 }
 
 // As capture_step, for one step of the whole batch.
@@ -1138,18 +1127,14 @@ static void capture_batch_steady_state(spx_batch* b) {
     before.push_back(v);
     pend.push_back(c->pending_push);
   }
-  for (uint32_t oc = 0; oc < 2; ++oc)
-    for (uint32_t cp = 0; cp < 2; ++cp) {
-      for (spx_ctx* c : b->sims) {
-        for (auto& sp : c->species) {
-          sp.slot.ocur = oc;
-          sp.slot.moves_since_compact = cp ? sp.slot.compact_every - 1 : 0;
-        }
-        c->pending_push = true;
-      }
-      const uint32_t key = batch_key(b);
-      if (!b->graphs.count(key)) capture_batch_step(b, key);
+  for (uint32_t oc = 0; oc < 2; ++oc) {
+    for (spx_ctx* c : b->sims) {
+      for (auto& sp : c->species) sp.slot.ocur = oc;
+      c->pending_push = true;
     }
+    const uint32_t key = batch_key(b);
+    if (!b->graphs.count(key)) capture_batch_step(b, key);
+  }
   for (size_t i = 0; i < b->sims.size(); ++i) {
     for (size_t s = 0; s < b->sims[i]->species.size(); ++s) b->sims[i]->species[s].slot = before[i][s];
     b->sims[i]->pending_push = pend[i];
@@ -1160,12 +1145,10 @@ extern "C" int spx_batch_step(spx_batch* b, uint32_t steps) {
   if (!b) return SPX_ERR_ARG;
   if (!b->built) return bfail(b, SPX_ERR_STATE, "spx_batch_prepare first");
   try {
-    // the batch advances in lock-step: same overflow parity, compaction phase and pending push
+    // the batch advances in lock-step: same region parity and pending push
     for (spx_ctx* c : b->sims)
       for (auto& sp : c->species)
-        if (sp.slot.ocur != b->sims[0]->species[0].slot.ocur ||
-            sp.slot.moves_since_compact != b->sims[0]->species[0].slot.moves_since_compact ||
-            c->pending_push != b->sims[0]->pending_push)
+        if (sp.slot.ocur != b->sims[0]->species[0].slot.ocur || c->pending_push != b->sims[0]->pending_push)
           return bfail(b, SPX_ERR_STATE, "simulations of the batch were stepped separately");
     uint64_t launches = 0;
     float acc[2] = {0, 0};
@@ -1189,13 +1172,8 @@ extern "C" int spx_batch_step(spx_batch* b, uint32_t steps) {
       SPX_CUDA_TRY(cudaGraphLaunch(it->second.exec, b->st));
       ++launches;
       // what the captured step does to the host-side state
-      const bool compact = b->sims[0]->species[0].slot.moves_since_compact + 1 >=
-                           b->sims[0]->species[0].slot.compact_every;
       for (spx_ctx* c : b->sims) {
-        for (auto& sp : c->species) {
-          sp.slot.ocur ^= 1;
-          sp.slot.moves_since_compact = compact ? 0 : sp.slot.moves_since_compact + 1;
-        }
+        for (auto& sp : c->species) sp.slot.ocur ^= 1;
         c->pending_push = true;
       }
     }

@@ -185,15 +185,12 @@ __device__ __forceinline__ void apply_bc(const PhysParams& p, int nx, int ny, in
 }
 
 // ---------------------------------------------------------------- split path kernel
-// Slot of a particle that left its cell: dx holds this NaN bit pattern.
-constexpr uint32_t HOLE_BITS = 0xFFFFFFFFu;
-__device__ __forceinline__ bool is_hole(float dx) { return __float_as_uint(dx) == HOLE_BITS; }
-
 struct SpeciesArgs {
   float *dx, *dy, *px, *py, *pz;
   uint32_t* tag;
-  const uint32_t *nlow, *top;  // read-only during a step
-  uint32_t* arr;               // arrivals of this step (atomic)
+  uint32_t* nlow;  // low range extents: rewritten by each cell's owner during a moving step
+  uint32_t* ain;   // entries of the arrival region read this step (emptied by the owner)
+  uint32_t* aout;  // entries of the arrival region written this step (atomic)
   // overflow lists: read (r*) and write (w*)
   const uint32_t* rocell;
   float *rodx, *rody, *ropx, *ropy, *ropz;
@@ -205,7 +202,8 @@ struct SpeciesArgs {
   uint32_t* wocount;
   uint32_t ocap;
   float charge, alpha, beta;
-  int K;
+  int K, KL, H;
+  int rin, rout;  // first slot of the region read / written
 };
 
 struct StepArgs {
@@ -238,10 +236,28 @@ __device__ __forceinline__ void dep9(float* win, int WX, int WY, int wx0, int wy
   }
 }
 
-// Append a particle that left its cell to the destination cell: slot
-// K-1-(top+i) below the destination's committed top range, i from the
-// arrivals counter; the bound K - nlow - top keeps it clear of every slot the
-// destination's owner reads or writes this step.  No room: the overflow list.
+// Park a particle in the overflow list (no room in its cell); the fallback
+// kernel advances it with the rest until the host repacks.
+__device__ __forceinline__ void park(const StepArgs& a, const SpeciesArgs& S, int ix, int iy, float dx, float dy,
+                                     float px, float py, float pz, uint32_t tag) {
+  const uint32_t o = atomicAdd(S.wocount, 1u);
+  if (o < S.ocap) {
+    S.wocell[o] = (uint32_t)ix | ((uint32_t)iy << 16);
+    S.wodx[o] = dx;
+    S.wody[o] = dy;
+    S.wopx[o] = px;
+    S.wopy[o] = py;
+    S.wopz[o] = pz;
+    S.wotag[o] = tag;
+  } else {
+    atomicOr(a.derr, DERR_OVERFLOW_LOST);
+  }
+}
+
+// Append a particle that left its cell (or found its low range full) to the
+// arrival region written this step: entry i of the destination's region, i
+// from its arrivals counter.  The owner of the destination reads another
+// region and writes only below KL, so the append never meets its accesses.
 __device__ __forceinline__ void relocate(const StepArgs& a, const SpeciesArgs& S, int ix, int iy, float dx, float dy,
                                          float px, float py, float pz, uint32_t tag) {
   const int TC = a.TX * a.TY;
@@ -249,11 +265,9 @@ __device__ __forceinline__ void relocate(const StepArgs& a, const SpeciesArgs& S
   const int dc = (((iy - 1) & (a.TY - 1)) << a.logTX) | ((ix - 1) & (a.TX - 1));
   const size_t dtile = (size_t)dty * a.NTX + dtx;
   const size_t dgc = dtile * TC + dc;
-  const int top = (int)S.top[dgc];
-  const int limit = S.K - (int)S.nlow[dgc] - top;
-  const int i = (int)atomicAdd(&S.arr[dgc], 1u);
-  if (i < limit) {
-    const size_t widx = dtile * (size_t)S.K * TC + (size_t)(S.K - 1 - top - i) * TC + dc;
+  const int i = (int)atomicAdd(&S.aout[dgc], 1u);
+  if (i < S.H) {
+    const size_t widx = dtile * (size_t)S.K * TC + (size_t)(S.rout + i) * TC + dc;
     S.dx[widx] = dx;
     S.dy[widx] = dy;
     S.px[widx] = px;
@@ -261,19 +275,8 @@ __device__ __forceinline__ void relocate(const StepArgs& a, const SpeciesArgs& S
     S.pz[widx] = pz;
     S.tag[widx] = tag;
   } else {
-    atomicSub(&S.arr[dgc], 1u);
-    const uint32_t o = atomicAdd(S.wocount, 1u);
-    if (o < S.ocap) {
-      S.wocell[o] = (uint32_t)ix | ((uint32_t)iy << 16);
-      S.wodx[o] = dx;
-      S.wody[o] = dy;
-      S.wopx[o] = px;
-      S.wopy[o] = py;
-      S.wopz[o] = pz;
-      S.wotag[o] = tag;
-    } else {
-      atomicOr(a.derr, DERR_OVERFLOW_LOST);
-    }
+    atomicSub(&S.aout[dgc], 1u);
+    park(a, S, ix, iy, dx, dy, px, py, pz, tag);
   }
 }
 
@@ -299,13 +302,47 @@ __host__ __device__ inline size_t slot_smem_floats(int TX, int TY, bool push, bo
   return win + eb + q;
 }
 
+// The queue drains run rarely (once per ~32 queued particles of a warp); as
+// separate functions they keep their registers out of the main loop's budget.
+__device__ __noinline__ void drain_j_fn(const StepArgs& a, const float* qj, int nq, int lane, float* win, int WX,
+                                        int WY, int wx0, int wy0) {
+  const int WN = WX * WY, W = a.g.W;
+  for (int e = lane; e < nq; e += 32) {
+    const uint32_t cell = __float_as_uint(qj[0 * QCAP + e]);
+    const int jx = (int)(cell & 0xFFFFu), jy = (int)(cell >> 16);
+    float w[9];
+    tsc_weights(qj[1 * QCAP + e], qj[2 * QCAP + e], w);
+    dep9(win, WX, WY, wx0, wy0, a.f.J[0], W, jx, jy, w, qj[3 * QCAP + e]);
+    dep9(win + WN, WX, WY, wx0, wy0, a.f.J[1], W, jx, jy, w, qj[4 * QCAP + e]);
+    dep9(win + 2 * WN, WX, WY, wx0, wy0, a.f.J[2], W, jx, jy, w, qj[5 * QCAP + e]);
+  }
+  __syncwarp();
+}
+__device__ __noinline__ void drain_m_fn(const StepArgs& a, const SpeciesArgs& S, const float* qm, int nq, int lane,
+                                        float* win, int WX, int WY, int wx0, int wy0, float q) {
+  const int WN = WX * WY, W = a.g.W;
+  for (int e = lane; e < nq; e += 32) {
+    const uint32_t cell = __float_as_uint(qm[0 * QCAP + e]);
+    const int mx = (int)(cell & 0xFFFFu), my = (int)(cell >> 16);
+    const float mdx = qm[1 * QCAP + e], mdy = qm[2 * QCAP + e];
+    float w[9];
+    tsc_weights(mdx, mdy, w);
+    dep9(win + 3 * WN, WX, WY, wx0, wy0, a.f.dsty, W, mx, my, w, q);
+    dep9(win + 4 * WN, WX, WY, wx0, wy0, a.f.dens, W, mx, my, w, 1.0f);
+    relocate(a, S, mx, my, mdx, mdy, qm[3 * QCAP + e], qm[4 * QCAP + e], qm[5 * QCAP + e],
+             __float_as_uint(qm[6 * QCAP + e]));
+  }
+  __syncwarp();
+}
+
 // One CTA per tile, one thread per cell.  Every particle a thread processes
 // starts in the thread's cell: E/B of the tile (+1 halo) is staged once in
 // shared memory and gathered with conflict-free loads; J and rho deposits that
-// stay in the owner cell's stencil accumulate in registers.  The particles stay
-// in their slot (in place); a particle that leaves marks its slot as a hole.
-// The warp walks its cells' slots in lock-step rounds (low range, then the top
-// range of arrivals), so the loads and stores of a round are coalesced.
+// stay in the owner cell's stencil accumulate in registers.  The warp walks its
+// cells' slots in lock-step rounds (low range, then the arrival region), so
+// the loads of a round are coalesced; the particles that stay are written back
+// densely from slot 0 (a round's stores cover a few neighbouring slot rows and
+// merge in L2).
 #ifndef SPX_SLOT_MIN_BLOCKS
 #define SPX_SLOT_MIN_BLOCKS 2  // resident 256-thread CTAs per SM the register budget is sized for
 #endif
@@ -368,9 +405,12 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
     float* __restrict__ spx = S.px + tb;
     float* __restrict__ spy = S.py + tb;
     float* __restrict__ spz = S.pz + tb;
-    const int nlow = (int)S.nlow[gc], ntop = (int)S.top[gc];
+    uint32_t* __restrict__ stg = S.tag + tb;
+    const int nlow = (int)S.nlow[gc], nin = (int)S.ain[gc];
     const int wl = __reduce_max_sync(0xffffffffu, nlow);
-    const int rounds = wl + __reduce_max_sync(0xffffffffu, ntop);
+    const int rounds = wl + __reduce_max_sync(0xffffffffu, nin);
+    const int KL = S.KL, rin = S.rin;
+    int kept = 0;  // particles kept so far (moving steps): the next low-range slot
     const float q = S.charge, beta = S.beta, alpha = S.alpha;
     float accD[9];
 #pragma unroll
@@ -382,37 +422,17 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
         act = r < nlow;
         return r;
       }
-      act = (r - wl) < ntop;
-      return K - 1 - (r - wl);
+      act = (r - wl) < nin;
+      return rin + (r - wl);
     };
     // drain the J queue: deposit the stencils whose centre left the owner cell
     auto drain_j = [&]() {
-      for (int e = lane; e < nq_j; e += 32) {
-        const uint32_t cell = __float_as_uint(qj[0 * QCAP + e]);
-        const int jx = (int)(cell & 0xFFFFu), jy = (int)(cell >> 16);
-        float w[9];
-        tsc_weights(qj[1 * QCAP + e], qj[2 * QCAP + e], w);
-        dep9(wjx, WX, WY, wx0, wy0, a.f.J[0], W, jx, jy, w, qj[3 * QCAP + e]);
-        dep9(wjy, WX, WY, wx0, wy0, a.f.J[1], W, jx, jy, w, qj[4 * QCAP + e]);
-        dep9(wjz, WX, WY, wx0, wy0, a.f.J[2], W, jx, jy, w, qj[5 * QCAP + e]);
-      }
-      __syncwarp();
+      drain_j_fn(a, qj, nq_j, lane, win, WX, WY, wx0, wy0);
       nq_j = 0;
     };
     // drain the mover queue: rho/dens at the new cell, then relocation
     auto drain_m = [&]() {
-      for (int e = lane; e < nq_m; e += 32) {
-        const uint32_t cell = __float_as_uint(qm[0 * QCAP + e]);
-        const int mx = (int)(cell & 0xFFFFu), my = (int)(cell >> 16);
-        const float mdx = qm[1 * QCAP + e], mdy = qm[2 * QCAP + e];
-        float w[9];
-        tsc_weights(mdx, mdy, w);
-        dep9(wrho, WX, WY, wx0, wy0, a.f.dsty, W, mx, my, w, q);
-        dep9(wdens, WX, WY, wx0, wy0, a.f.dens, W, mx, my, w, 1.0f);
-        relocate(a, S, mx, my, mdx, mdy, qm[3 * QCAP + e], qm[4 * QCAP + e], qm[5 * QCAP + e],
-                 __float_as_uint(qm[6 * QCAP + e]));
-      }
-      __syncwarp();
+      drain_m_fn(a, S, qm, nq_m, lane, win, WX, WY, wx0, wy0, q);
       nq_m = 0;
     };
 
@@ -433,7 +453,7 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
     }
     for (int r = 0; r < rounds; ++r) {
       const int idx = nidx;
-      const bool act = nact && !is_hole(ndx);
+      const bool act = nact;
       float dx = ndx, dy = ndy, px = npx, py = npy, pz = npz;
       if (r + 1 < rounds) {
         const int sl = slot_of(r + 1, nact);
@@ -517,19 +537,22 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
           // second half: position, boundaries, density (src/lib.rs:486-488)
           move_half(c1, px, py, ix, iy, dx, dy);
           apply_bc(a.p, nx, ny, ix, iy, dx, px, a.derr);
-          mover = ix != ox || iy != oy;
+          // a particle that stays but finds the low range full joins its own
+          // cell's arrivals like a mover
+          mover = ix != ox || iy != oy || kept >= KL;
           if (!mover) {
             float w[9];
             tsc_weights_x2(dx, dy, w);
 #pragma unroll
             for (int k = 0; k < 9; ++k) accD[k] += w[k];
-            sdx[idx] = dx;
-            sdy[idx] = dy;
-            spx[idx] = px;
-            spy[idx] = py;
-            spz[idx] = pz;
-          } else {
-            sdx[idx] = __uint_as_float(HOLE_BITS);
+            const int o = kept * TC + c;
+            sdx[o] = dx;
+            sdy[o] = dy;
+            spx[o] = px;
+            spy[o] = py;
+            spz[o] = pz;
+            if (o != idx) stg[o] = stg[idx];
+            ++kept;
           }
         }
       }
@@ -559,7 +582,7 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
             qm[3 * QCAP + e] = px;
             qm[4 * QCAP + e] = py;
             qm[5 * QCAP + e] = pz;
-            qm[6 * QCAP + e] = __uint_as_float(S.tag[tb + idx]);
+            qm[6 * QCAP + e] = __uint_as_float(stg[idx]);
           }
           nq_m += __popc(mm);
           __syncwarp();
@@ -570,6 +593,8 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
     if (MOVE) {
       if (nq_j) drain_j();
       if (nq_m) drain_m();
+      S.nlow[gc] = (uint32_t)kept;
+      S.ain[gc] = 0u;
       // this species' density stencil of the owner cell -> window
       const int bl = (oy - 1 - wy0) * WX + (ox - 1 - wx0);
 #pragma unroll
@@ -729,101 +754,6 @@ __device__ __forceinline__ void slot_overflow(const StepArgs& a, int s) {
   }
 }
 
-// After a moving step: the arrivals become part of the committed top range.
-__global__ void k_commit(uint32_t* top, uint32_t* arr, size_t ncells) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < ncells; i += (size_t)gridDim.x * blockDim.x) {
-    const uint32_t a = arr[i];
-    if (a) {
-      top[i] += a;
-      arr[i] = 0;
-    }
-  }
-}
-
-// Remove the holes: one CTA per tile, one thread per cell, packing the cell's
-// particles into slots 0..n-1 in place: the low range in rounds shared by the
-// warp, then the top range in ascending slot order (a destination never lies
-// above its source, so nothing unread is overwritten).
-__device__ __forceinline__ void compact_tile(float* dx, float* dy, float* px, float* py, float* pz, uint32_t* tag,
-                                             uint32_t* nlow, uint32_t* top, int K, int tile) {
-  const int TC = blockDim.x, c = threadIdx.x;
-  const size_t gc = (size_t)tile * TC + c;
-  const size_t tb = (size_t)tile * K * TC;
-  dx += tb;
-  dy += tb;
-  px += tb;
-  py += tb;
-  pz += tb;
-  tag += tb;
-  const int nl = (int)nlow[gc], nt = (int)top[gc];
-  const int wl = __reduce_max_sync(0xffffffffu, nl);
-  const int rounds = wl + __reduce_max_sync(0xffffffffu, nt);
-  int w = 0;
-  for (int r = 0; r < rounds; ++r) {
-    bool act;
-    int slot;
-    if (r < wl) {
-      act = r < nl;
-      slot = r;
-    } else {
-      act = (r - wl) < nt;
-      slot = K - nt + (r - wl);
-    }
-    if (!act) continue;
-    const int i = slot * TC + c;
-    const float x = dx[i];
-    if (is_hole(x)) continue;
-    if (slot != w) {
-      const int o = w * TC + c;
-      const float y = dy[i], u = px[i], v = py[i], z = pz[i];
-      const uint32_t t = tag[i];
-      dx[o] = x;
-      dy[o] = y;
-      px[o] = u;
-      py[o] = v;
-      pz[o] = z;
-      tag[o] = t;
-    }
-    ++w;
-  }
-  nlow[gc] = (uint32_t)w;
-  top[gc] = 0;
-}
-
-__global__ void __launch_bounds__(256) k_compact(float* dx, float* dy, float* px, float* py, float* pz,
-                                                 uint32_t* tag, uint32_t* nlow, uint32_t* top, int K) {
-  compact_tile(dx, dy, px, py, pz, tag, nlow, top, K, blockIdx.x);
-}
-
-// batch: one CTA per (simulation, tile) item, every species of the simulation
-__global__ void __launch_bounds__(256) k_compact_batch(const StepArgs* __restrict__ args,
-                                                       const int2* __restrict__ items) {
-  const int2 item = items[blockIdx.x];
-  const StepArgs& a = args[item.x];
-  for (int s = 0; s < a.ns; ++s) {
-    const SpeciesArgs& S = a.sp[s];
-    compact_tile(S.dx, S.dy, S.px, S.py, S.pz, S.tag, const_cast<uint32_t*>(S.nlow), const_cast<uint32_t*>(S.top),
-                 S.K, item.y);
-  }
-}
-
-// batch: arrivals join the top ranges (blockIdx.y = simulation)
-__global__ void k_commit_batch(const StepArgs* __restrict__ args) {
-  const StepArgs& a = args[blockIdx.y];
-  const size_t n = (size_t)a.g.nx * a.g.ny;
-  for (int s = 0; s < a.ns; ++s) {
-    uint32_t* top = const_cast<uint32_t*>(a.sp[s].top);
-    uint32_t* arr = a.sp[s].arr;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-      const uint32_t v = arr[i];
-      if (v) {
-        top[i] += v;
-        arr[i] = 0;
-      }
-    }
-  }
-}
-
 // batch: clear the overflow lists the coming step writes, and the work-queue counter
 __global__ void k_batch_reset(const StepArgs* __restrict__ args, int nsims, int* counter) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -843,8 +773,8 @@ static SpeciesArgs species_args(Species& sp) {
   A.pz = s.pz;
   A.tag = s.tag;
   A.nlow = s.nlow;
-  A.top = s.top;
-  A.arr = s.arr;
+  A.ain = s.narr + (size_t)r * s.ncells;
+  A.aout = s.narr + (size_t)w * s.ncells;
   A.rocell = s.ocell[r];
   A.rodx = s.odx[r];
   A.rody = s.ody[r];
@@ -866,6 +796,10 @@ static SpeciesArgs species_args(Species& sp) {
   A.alpha = sp.alpha;
   A.beta = sp.beta;
   A.K = s.K;
+  A.KL = s.KL;
+  A.H = s.H;
+  A.rin = s.KL + r * s.H;
+  A.rout = s.KL + w * s.H;
   return A;
 }
 
@@ -913,19 +847,8 @@ int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysPar
       k_slot_overflow<false, true><<<64, 256, 0, st>>>(a, s);
     ++launches;
   }
-  if (move) {
-    for (int s = s0; s < s1; ++s) {
-      SlotSpecies& S = sp[s].slot;
-      k_commit<<<148 * 8, 256, 0, st>>>(S.top, S.arr, pg.ncells());
-      ++launches;
-      S.ocur ^= 1;
-      if (++S.moves_since_compact >= S.compact_every) {
-        k_compact<<<pg.ntiles(), TC, 0, st>>>(S.dx, S.dy, S.px, S.py, S.pz, S.tag, S.nlow, S.top, S.K);
-        ++launches;
-        S.moves_since_compact = 0;
-      }
-    }
-  }
+  if (move)
+    for (int s = s0; s < s1; ++s) sp[s].slot.ocur ^= 1;
   SPX_CUDA_TRY(cudaGetLastError());
   return launches;
 }
@@ -993,8 +916,7 @@ void slot_batch_build(SlotBatch& b, const std::vector<SlotBatchSim>& sims) {
   b.grid = std::max(1, std::min(b.nitems, std::max(per_sm, 1) * nsm));
 }
 
-int slot_batch_step(SlotBatch& b, std::vector<SlotBatchSim>& sims, bool push, bool move, bool compact,
-                    cudaStream_t st) {
+int slot_batch_step(SlotBatch& b, std::vector<SlotBatchSim>& sims, bool push, bool move, cudaStream_t st) {
   const int par = sims[0].sp[0].slot.ocur;
   const StepArgs* args = b.d_args[par];
   const int TC = sims[0].pg.TC();
@@ -1017,20 +939,9 @@ int slot_batch_step(SlotBatch& b, std::vector<SlotBatchSim>& sims, bool push, bo
   else
     k_slot_overflow_batch<false, true><<<og, 256, 0, st>>>(args);
   ++launches;
-  if (move) {
-    k_commit_batch<<<dim3(64, b.nsims), 256, 0, st>>>(args);
-    ++launches;
-    if (compact) {
-      k_compact_batch<<<b.nitems, TC, 0, st>>>(args, b.d_items);
-      ++launches;
-    }
+  if (move)
     for (auto& m : sims)
-      for (int s = 0; s < m.ns; ++s) {
-        SlotSpecies& S = m.sp[s].slot;
-        S.ocur ^= 1;
-        S.moves_since_compact = compact ? 0 : S.moves_since_compact + 1;
-      }
-  }
+      for (int s = 0; s < m.ns; ++s) m.sp[s].slot.ocur ^= 1;
   SPX_CUDA_TRY(cudaGetLastError());
   return launches;
 }
@@ -1057,7 +968,7 @@ __global__ void k_scatter(uint64_t n, const uint32_t* cell, const float* dx, con
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const size_t gc = cell_gc(cell[i], TX, TY, logTX, logTY, NTX);
     const uint32_t r = atomicAdd(&cursor[gc], 1u);
-    if ((int)r >= K) continue;  // cannot happen: K >= max count
+    if ((int)r >= K) continue;  // cannot happen: the low range holds the largest count
     const size_t tile = gc / TC, c = gc - tile * TC;
     const size_t o = tile * (size_t)K * TC + (size_t)r * TC + c;
     odx[o] = dx[i];
@@ -1080,14 +991,12 @@ void slot_scatter(Species& s, const ParticleGeom& pg, uint64_t n, const uint32_t
                   uint32_t* cursor, cudaStream_t st) {
   SlotSpecies& S = s.slot;
   S.ocur = 0;
-  S.moves_since_compact = 0;
   SPX_CUDA_TRY(cudaMemsetAsync(cursor, 0, pg.ncells() * sizeof(uint32_t), st));
   if (n)
     k_scatter<<<148 * 8, 256, 0, st>>>(n, cell, dx, dy, px, py, pz, tag, cursor, S.dx, S.dy, S.px, S.py, S.pz, S.tag,
                                        S.K, pg.TX, pg.TY, pg.logTX, pg.logTY, pg.NTX);
   SPX_CUDA_TRY(cudaMemcpyAsync(S.nlow, cursor, pg.ncells() * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-  SPX_CUDA_TRY(cudaMemsetAsync(S.top, 0, pg.ncells() * sizeof(uint32_t), st));
-  SPX_CUDA_TRY(cudaMemsetAsync(S.arr, 0, pg.ncells() * sizeof(uint32_t), st));
+  SPX_CUDA_TRY(cudaMemsetAsync(S.narr, 0, 2 * pg.ncells() * sizeof(uint32_t), st));
   SPX_CUDA_TRY(cudaMemsetAsync(S.ocount, 0, 2 * sizeof(uint32_t), st));
   SPX_CUDA_TRY(cudaGetLastError());
 }
@@ -1101,12 +1010,11 @@ __global__ void k_unpack(SpeciesArgs S, int TX, int TY, int logTX, int NTX, size
     const int c = (int)(gc - tile * TC);
     const int tx = (int)(tile % NTX), ty = (int)(tile / NTX);
     const uint32_t cx = tx * TX + (c & (TX - 1)) + 1, cy = ty * TY + (c >> logTX) + 1;
-    const int nlow = (int)S.nlow[gc], ntop = (int)S.top[gc];
+    const int nlow = (int)S.nlow[gc], nin = (int)S.ain[gc];
     const size_t base = tile * (size_t)S.K * TC + c;
-    for (int n = 0; n < nlow + ntop; ++n) {
-      const int slot = n < nlow ? n : S.K - 1 - (n - nlow);
+    for (int n = 0; n < nlow + nin; ++n) {
+      const int slot = n < nlow ? n : S.rin + (n - nlow);
       const size_t i = base + (size_t)slot * TC;
-      if (is_hole(S.dx[i])) continue;
       const uint32_t t = S.tag[i];
       if (ix) ix[t] = cx;
       if (iy) iy[t] = cy;
@@ -1146,34 +1054,39 @@ void slot_unpack(const Species& s, const ParticleGeom& pg, uint32_t* ix, uint32_
   SPX_CUDA_TRY(cudaGetLastError());
 }
 
-__global__ void k_max_occ(const uint32_t* nlow, const uint32_t* top, size_t n, uint32_t* out) {
+__global__ void k_max_occ(const uint32_t* nlow, const uint32_t* ain, size_t n, uint32_t* out) {
   uint32_t m = 0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    m = max(m, nlow[i] + top[i]);
+    m = max(m, nlow[i] + (ain ? ain[i] : 0u));
   for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
   if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
 void slot_max_occupancy(const Species& s, const ParticleGeom& pg, uint32_t* d_out, cudaStream_t st) {
   const SlotSpecies& S = s.slot;
-  k_max_occ<<<148 * 4, 256, 0, st>>>(S.nlow, S.top, pg.ncells(), d_out);
+  k_max_occ<<<148 * 4, 256, 0, st>>>(S.nlow, S.narr ? S.narr + (size_t)S.ocur * pg.ncells() : nullptr, pg.ncells(),
+                                     d_out);
   SPX_CUDA_TRY(cudaGetLastError());
 }
 
-void slot_allocate(Species& s, const ParticleGeom& pg, int K, uint64_t n) {
+void slot_allocate(Species& s, const ParticleGeom& pg, int KL, int H, uint64_t n) {
   SlotSpecies& S = s.slot;
+  const int K = KL + 2 * H;
   const size_t cap = pg.ncells() * (size_t)K;
   S.K = K;
+  S.KL = KL;
+  S.H = H;
+  S.ncells = pg.ncells();
   SPX_CUDA_TRY(cudaMalloc(&S.dx, cap * sizeof(float)));
   SPX_CUDA_TRY(cudaMalloc(&S.dy, cap * sizeof(float)));
   SPX_CUDA_TRY(cudaMalloc(&S.px, cap * sizeof(float)));
   SPX_CUDA_TRY(cudaMalloc(&S.py, cap * sizeof(float)));
   SPX_CUDA_TRY(cudaMalloc(&S.pz, cap * sizeof(float)));
   SPX_CUDA_TRY(cudaMalloc(&S.tag, cap * sizeof(uint32_t)));
-  for (uint32_t** p : {&S.nlow, &S.top, &S.arr}) {
-    SPX_CUDA_TRY(cudaMalloc(p, pg.ncells() * sizeof(uint32_t)));
-    SPX_CUDA_TRY(cudaMemset(*p, 0, pg.ncells() * sizeof(uint32_t)));
-  }
+  SPX_CUDA_TRY(cudaMalloc(&S.nlow, pg.ncells() * sizeof(uint32_t)));
+  SPX_CUDA_TRY(cudaMemset(S.nlow, 0, pg.ncells() * sizeof(uint32_t)));
+  SPX_CUDA_TRY(cudaMalloc(&S.narr, 2 * pg.ncells() * sizeof(uint32_t)));
+  SPX_CUDA_TRY(cudaMemset(S.narr, 0, 2 * pg.ncells() * sizeof(uint32_t)));
   S.ocap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(1u << 16, n / 32), 1u << 28);
   for (int b = 0; b < 2; ++b) {
     SPX_CUDA_TRY(cudaMalloc(&S.ocell[b], S.ocap * sizeof(uint32_t)));
@@ -1191,7 +1104,7 @@ void slot_allocate(Species& s, const ParticleGeom& pg, int K, uint64_t n) {
 void slot_release(Species& s) {
   SlotSpecies& S = s.slot;
   for (void* p : {(void*)S.dx, (void*)S.dy, (void*)S.px, (void*)S.py, (void*)S.pz, (void*)S.tag, (void*)S.nlow,
-                  (void*)S.top, (void*)S.arr})
+                  (void*)S.narr})
     if (p) cudaFree(p);
   for (int b = 0; b < 2; ++b) {
     for (void* p : {(void*)S.ocell[b], (void*)S.odx[b], (void*)S.ody[b], (void*)S.opx[b], (void*)S.opy[b],
@@ -1199,9 +1112,7 @@ void slot_release(Species& s) {
       if (p) cudaFree(p);
   }
   if (S.ocount) cudaFree(S.ocount);
-  const int ce = S.compact_every;
   S = SlotSpecies();
-  S.compact_every = ce;
 }
 
 // ---------------------------------------------------------------- plain FP32 path
@@ -1340,12 +1251,11 @@ __global__ void k_kinetic_slot(SpeciesArgs S, int TC, size_t ncells, float mass,
   for (size_t gc = blockIdx.x * (size_t)blockDim.x + threadIdx.x; gc < ncells; gc += (size_t)gridDim.x * blockDim.x) {
     const size_t tile = gc / TC;
     const int cc = (int)(gc - tile * TC);
-    const int nlow = (int)S.nlow[gc], ntop = (int)S.top[gc];
+    const int nlow = (int)S.nlow[gc], nin = (int)S.ain[gc];
     const size_t base = tile * (size_t)S.K * TC + cc;
-    for (int n = 0; n < nlow + ntop; ++n) {
-      const int slot = n < nlow ? n : S.K - 1 - (n - nlow);
+    for (int n = 0; n < nlow + nin; ++n) {
+      const int slot = n < nlow ? n : S.rin + (n - nlow);
       const size_t i = base + (size_t)slot * TC;
-      if (is_hole(S.dx[i])) continue;
       const double g = (double)gamma_of(S.px[i], S.py[i], S.pz[i], csqinv);
       e += (double)mass * (g - 1.0) * csq;
       cnt += 1.0;

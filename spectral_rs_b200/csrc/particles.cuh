@@ -18,16 +18,17 @@ constexpr int MAX_SPECIES = 4;
 // a particle is {dx, dy, px, py, pz, tag} = 24 bytes (tag = its index in the
 // reference's particle order, used only to return data in that order).
 //
-// Particles stay in their slot: a cell's particles occupy slots [0, nlow) and
-// [K - top, K).  During a step the thread that owns the cell updates every
-// particle in place; a particle that moves to another cell marks its old slot
-// as a hole and is appended below the destination's top range (slot
-// K-1-(top+i), i from an atomic arrivals counter); the bound i < K - nlow - top
-// keeps appends clear of every slot the destination's owner touches.  After
-// the step the arrivals join the top range; every `compact_every` moving steps
-// a compaction pass removes the holes.  A particle that finds no room goes to
-// the overflow list, which a fallback kernel processes every step until the
-// host repacks with a larger K.
+// The K = KL + 2H slots of a cell hold a low range [0, nlow) and two arrival
+// regions of H slots, region r = [KL + r*H, KL + (r+1)*H) with narr[r] entries.
+// A moving step with parity q (= ocur) reads the low range and region q (the
+// previous step's arrivals); the thread that owns the cell writes the
+// particles that stay, in order, to [0, w) (w never passes the slot being
+// read), so the low range stays dense: no holes, no compaction pass.  A
+// particle that leaves goes to region q^1 of its destination (slot from an
+// atomic arrivals counter, bounded by H); region q is then empty.  A particle
+// that finds no room (low range or region full) goes to the overflow list,
+// which a fallback kernel processes every step until the host repacks with a
+// larger capacity.
 struct SlotSpecies {
   float* dx = nullptr;
   float* dy = nullptr;
@@ -35,9 +36,8 @@ struct SlotSpecies {
   float* py = nullptr;
   float* pz = nullptr;
   uint32_t* tag = nullptr;
-  uint32_t* nlow = nullptr;  // low range extent per cell (holes included)
-  uint32_t* top = nullptr;   // committed top range extent per cell
-  uint32_t* arr = nullptr;   // arrivals of the running step per cell
+  uint32_t* nlow = nullptr;  // low range extent per cell
+  uint32_t* narr = nullptr;  // [2][ncells] entries of the two arrival regions
   // overflow lists (double buffered): cell packed as ix | iy << 16 (reference coords)
   uint32_t* ocell[2] = {};
   float* odx[2] = {};
@@ -48,10 +48,9 @@ struct SlotSpecies {
   uint32_t* otag[2] = {};
   uint32_t* ocount = nullptr;  // [2]
   uint32_t ocap = 0;
-  int K = 0;
-  int ocur = 0;  // overflow list read by the next step
-  int moves_since_compact = 0;
-  int compact_every = 8;
+  int K = 0, KL = 0, H = 0;
+  size_t ncells = 0;
+  int ocur = 0;  // arrival region and overflow list read by the next step
 };
 
 // Plain-path storage: global FP32 positions x = ix + dx, y = iy + dy in the
@@ -92,9 +91,9 @@ struct FieldPtrs {
 enum : int { DERR_BOUNDS = 1, DERR_WALL = 2, DERR_OVERFLOW_LOST = 4, DERR_GAMMA = 8, DERR_TIMEOUT = 16 };
 
 // --- split path ---------------------------------------------------------------
-// Upload: pack n particles (device arrays, cell packed ix | iy << 16) into the
-// slot layout with capacity K, in buffer 0.  Returns kernel launch count.
-void slot_allocate(Species& s, const ParticleGeom& pg, int K, uint64_t n);
+// Storage for n particles with a low range of KL slots and arrival regions of
+// H slots per cell.
+void slot_allocate(Species& s, const ParticleGeom& pg, int KL, int H, uint64_t n);
 void slot_release(Species& s);
 // Count particles per cell (for choosing K).  counts: ncells uint32 (zeroed inside).
 void slot_count(const ParticleGeom& pg, uint64_t n, const uint32_t* cell, uint32_t* counts, cudaStream_t st);
@@ -109,7 +108,7 @@ void slot_unpack(const Species& s, const ParticleGeom& pg, uint32_t* ix, uint32_
 // relocation.  Returns the number of kernel launches (memsets not counted).
 int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysParams& pp, const FieldPtrs& fp,
               bool push, bool move, int* derr, cudaStream_t st);
-// Maximum cell occupancy (low + top range, holes included), for repack decisions.
+// Maximum cell occupancy (low range + pending arrivals), reported with the layout counters.
 void slot_set_kernel_attributes();
 void slot_max_occupancy(const Species& s, const ParticleGeom& pg, uint32_t* d_out, cudaStream_t st);
 
@@ -134,10 +133,8 @@ struct SlotBatch {
 // simulations must share the tile shape.
 void slot_batch_build(SlotBatch& b, const std::vector<SlotBatchSim>& sims);
 // One particle phase for every simulation: reset, persistent particle kernel,
-// overflow fallback, commit and (when `compact`) compaction.  Advances the
-// host-side slot state.  Returns kernel launches.
-int slot_batch_step(SlotBatch& b, std::vector<SlotBatchSim>& sims, bool push, bool move, bool compact,
-                    cudaStream_t st);
+// overflow fallback.  Advances the host-side slot state.  Returns kernel launches.
+int slot_batch_step(SlotBatch& b, std::vector<SlotBatchSim>& sims, bool push, bool move, cudaStream_t st);
 
 // --- plain path ---------------------------------------------------------------
 int plain_move_deposit(Species& s, uint64_t n, const ParticleGeom& pg, const PhysParams& pp, const FieldPtrs& fp,
