@@ -55,6 +55,8 @@ def params(w, **over):
     from spectral_rs_b200.config import Params
     d = dict(size_x=w["size_x"], size_y=w["size_y"], delta=w["delta"], dt=w["dt"], c=w["c"], dens=w["dens"],
              gamma_inj=1.0, n_pass=w["n_pass"], mass_ratio=w["mass_ratio"], vth=w["vth"], periodic_x=True)
+    if w.get("tile"):
+        d["tile_x"], d["tile_y"] = w["tile"]
     d.update(over)
     return Params(**d)
 
@@ -455,6 +457,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--small", action="store_true", help="1/16 of the workload (quick checks)")
     ap.add_argument("--workload", default="thermal", choices=["thermal", "ensemble"])
+    ap.add_argument("--tile", default=None, help="split-path tile shape TXxTY (default: the library's choice)")
     ap.add_argument("--ensemble", type=int, default=64, help="members of the batched ensemble")
     args = ap.parse_args()
     if args.workload == "ensemble":
@@ -463,6 +466,8 @@ def main():
     w = dict(WORKLOAD)
     if args.small:
         w.update(size_x=1024, size_y=256, name="thermal_ep_1024x256_ppc64")
+    if args.tile:
+        w["tile"] = tuple(int(v) for v in args.tile.lower().split("x"))
     if args.impl == "reference":
         run_reference(args, w)
     else:

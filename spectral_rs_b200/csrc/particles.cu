@@ -98,32 +98,50 @@ __device__ __forceinline__ void tsc_weights_x2(float dx, float dy, float (&w)[9]
 }
 
 // Boris push of src/prtls.rs:412-440 given the gathered fields g[0..5] = E, B.
+// Every operation is the reference's, in its order (Rust evaluates a + b * c - d * e
+// as (a + (b*c)) - (d*e)); independent multiplications run in pairs as packed
+// FP32x2 products, and every sum that consumes a product stays scalar.
 __device__ __forceinline__ void boris(const float (&g)[6], float beta, float alpha, float csqinv, float& px,
                                       float& py, float& pz, float& psa) {
-  const float ext = g[0] * beta, eyt = g[1] * beta, ezt = g[2] * beta;
-  float bxt = g[3] * alpha, byt = g[4] * alpha, bzt = g[5] * alpha;
-  const float ux = px + ext, uy = py + eyt, uz = pz + ezt;
-  const float gt = 1.0f / sqrtf(1.0f + (ux * ux + uy * uy + uz * uz) * csqinv);
-  bxt *= gt;
-  byt *= gt;
-  bzt *= gt;
-  const float boris = 2.0f * (1.0f / (1.0f + bxt * bxt + byt * byt + bzt * bzt));
-  const float uxt = ux + uy * bzt - uz * byt;
-  const float uyt = uy + uz * bxt - ux * bzt;
-  const float uzt = uz + ux * byt - uy * bxt;
-  px = ux + boris * (uyt * bzt - uzt * byt) + ext;
-  py = uy + boris * (uzt * bxt - uxt * bzt) + eyt;
-  pz = uz + boris * (uxt * byt - uyt * bxt) + ezt;
-  psa = sqrtf(1.0f + (px * px + py * py + pz * pz) * csqinv);
+  const float2 exy = mul2(make_float2(g[0], g[1]), bc2(beta));  // (ext, eyt)
+  const float ezt = g[2] * beta;
+  const float2 bxy = mul2(make_float2(g[3], g[4]), bc2(alpha));
+  const float ux = px + exy.x, uy = py + exy.y, uz = pz + ezt;
+  const float2 uu = mul2(make_float2(ux, uy), make_float2(ux, uy));
+  const float gt = 1.0f / sqrtf(1.0f + (uu.x + uu.y + uz * uz) * csqinv);
+  const float2 bt = mul2(bxy, bc2(gt));  // (bxt, byt)
+  const float bxt = bt.x, byt = bt.y, bzt = (g[5] * alpha) * gt;
+  const float2 bb = mul2(bt, bt);
+  const float boris = 2.0f * (1.0f / (1.0f + bb.x + bb.y + bzt * bzt));
+  // u' = u + u x B
+  const float2 p1 = mul2(make_float2(uy, uz), make_float2(bzt, bxt));  // (uy bzt, uz bxt)
+  const float2 p2 = mul2(make_float2(uz, ux), make_float2(byt, bzt));  // (uz byt, ux bzt)
+  const float2 p3 = mul2(make_float2(ux, uy), make_float2(byt, bxt));  // (ux byt, uy bxt)
+  const float uxt = ux + p1.x - p2.x;
+  const float uyt = uy + p1.y - p2.y;
+  const float uzt = uz + p3.x - p3.y;
+  // p = u + boris (u' x B) + E
+  const float2 q1 = mul2(make_float2(uyt, uzt), make_float2(bzt, bxt));  // (uyt bzt, uzt bxt)
+  const float2 q2 = mul2(make_float2(uzt, uxt), make_float2(byt, bzt));  // (uzt byt, uxt bzt)
+  const float2 q3 = mul2(make_float2(uxt, uyt), make_float2(byt, bxt));  // (uxt byt, uyt bxt)
+  const float2 bxy2 = mul2(bc2(boris), make_float2(q1.x - q2.x, q1.y - q2.y));
+  const float bz2 = boris * (q3.x - q3.y);
+  px = ux + bxy2.x + exy.x;
+  py = uy + bxy2.y + exy.y;
+  pz = uz + bz2 + ezt;
+  const float2 pp = mul2(make_float2(px, py), make_float2(px, py));
+  psa = sqrtf(1.0f + (pp.x + pp.y + pz * pz) * csqinv);
 }
 
 __device__ __forceinline__ float gamma_of(float px, float py, float pz, float csqinv) {
-  return sqrtf(1.0f + (px * px + py * py + pz * pz) * csqinv);  // src/prtls.rs:440
+  const float2 pp = mul2(make_float2(px, py), make_float2(px, py));
+  return sqrtf(1.0f + (pp.x + pp.y + pz * pz) * csqinv);  // src/prtls.rs:440
 }
 
 // update_position (src/prtls.rs:103-119) for one particle; inv = 1/psa.
 __device__ __forceinline__ void move_half(float c1, float px, float py, int& ix, int& iy, float& dx, float& dy) {
-  dx += c1 * px;
+  const float2 d = mul2(bc2(c1), make_float2(px, py));
+  dx += d.x;
   if (dx >= 0.5f) {
     dx -= 1.0f;
     ix += 1;
@@ -131,7 +149,7 @@ __device__ __forceinline__ void move_half(float c1, float px, float py, int& ix,
     dx += 1.0f;
     ix -= 1;
   }
-  dy += c1 * py;
+  dy += d.y;
   if (dy >= 0.5f) {
     dy -= 1.0f;
     iy += 1;
@@ -476,27 +494,22 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
           tsc_weights_x2(dx, dy, w);
           // six running sums, neighbour cells in the reference's order w00 .. w22
           float gth[6];
+          float2 g01, g23, g45;
 #pragma unroll
           for (int k = 0; k < 9; ++k) {
             const int o = ebo + (k / 3) * EX + (k % 3);
             const float4 e4 = eb4[o];
             const float2 e2 = eb2[o];
+            const float2 p01 = make_float2(w[k] * e4.x, w[k] * e4.y);
+            const float2 p23 = make_float2(w[k] * e4.z, w[k] * e4.w);
+            const float2 p45 = make_float2(w[k] * e2.x, w[k] * e2.y);
             if (k == 0) {
-              gth[0] = w[0] * e4.x;
-              gth[1] = w[0] * e4.y;
-              gth[2] = w[0] * e4.z;
-              gth[3] = w[0] * e4.w;
-              gth[4] = w[0] * e2.x;
-              gth[5] = w[0] * e2.y;
+              g01 = p01; g23 = p23; g45 = p45;
             } else {
-              gth[0] += w[k] * e4.x;
-              gth[1] += w[k] * e4.y;
-              gth[2] += w[k] * e4.z;
-              gth[3] += w[k] * e4.w;
-              gth[4] += w[k] * e2.x;
-              gth[5] += w[k] * e2.y;
+              g01 = add2(g01, p01); g23 = add2(g23, p23); g45 = add2(g45, p45);
             }
           }
+          gth[0] = g01.x; gth[1] = g01.y; gth[2] = g23.x; gth[3] = g23.y; gth[4] = g45.x; gth[5] = g45.y;
           boris(gth, beta, alpha, csqinv, px, py, pz, psa);
         } else {
           psa = gamma_of(px, py, pz, csqinv);
