@@ -43,9 +43,33 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = dict(name="thermal_ep_4096x1024_ppc64", size_x=4096, size_y=1024, delta=0, dt=0.1, c=3.0, dens=64,
-                n_pass=4, mass_ratio=64.0, vth=0.05, ppc=64)
-CROP = dict(size_x=512, size_y=256)  # CPU sample of the same plasma
+def _sp(q, m, vth, ppc, gamma=0.0, sign=1.0):
+    return dict(q=q, m=m, vth=vth, ppc=ppc, gamma=gamma, sign=sign)
+
+
+# Workloads (species: ions first, as run() creates them, src/lib.rs:124-126).
+# c = 3.0, dt = 0.1 everywhere: Courant number c dt = 0.3 (the reference
+# algorithm is numerically unstable for these plasmas at c dt = 0.45).
+WORKLOADS = {
+    # the headline: the plain method at scale
+    "thermal": dict(name="thermal_ep_4096x1024_ppc64", size_x=4096, size_y=1024, delta=0, dt=0.1, c=3.0, dens=64,
+                    n_pass=4, periodic_x=True, left_wall=False,
+                    species=[_sp(1.0, 64.0, 0.05, 64), _sp(-1.0, 1.0, 0.05, 64)],
+                    small=(1024, 256), crop=(512, 256)),
+    # small unmagnetized shock: drift 0.1c toward the reflecting wall (the
+    # reference's wall is on the right), mirror wall on the left
+    "shock": dict(name="shock_512x64_ppc16", size_x=512, size_y=64, delta=8, dt=0.1, c=3.0, dens=16,
+                  n_pass=4, periodic_x=False, left_wall=True,
+                  species=[_sp(1.0, 16.0, 0.1, 16, 1.0050378), _sp(-1.0, 1.0, 0.1, 16, 1.0050378)],
+                  small=(512, 64), crop=(512, 64)),
+    # large Weibel filamentation: counter-streaming pair beams along x at +-0.5c
+    "weibel": dict(name="weibel_pair_8192x2048_ppc16x4", size_x=8192, size_y=2048, delta=0, dt=0.1, c=3.0,
+                   dens=32, n_pass=8, periodic_x=True, left_wall=False,
+                   species=[_sp(-1.0, 1.0, 0.05, 16, 1.1547005, 1.0), _sp(-1.0, 1.0, 0.05, 16, 1.1547005, -1.0),
+                            _sp(1.0, 1.0, 0.05, 16, 1.1547005, 1.0), _sp(1.0, 1.0, 0.05, 16, 1.1547005, -1.0)],
+                   small=(2048, 512), crop=(512, 256)),
+}
+WORKLOAD = WORKLOADS["thermal"]
 FALLBACK_HBM_GBS = 6650.0
 B_PER_PARTICLE = 48.0  # {cell, dx, dy, px, py, pz} read and written once
 B_PER_CELL = 44.0      # E, B read (24 B); Jx, Jy, Jz, rho, dens written (20 B)
@@ -53,8 +77,10 @@ B_PER_CELL = 44.0      # E, B read (24 B); Jx, Jy, Jz, rho, dens written (20 B)
 
 def params(w, **over):
     from spectral_rs_b200.config import Params
+    sp = w["species"]
     d = dict(size_x=w["size_x"], size_y=w["size_y"], delta=w["delta"], dt=w["dt"], c=w["c"], dens=w["dens"],
-             gamma_inj=1.0, n_pass=w["n_pass"], mass_ratio=w["mass_ratio"], vth=w["vth"], periodic_x=True)
+             gamma_inj=max(1.0 + 1e-6, sp[0]["gamma"]), n_pass=w["n_pass"], mass_ratio=sp[0]["m"],
+             vth=sp[0]["vth"], periodic_x=w["periodic_x"], left_wall=w["left_wall"])
     if w.get("tile"):
         d["tile_x"], d["tile_y"] = w["tile"]
     d.update(over)
@@ -66,9 +92,10 @@ def make_sim(w, path="split", seed=0):
     from spectral_rs_b200.config import Config, Setup, Output
     cfg = Config(params(w), Setup(0), Output(False, False, 1, 1, 1, 1))
     sim = Sim(cfg, path=path)
-    # ions then electrons, as run() creates them (src/lib.rs:124-126); seeded device init
-    sim.init_species(1.0, w["mass_ratio"], w["vth"], w["ppc"], 0, w["size_x"], 0.0, 1.0, True, seed * 2 + 1)
-    sim.init_species(-1.0, 1.0, w["vth"], w["ppc"], 0, w["size_x"], 0.0, 1.0, True, seed * 2 + 2)
+    # seeded device init, columns [delta, size_x - delta) as the reference fills them
+    for k, sp in enumerate(w["species"]):
+        sim.init_species(sp["q"], sp["m"], sp["vth"], sp["ppc"], w["delta"], w["size_x"] - w["delta"], sp["gamma"],
+                         sp["sign"], True, seed * len(w["species"]) + k + 1)
     return sim
 
 
@@ -139,13 +166,16 @@ def oracle_crop_rate(w, seconds_target, steps=None, warmup=1):
     from oracle import oracle as orc
     from spectral_rs_b200.config import SpeciesSpec
     from spectral_rs_b200.init import species_arrays
-    p = params(w, size_x=CROP["size_x"], size_y=CROP["size_y"], random_positions=True, seed=7)
+    cx, cy = w["crop"]
+    p = params(w, size_x=cx, size_y=cy, random_positions=True, seed=7)
     o = orc.OracleSim.from_params(p, dtype=np.float32)
     n = 0
-    for k, (q, m) in enumerate(((1.0, w["mass_ratio"]), (-1.0, 1.0))):
-        spec = SpeciesSpec(charge=q, mass=m, vth=w["vth"], ppc=w["ppc"], drift_gamma=0.0, x0=0, x1=p.size_x)
+    for k, sp in enumerate(w["species"]):
+        spec = SpeciesSpec(charge=sp["q"], mass=sp["m"], vth=sp["vth"], ppc=sp["ppc"], drift_gamma=sp["gamma"],
+                           drift_sign=sp["sign"], x0=w["delta"], x1=p.size_x - w["delta"])
         a = species_arrays(p, spec, seed_offset=k)
-        o.add_species(q, m, w["vth"], a["ix"], a["iy"], a["dx"], a["dy"], a["px"], a["py"], a["pz"], a["psa"])
+        o.add_species(sp["q"], sp["m"], sp["vth"], a["ix"], a["iy"], a["dx"], a["dy"], a["px"], a["py"], a["pz"],
+                      a["psa"])
         n += len(a["ix"])
     o.prepare()
     o.step(warmup)
@@ -157,7 +187,7 @@ def oracle_crop_rate(w, seconds_target, steps=None, warmup=1):
     t0 = time.perf_counter()
     o.step(steps)
     dt = time.perf_counter() - t0
-    sample = f"{CROP['size_x']}x{CROP['size_y']} crop, {w['ppc']} ppc/species, {n} particles, {steps} steps"
+    sample = f"{cx}x{cy} crop, {len(w['species'])} species, {n} particles, {steps} steps"
     return n * steps / dt, orc.num_threads(), sample, dt
 
 
@@ -171,8 +201,8 @@ def run_reference(args, w):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded)", "impl": "reference",
-            "config": {"workload": w["name"], "grid": [w["size_x"], w["size_y"]], "ppc_per_species": w["ppc"],
-                       "sample": sample},
+            "config": {"workload": w["name"], "grid": [w["size_x"], w["size_y"]],
+                       "ppc_per_species": [sp["ppc"] for sp in w["species"]], "sample": sample},
             "cpu_baseline": {"value": rate, "unit": "particle-steps/s", "cores": cores, "kind": "port",
                              "sample": sample + " (C++ restatement of the reference CPU path)"},
             "e2e": {"value": rate, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -206,9 +236,9 @@ def e2e_run(w, steps, seed):
     from spectral_rs_b200.init import positions, draws, velocities
     p = params(w, random_positions=True, seed=seed)
     host = []
-    for k, (q, m) in enumerate(((1.0, w["mass_ratio"]), (-1.0, 1.0))):
+    for k, sp in enumerate(w["species"]):
         rng = np.random.default_rng([seed, k])
-        ix, iy, dx, dy = positions(p.size_x, p.size_y, 0, w["ppc"], 0, p.size_x, True, rng)
+        ix, iy, dx, dy = positions(p.size_x, p.size_y, w["delta"], sp["ppc"], None, None, True, rng)
         n = len(ix)
         arrs = {}
         for name, src in (("ix", ix), ("iy", iy), ("dx", dx), ("dy", dy)):
@@ -222,15 +252,16 @@ def e2e_run(w, steps, seed):
         for s0 in range(0, n, chunk):
             s1 = min(n, s0 + chunk)
             nrm, uni = draws(s1 - s0, rng)
-            px, py, pz, psa = velocities(nrm, uni, p.c, w["vth"], 0.0)
+            px, py, pz, psa = velocities(nrm, uni, p.c, sp["vth"], sp["gamma"], sp["sign"])
             arrs["px"][s0:s1], arrs["py"][s0:s1], arrs["pz"][s0:s1], arrs["psa"][s0:s1] = px, py, pz, psa
-        host.append((q, m, arrs))
+        host.append((sp, arrs))
     cfg = Config(p, Setup(steps), Output(False, False, 1, 1, 1, 1))
     sim = Sim(cfg)
-    h2d = sum(a["ix"].nbytes + a["iy"].nbytes + 6 * a["dx"].nbytes for (_, _, a) in host)
+    h2d = sum(a["ix"].nbytes + a["iy"].nbytes + 6 * a["dx"].nbytes for (_, a) in host)
     t0 = time.perf_counter()
-    for q, m, a in host:
-        sim.add_species(q, m, w["vth"], a["ix"], a["iy"], a["dx"], a["dy"], a["px"], a["py"], a["pz"], a["psa"])
+    for sp, a in host:
+        sim.add_species(sp["q"], sp["m"], sp["vth"], a["ix"], a["iy"], a["dx"], a["dy"], a["px"], a["py"], a["pz"],
+                        a["psa"])
     sim.prepare()
     sim.step(steps)
     out = [sim.flds.spatial(name, with_ghosts=False) for name in
@@ -238,7 +269,7 @@ def e2e_run(w, steps, seed):
     d = sim.diag()
     dt = time.perf_counter() - t0
     d2h = sum(o.nbytes for o in out) + d.nbytes
-    n = sum(len(a["ix"]) for (_, _, a) in host)
+    n = sum(len(a["ix"]) for (_, a) in host)
     sim.close()
     return {"value": n * steps / dt, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d / steps,
             "d2h_bytes_per_step": d2h / steps, "wall_s": dt,
@@ -328,11 +359,15 @@ def run_gpu(args, w):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded device init)",
-                "config": {"workload": w["name"], "grid": [w["size_x"], w["size_y"]], "ppc_per_species": w["ppc"],
-                           "particles_per_gpu": n_particles, "mass_ratio": w["mass_ratio"], "vth": w["vth"],
-                           "n_pass": w["n_pass"], "c": w["c"], "dt": w["dt"], "path": "split",
-                           "parallelism": "replicas" if world > 1 else "single",
-                           "l2": "inputs larger than L2 (13 GB particle state)"},
+                "config": {"workload": w["name"], "grid": [w["size_x"], w["size_y"]],
+                           "species": [{"charge": sp["q"], "mass": sp["m"], "vth": sp["vth"], "ppc": sp["ppc"],
+                                        "drift_gamma": sp["gamma"], "drift_sign": sp["sign"]}
+                                       for sp in w["species"]],
+                           "particles_per_gpu": n_particles, "n_pass": w["n_pass"], "c": w["c"], "dt": w["dt"],
+                           "delta": w["delta"], "periodic_x": w["periodic_x"], "left_wall": w["left_wall"],
+                           "path": "split", "parallelism": "replicas" if world > 1 else "single",
+                           "l2": f"inputs larger than L2 ({24 * n_particles / 1e9:.1f} GB particle state)"
+                           if 24 * n_particles > 126e6 else "inputs smaller than L2 (no flush)"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                              "kernel": "k_slot<push,move> (fused push + move + deposit)",
@@ -456,16 +491,17 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--small", action="store_true", help="1/16 of the workload (quick checks)")
-    ap.add_argument("--workload", default="thermal", choices=["thermal", "ensemble"])
+    ap.add_argument("--workload", default="thermal", choices=sorted(WORKLOADS) + ["ensemble"])
     ap.add_argument("--tile", default=None, help="split-path tile shape TXxTY (default: the library's choice)")
     ap.add_argument("--ensemble", type=int, default=64, help="members of the batched ensemble")
     args = ap.parse_args()
     if args.workload == "ensemble":
         run_ensemble(args)
         return
-    w = dict(WORKLOAD)
+    w = dict(WORKLOADS[args.workload])
     if args.small:
-        w.update(size_x=1024, size_y=256, name="thermal_ep_1024x256_ppc64")
+        sx, sy = w["small"]
+        w.update(size_x=sx, size_y=sy, name=f"{w['name']}_small_{sx}x{sy}")
     if args.tile:
         w["tile"] = tuple(int(v) for v in args.tile.lower().split("x"))
     if args.impl == "reference":

@@ -142,7 +142,8 @@ def check(code, ctx=None):
 
 
 def field_op(size_x, size_y, op, spatial, n_pass=0):
-    """Standalone Field op on the GPU: 0 deposit_ghosts, 1 update_ghosts, 2 binomial filter."""
+    """Standalone Field op on the GPU: 0 deposit_ghosts, 1 update_ghosts, 2 binomial filter
+    (one kernel per pass), 3 binomial filter (the fused n-pass kernel)."""
     lib = load()
     a = np.ascontiguousarray(spatial, dtype=np.float32).copy()
     check(lib.spx_field_op(size_x, size_y, op, n_pass, ptr(a)))

@@ -883,7 +883,8 @@ extern "C" int spx_diag(spx_ctx* c, double* out5) {
 
 // ---------------------------------------------------------------- standalone ops
 extern "C" int spx_field_op(uint64_t nx, uint64_t ny, int32_t op, uint32_t n_pass, float* spatial) {
-  if (!spatial || nx < 2 || ny < 2 || op < 0 || op > 2) return fail(nullptr, SPX_ERR_ARG, "bad field op arguments");
+  if (!spatial || nx < 2 || ny < 2 || op < 0 || op > 3) return fail(nullptr, SPX_ERR_ARG, "bad field op arguments");
+  if (op == 3 && !filter_fused_fits(n_pass)) return fail(nullptr, SPX_ERR_ARG, "n_pass out of the fused filter's range");
   try {
     Grid g{(int)nx, (int)ny, (int)nx + 2, 0, 0};
     const size_t bytes = g.spatial_size() * 4;
@@ -893,7 +894,12 @@ extern "C" int spx_field_op(uint64_t nx, uint64_t ny, int32_t op, uint32_t n_pas
     SPX_CUDA_TRY(cudaMemcpy(a, spatial, bytes, cudaMemcpyHostToDevice));
     if (op == 0) launch_fold(g, &a, 1, 0);
     else if (op == 1) launch_update_ghosts(g, &a, 1, 0);
-    else {
+    else if (op == 3) {  // the fused kernel of Flds::update, then the ghost fill its consumer does
+      fields_set_kernel_attributes();
+      launch_filter_fused(g, &a, &b, 1, n_pass, 0);
+      launch_update_ghosts(g, &b, 1, 0);
+      std::swap(a, b);
+    } else {
       for (uint32_t p = 0; p < n_pass; ++p) {
         launch_filter_pass(g, &a, &b, 1, 0);
         std::swap(a, b);

@@ -173,8 +173,30 @@ __host__ __device__ inline int col_logW(int logNy, int logNx) {
 struct RowArgs {
   const void* src[8];
   void* dst[8];
+  float* back[8];  // IN == 0: when set, the input value is also stored here (ghosted, periodic ghosts)
   float scale[8];
 };
+
+// Store the value of interior cell (row, e) (0-based) into a ghosted spatial
+// field together with the ghost cells that are its periodic images
+// (copy_to_spatial followed by update_ghosts, src/flds/field.rs:128-257).
+__device__ __forceinline__ void store_ghosted(float* dst, const Grid& g, int row, int e, float v) {
+  const int N = g.nx, W = g.W;
+  const int R = row + 1;  // ghosted row
+  dst[(size_t)R * W + e + 1] = v;
+  if (e == N - 1) dst[(size_t)R * W + 0] = v;  // left ghost <- last column
+  if (e == 0) dst[(size_t)R * W + N + 1] = v;  // right ghost <- first column
+  if (R == g.ny) {                             // top ghost row <- last row
+    dst[e + 1] = v;
+    if (e == N - 1) dst[0] = v;      // top-left <- bottom-right
+    if (e == 0) dst[N + 1] = v;      // top-right <- bottom-left
+  }
+  if (R == 1) {  // bottom ghost row <- first row
+    dst[(size_t)(g.ny + 1) * W + e + 1] = v;
+    if (e == N - 1) dst[(size_t)(g.ny + 1) * W + 0] = v;      // bottom-left <- top-right
+    if (e == 0) dst[(size_t)(g.ny + 1) * W + N + 1] = v;      // bottom-right <- top-left
+  }
+}
 
 template <int IN, int OUT, bool INV>
 __global__ void __launch_bounds__(1024) k_rows(const __grid_constant__ RowArgs a, Grid g, const float2* __restrict__ tw) {
@@ -191,7 +213,9 @@ __global__ void __launch_bounds__(1024) k_rows(const __grid_constant__ RowArgs a
     if (row < g.ny) {
       if (IN == 0) {
         const float* src = (const float*)a.src[f];
-        v = make_float2(src[(size_t)(row + 1) * g.W + e + 1] * sc, 0.f * sc);
+        const float x = src[(size_t)(row + 1) * g.W + e + 1];
+        if (a.back[f]) store_ghosted(a.back[f], g, row, e, x);
+        v = make_float2(x * sc, 0.f * sc);
       } else {
         const float2* src = (const float2*)a.src[f];
         v = src[(size_t)row * N + e];
@@ -212,24 +236,8 @@ __global__ void __launch_bounds__(1024) k_rows(const __grid_constant__ RowArgs a
       dst[(size_t)row * N + e] = INV ? c_scale(v, sc) : v;
     } else {
       // spatial = Re(ifft) * (1/(nx ny)); the CTA that owns row r also fills the
-      // ghost columns of row r+1 and, for r == ny-1 / r == 0, the ghost rows.
-      float* dst = (float*)a.dst[f];
-      const float re = v.x * sc;
-      const int W = g.W;
-      const int R = row + 1;  // ghosted row
-      dst[(size_t)R * W + e + 1] = re;
-      if (e == N - 1) dst[(size_t)R * W + 0] = re;        // left ghost <- last column
-      if (e == 0) dst[(size_t)R * W + N + 1] = re;        // right ghost <- first column
-      if (R == g.ny) {                                    // top ghost row <- last row
-        dst[e + 1] = re;
-        if (e == N - 1) dst[0] = re;                      // top-left <- bottom-right
-        if (e == 0) dst[N + 1] = re;                      // top-right <- bottom-left
-      }
-      if (R == 1) {                                       // bottom ghost row <- first row
-        dst[(size_t)(g.ny + 1) * W + e + 1] = re;
-        if (e == N - 1) dst[(size_t)(g.ny + 1) * W + 0] = re;      // bottom-left <- top-right
-        if (e == 0) dst[(size_t)(g.ny + 1) * W + N + 1] = re;      // bottom-right <- top-left
-      }
+      // ghost cells that are images of row r
+      store_ghosted((float*)a.dst[f], g, row, e, v.x * sc);
     }
   }
 }
@@ -399,6 +407,92 @@ __global__ void k_filter(const __grid_constant__ ConstFieldList S, const __grid_
   out[r * W + c] = v;
 }
 
+constexpr int FILT_TX = 64, FILT_TY = 16;  // output tile of the fused filter
+
+// binomial_filter_2_d's stencil at the cell whose 3x3 neighbourhood rows start
+// at up, md, dn (left column): reference summation order, no contraction.
+__device__ __forceinline__ float binomial9(const float* up, const float* md, const float* dn) {
+  float v = __fmul_rn(0.0625f, up[0]);
+  v = __fadd_rn(v, __fmul_rn(0.125f, up[1]));
+  v = __fadd_rn(v, __fmul_rn(0.0625f, up[2]));
+  v = __fadd_rn(v, __fmul_rn(0.125f, md[0]));
+  v = __fadd_rn(v, __fmul_rn(0.25f, md[1]));
+  v = __fadd_rn(v, __fmul_rn(0.125f, md[2]));
+  v = __fadd_rn(v, __fmul_rn(0.0625f, dn[0]));
+  v = __fadd_rn(v, __fmul_rn(0.125f, dn[1]));
+  v = __fadd_rn(v, __fmul_rn(0.0625f, dn[2]));
+  return v;
+}
+
+// n passes of binomial_filter_2_d in one kernel (the reference runs them one
+// after another, each followed by update_ghosts, src/flds/mod.rs:90-94).  Pass
+// 1 reads the raw ghosted input around each cell's periodic image; after it
+// every neighbour is a periodic image, so passes 2..n run on a shared-memory
+// tile whose halo shrinks by one cell per pass.  Writes the interior of `out`;
+// each value is computed exactly as the separate passes compute it.
+__host__ __device__ inline size_t filter_fused_smem_floats(int npass) {
+  const int h = npass - 1;
+  const size_t ew = FILT_TX + 2 * h, eh = FILT_TY + 2 * h;
+  return 2 * ew * eh + (ew + 2) * (eh + 2);
+}
+__global__ void __launch_bounds__(256) k_filter_fused(const __grid_constant__ ConstFieldList S,
+                                                      const __grid_constant__ FieldList D, Grid g, int npass) {
+  extern __shared__ float fs[];
+  const float* in = S.f[blockIdx.z];
+  float* out = D.f[blockIdx.z];
+  const int W = g.W, nx = g.nx, ny = g.ny;
+  const int h = npass - 1;
+  const int EW = FILT_TX + 2 * h, EH = FILT_TY + 2 * h;
+  const int x0 = blockIdx.x * FILT_TX + 1, y0 = blockIdx.y * FILT_TY + 1;  // first interior cell of the tile
+  const int ex0 = x0 - h, ey0 = y0 - h;                                    // origin of the extended frame
+  float* s0 = fs;
+  float* s1 = fs + EW * EH;
+  float* raw = fs + 2 * EW * EH;
+  const bool inner = ex0 >= 1 && ey0 >= 1 && ex0 + EW - 1 <= nx && ey0 + EH - 1 <= ny;
+  if (inner) {  // the frame and its one-cell border are plain array cells
+    const int RW = EW + 2, RH = EH + 2;
+    for (int i = threadIdx.x; i < RW * RH; i += blockDim.x) {
+      const int r = i / RW, q = i - r * RW;
+      raw[i] = in[(size_t)(ey0 - 1 + r) * W + (ex0 - 1 + q)];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < EW * EH; i += blockDim.x) {
+      const int r = i / EW, q = i - r * EW;
+      const float* up = raw + r * RW + q;
+      s0[i] = binomial9(up, up + RW, up + 2 * RW);
+    }
+  } else {  // near the domain edge: the periodic image of each frame cell, raw ghosts included
+    for (int i = threadIdx.x; i < EW * EH; i += blockDim.x) {
+      const int r = i / EW, q = i - r * EW;
+      const int yy = (((ey0 + r - 1) % ny) + ny) % ny + 1;
+      const int xx = (((ex0 + q - 1) % nx) + nx) % nx + 1;
+      const float* md = in + (size_t)yy * W + xx - 1;
+      s0[i] = binomial9(md - W, md, md + W);
+    }
+  }
+  __syncthreads();
+  float* src = s0;
+  float* dst = s1;
+  for (int p = 2; p <= npass; ++p) {
+    const int m = p - 1;  // frame cells [m, EW - m) x [m, EH - m)
+    const int w = EW - 2 * m, hh = EH - 2 * m;
+    for (int i = threadIdx.x; i < w * hh; i += blockDim.x) {
+      const int r = i / w + m, q = i % w + m;
+      const float* up = src + (r - 1) * EW + (q - 1);
+      dst[r * EW + q] = binomial9(up, up + EW, up + 2 * EW);
+    }
+    __syncthreads();
+    float* t = src;
+    src = dst;
+    dst = t;
+  }
+  for (int i = threadIdx.x; i < FILT_TX * FILT_TY; i += blockDim.x) {
+    const int r = i / FILT_TX, q = i - r * FILT_TX;
+    const int yy = y0 + r, xx = x0 + q;
+    if (yy <= ny && xx <= nx) out[(size_t)yy * W + xx] = src[(r + h) * EW + (q + h)];
+  }
+}
+
 __global__ void k_scale_c(float2* d, size_t n, float s) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     d[i] = c_scale(d[i], s);
@@ -420,6 +514,23 @@ void launch_update_ghosts(const Grid& g, float* const* fields, int nf, cudaStrea
   k_update_ghosts<<<dim3((nper + 255) / 256, nf), 256, 0, st>>>(L, g);
 }
 
+bool filter_fused_fits(uint32_t npass) {
+  return npass >= 1 && filter_fused_smem_floats((int)npass) * sizeof(float) <= 96 * 1024;
+}
+
+void launch_filter_fused(const Grid& g, float* const* src, float* const* dst, int nf, uint32_t npass,
+                         cudaStream_t st) {
+  ConstFieldList S{};
+  FieldList D{};
+  for (int i = 0; i < nf; ++i) {
+    S.f[i] = src[i];
+    D.f[i] = dst[i];
+  }
+  const size_t smem = filter_fused_smem_floats((int)npass) * sizeof(float);
+  dim3 grd((g.nx + FILT_TX - 1) / FILT_TX, (g.ny + FILT_TY - 1) / FILT_TY, nf);
+  k_filter_fused<<<grd, 256, smem, st>>>(S, D, g, (int)npass);
+}
+
 void launch_filter_pass(const Grid& g, float* const* src, float* const* dst, int nf, cudaStream_t st) {
   ConstFieldList S{};
   FieldList D{};
@@ -438,7 +549,7 @@ void launch_filter_pass(const Grid& g, float* const* src, float* const* dst, int
 void fields_set_kernel_attributes() {
   for (const void* f : {(const void*)k_rows<0, 0, false>, (const void*)k_rows<1, 0, false>,
                         (const void*)k_rows<1, 0, true>, (const void*)k_rows<1, 1, true>, (const void*)k_cols<false>,
-                        (const void*)k_cols<true>})
+                        (const void*)k_cols<true>, (const void*)k_filter_fused})
     SPX_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
 }
 
@@ -497,17 +608,27 @@ void FieldBuffers::release() {
 int field_update(FieldBuffers& fb, cudaStream_t st) {
   const Grid& g = fb.g;
   int launches = 0;
-  // 1. n_pass binomial passes on jx, jy, jz, dsty (mod.rs:90-94), ping-pong.
-  float* cur[4] = {fb.spatial[SPX_JX], fb.spatial[SPX_JY], fb.spatial[SPX_JZ], fb.spatial[SPX_DSTY]};
-  float* oth[4] = {fb.filt_tmp[0], fb.filt_tmp[1], fb.filt_tmp[2], fb.filt_tmp[3]};
-  for (uint32_t p = 0; p < fb.n_pass; ++p) {
-    launch_filter_pass(g, cur, oth, 4, st);
+  // 1. n_pass binomial passes on jx, jy, jz, dsty (mod.rs:90-94).  Fused: all
+  // passes in one kernel into filt_tmp; the row transforms below read the
+  // filtered interior from there and store it back into the fields with their
+  // periodic ghosts, which is the state the reference leaves.
+  float* srcs[4] = {fb.spatial[SPX_JX], fb.spatial[SPX_JY], fb.spatial[SPX_JZ], fb.spatial[SPX_DSTY]};
+  const bool fused = filter_fused_fits(fb.n_pass);
+  if (fused) {
+    launch_filter_fused(g, srcs, fb.filt_tmp, 4, fb.n_pass, st);
     ++launches;
-    for (int i = 0; i < 4; ++i) std::swap(cur[i], oth[i]);
-  }
-  if (fb.n_pass & 1) {  // keep the filtered result in the field's own buffer
-    for (int i = 0; i < 4; ++i)
-      SPX_CUDA_TRY(cudaMemcpyAsync(oth[i], cur[i], g.spatial_size() * sizeof(float), cudaMemcpyDeviceToDevice, st));
+  } else {  // separate passes, ping-pong (no filter when n_pass == 0)
+    float* cur[4] = {srcs[0], srcs[1], srcs[2], srcs[3]};
+    float* oth[4] = {fb.filt_tmp[0], fb.filt_tmp[1], fb.filt_tmp[2], fb.filt_tmp[3]};
+    for (uint32_t p = 0; p < fb.n_pass; ++p) {
+      launch_filter_pass(g, cur, oth, 4, st);
+      ++launches;
+      for (int i = 0; i < 4; ++i) std::swap(cur[i], oth[i]);
+    }
+    if (fb.n_pass & 1) {  // keep the filtered result in the field's own buffer
+      for (int i = 0; i < 4; ++i)
+        SPX_CUDA_TRY(cudaMemcpyAsync(oth[i], cur[i], g.spatial_size() * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    }
   }
   // 2. copy_to_spectral (+ dsty/dens) fused with the row FFTs (mod.rs:66-85, 101-103, 122-124)
   {
@@ -517,8 +638,14 @@ int field_update(FieldBuffers& fb, cudaStream_t st) {
     for (int i = 0; i < 7; ++i) {
       a.src[i] = fb.spatial[src_ids[i]];
       a.dst[i] = fb.spec[dst_ids[i]];
+      a.back[i] = nullptr;
       a.scale[i] = 1.0f;
     }
+    if (fused)
+      for (int i = 0; i < 4; ++i) {
+        a.src[i] = fb.filt_tmp[i];
+        a.back[i] = srcs[i];
+      }
     a.scale[3] = 1.0f / (float)fb.dens;
     launch_rows<0, 0, false>(g, a, 7, fb.tw_x, st);
     ++launches;

@@ -33,6 +33,11 @@ void launch_fold(const Grid& g, float* const* fields, int nf, cudaStream_t st);
 void launch_update_ghosts(const Grid& g, float* const* fields, int nf, cudaStream_t st);
 // One binomial_filter_2_d pass (src/flds/field.rs:376-426) from src[f] into dst[f].
 void launch_filter_pass(const Grid& g, float* const* src, float* const* dst, int nf, cudaStream_t st);
+// n_pass binomial_filter_2_d passes in one kernel, from src[f] into the
+// interior of dst[f] (ghosts untouched); usable when filter_fused_fits(n_pass).
+bool filter_fused_fits(uint32_t npass);
+void launch_filter_fused(const Grid& g, float* const* src, float* const* dst, int nf, uint32_t npass,
+                         cudaStream_t st);
 // Flds::update (src/flds/mod.rs:87-309).  Returns the number of kernel launches.
 int field_update(FieldBuffers& fb, cudaStream_t st);
 // Fft2D::fft / inv_fft on one complex array in place (tests).

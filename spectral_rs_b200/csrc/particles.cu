@@ -454,8 +454,10 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
       nq_m = 0;
     };
 
-    // software pipeline: the state of round r+1 is loaded during round r
+    // software pipeline: the state of round r+1 is loaded during round r (with
+    // the tag on moving steps: a particle that moves or shifts down takes it along)
     float ndx = 0.f, ndy = 0.f, npx = 0.f, npy = 0.f, npz = 0.f;
+    uint32_t ntg = 0u;
     bool nact = false;
     int nidx = c;
     if (rounds > 0) {
@@ -467,12 +469,14 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
         npx = spx[nidx];
         npy = spy[nidx];
         npz = spz[nidx];
+        if (MOVE) ntg = stg[nidx];
       }
     }
     for (int r = 0; r < rounds; ++r) {
       const int idx = nidx;
       const bool act = nact;
       float dx = ndx, dy = ndy, px = npx, py = npy, pz = npz;
+      const uint32_t tg = ntg;
       if (r + 1 < rounds) {
         const int sl = slot_of(r + 1, nact);
         nidx = sl * TC + c;
@@ -482,6 +486,7 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
           npx = spx[nidx];
           npy = spy[nidx];
           npz = spz[nidx];
+          if (MOVE) ntg = stg[nidx];
         }
       }
       bool jcross = false, mover = false;
@@ -564,7 +569,7 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
             spx[o] = px;
             spy[o] = py;
             spz[o] = pz;
-            if (o != idx) stg[o] = stg[idx];
+            if (o != idx) stg[o] = tg;
             ++kept;
           }
         }
@@ -595,7 +600,7 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
             qm[3 * QCAP + e] = px;
             qm[4 * QCAP + e] = py;
             qm[5 * QCAP + e] = pz;
-            qm[6 * QCAP + e] = __uint_as_float(stg[idx]);
+            qm[6 * QCAP + e] = __uint_as_float(tg);
           }
           nq_m += __popc(mm);
           __syncwarp();
