@@ -86,6 +86,8 @@ typedef struct spx_params {
   int32_t slot_capacity; /* minimum particle slots per cell and species (split path);
                           negative: exactly -slot_capacity (testing the overflow path)  */
   int32_t device;      /* CUDA device ordinal                                              */
+  int32_t compensated; /* 1: current sums of the split path Kahan-compensated in registers and
+                          carried through the tile flush (one CTA per SM, slower); 0: plain FP32 */
 } spx_params;
 
 typedef struct spx_ctx spx_ctx;

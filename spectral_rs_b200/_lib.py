@@ -44,7 +44,7 @@ class SpxParams(ctypes.Structure):
         ("gamma_inj", ctypes.c_float), ("n_pass", ctypes.c_uint32), ("periodic_x", ctypes.c_int32),
         ("left_wall", ctypes.c_int32),
         ("path", ctypes.c_int32), ("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32),
-        ("slot_capacity", ctypes.c_int32), ("device", ctypes.c_int32),
+        ("slot_capacity", ctypes.c_int32), ("device", ctypes.c_int32), ("compensated", ctypes.c_int32),
     ]
 
 

@@ -13,6 +13,7 @@ reference's behaviour:
   left_wall = false       reflect at ix = delta+1 too (the reference asserts no particle gets there)
   path = "split"          "split" (integer cell + FP32 offset) or "plain" (global FP32 x)
   tile_x, tile_y, slot_capacity   GPU layout knobs (0 = automatic)
+  compensated = false     Kahan-compensated current sums in the split-path kernel
 
 [[species]]               optional list replacing the default ion/electron pair
   charge, mass, vth, ppc (default dens), drift_gamma (default gamma_inj; <= 1: none),
@@ -47,6 +48,7 @@ class Params:
     tile_x: int = 0
     tile_y: int = 0
     slot_capacity: int = 0
+    compensated: bool = False
 
 
 @dataclasses.dataclass

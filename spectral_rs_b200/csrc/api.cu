@@ -95,9 +95,9 @@ extern "C" int spx_create(const spx_params* p, spx_ctx** out) {
   if (!p || !out) return fail(nullptr, SPX_ERR_ARG, "null argument");
   *out = nullptr;
   if (p->size_x % 2 || p->size_y % 2) return fail(nullptr, SPX_ERR_ARG, "Number of cells must be even (src/lib.rs:76)");
-  if (!is_pow2(p->size_x) || !is_pow2(p->size_y) || p->size_x < 8 || p->size_y < 8 || p->size_x > 32768 ||
-      p->size_y > 32768)
-    return fail(nullptr, SPX_ERR_ARG, "GPU FFT needs power-of-two sizes in [8, 32768]");
+  if (!is_pow2(p->size_x) || !is_pow2(p->size_y) || p->size_x < 8 || p->size_y < 8 || p->size_x > 8192 ||
+      p->size_y > 8192)
+    return fail(nullptr, SPX_ERR_ARG, "GPU FFT needs power-of-two sizes in [8, 8192]");
   if (!p->periodic_x && p->delta * 2 >= p->size_x)
     return fail(nullptr, SPX_ERR_ARG, "Delta must be less than 1/2 the size of size_x (src/lib.rs:88)");
   if (p->dens == 0 || !(p->c > 0) || !(p->dt > 0)) return fail(nullptr, SPX_ERR_ARG, "dens, c and dt must be positive");
@@ -145,6 +145,7 @@ extern "C" int spx_create(const spx_params* p, spx_ctx** out) {
     c->pp.left_wall = p->left_wall;
     c->pp.wall_loc = (int)(p->size_x + 1 - p->delta);  // src/prtls.rs:153
     c->pp.delta = (int)p->delta;
+    c->pp.compensated = p->compensated != 0;
     c->plain = p->path == SPX_PATH_PLAIN;
     SPX_CUDA_TRY(cudaMalloc(&c->d_err, sizeof(int)));
     SPX_CUDA_TRY(cudaMemset(c->d_err, 0, sizeof(int)));
@@ -284,6 +285,21 @@ __global__ void k_check_gamma(uint64_t n, const float* px, const float* py, cons
   }
 }
 
+// Cell indices (1-based, usize in the reference) -> packed cell; the smallest
+// index of a particle outside the grid goes to *bad (initialised to ~0).
+__global__ void k_pack_check(uint64_t n, const uint64_t* ix, const uint64_t* iy, int nx, int ny, uint32_t* cell,
+                             uint32_t* bad) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t x = ix[i], y = iy[i];
+    if (x < 1 || y < 1 || x > (uint64_t)nx || y > (uint64_t)ny) {
+      atomicMin(bad, (uint32_t)i);
+      cell[i] = 1u | (1u << 16);
+    } else {
+      cell[i] = (uint32_t)x | ((uint32_t)y << 16);
+    }
+  }
+}
+
 extern "C" int spx_add_species(spx_ctx* c, float charge, float mass, float vth, uint64_t n, const uint64_t* ix,
                                const uint64_t* iy, const float* dx, const float* dy, const float* px, const float* py,
                                const float* pz, const float* psa, int32_t* species_out) {
@@ -304,13 +320,20 @@ extern "C" int spx_add_species(spx_ctx* c, float charge, float mass, float vth, 
     s.n = n;
     Staging st;
     st.alloc(n);
-    std::vector<uint32_t> cells(n);
-    for (uint64_t i = 0; i < n; ++i) {
-      if (ix[i] < 1 || iy[i] < 1 || ix[i] > (uint64_t)c->g.nx || iy[i] > (uint64_t)c->g.ny)
-        return fail(c, SPX_ERR_BOUNDS, "particle " + std::to_string(i) + " outside the grid");
-      cells[i] = (uint32_t)ix[i] | ((uint32_t)iy[i] << 16);
+    if (n) {  // cell indices checked and packed on the device (ix | iy << 16)
+      uint64_t* d_ixy = nullptr;
+      SPX_CUDA_TRY(cudaMallocAsync(&d_ixy, 2 * n * sizeof(uint64_t), c->st));
+      SPX_CUDA_TRY(cudaMemcpyAsync(d_ixy, ix, n * 8, cudaMemcpyHostToDevice, c->st));
+      SPX_CUDA_TRY(cudaMemcpyAsync(d_ixy + n, iy, n * 8, cudaMemcpyHostToDevice, c->st));
+      SPX_CUDA_TRY(cudaMemsetAsync(c->d_u32, 0xFF, sizeof(uint32_t), c->st));
+      k_pack_check<<<148 * 8, 256, 0, c->st>>>(n, d_ixy, d_ixy + n, c->g.nx, c->g.ny, st.cell, c->d_u32);
+      SPX_CUDA_TRY(cudaFreeAsync(d_ixy, c->st));
+      uint32_t bad = 0;
+      SPX_CUDA_TRY(cudaMemcpyAsync(&bad, c->d_u32, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
+      SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+      if (bad != 0xFFFFFFFFu)
+        return fail(c, SPX_ERR_BOUNDS, "particle " + std::to_string(bad) + " outside the grid");
     }
-    SPX_CUDA_TRY(cudaMemcpyAsync(st.cell, cells.data(), n * 4, cudaMemcpyHostToDevice, c->st));
     SPX_CUDA_TRY(cudaMemcpyAsync(st.dx, dx, n * 4, cudaMemcpyHostToDevice, c->st));
     SPX_CUDA_TRY(cudaMemcpyAsync(st.dy, dy, n * 4, cudaMemcpyHostToDevice, c->st));
     SPX_CUDA_TRY(cudaMemcpyAsync(st.px, px, n * 4, cudaMemcpyHostToDevice, c->st));
@@ -916,8 +939,8 @@ extern "C" int spx_field_op(uint64_t nx, uint64_t ny, int32_t op, uint32_t n_pas
 }
 
 extern "C" int spx_fft2d(uint64_t nx, uint64_t ny, int32_t inverse, float* data) {
-  if (!data || !is_pow2(nx) || !is_pow2(ny) || nx < 8 || ny < 8 || nx > 32768 || ny > 32768)
-    return fail(nullptr, SPX_ERR_ARG, "GPU FFT needs power-of-two sizes in [8, 32768]");
+  if (!data || !is_pow2(nx) || !is_pow2(ny) || nx < 8 || ny < 8 || nx > 8192 || ny > 8192)
+    return fail(nullptr, SPX_ERR_ARG, "GPU FFT needs power-of-two sizes in [8, 8192]");
   try {
     Grid g{(int)nx, (int)ny, (int)nx + 2, ilog2(nx), ilog2(ny)};
     const size_t bytes = nx * ny * 8;
@@ -994,6 +1017,7 @@ extern "C" int spx_batch_create(int32_t n, const spx_params* params, spx_batch**
     for (int i = 0; i < n; ++i) {
       spx_params p = params[i];
       if (p.path == SPX_PATH_PLAIN) throw spx::Error(SPX_ERR_ARG, "a batch runs the split path");
+      if (p.compensated) throw spx::Error(SPX_ERR_ARG, "compensated currents are a single-simulation option");
       if (p.tile_x <= 0 && p.tile_y <= 0) p.tile_x = p.tile_y = 16;  // one tile shape for the whole batch
       spx_ctx* c = nullptr;
       int rc = spx_create(&p, &c);

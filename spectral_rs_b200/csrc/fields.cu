@@ -12,10 +12,12 @@
 //   k_cols<inv>            : column inverse FFTs of B(t) and E
 //   k_rows<inv>            : row inverse FFTs, 1/(nx ny) scale, copy_to_spatial + update_ghosts fused
 //
-// The FFT is a shared-memory Stockham autosort transform (radix 8 passes, one
-// radix 4 or 2 pass for the remaining factor), one radix-8 butterfly per
-// thread per pass, twiddles from an FP64-generated table.  Inverse transforms
-// use ifft(x) = conj(fft(conj(x))), conjugating on load and store.
+// The FFT is a Stockham autosort transform (radix 8 passes, one radix 4 or 2
+// pass for the remaining factor), one radix-8 butterfly per thread per pass:
+// the first pass reads global memory into registers, the last one writes from
+// registers, the passes in between exchange through shared memory; twiddles
+// from an FP64-generated table.  Inverse transforms use
+// ifft(x) = conj(fft(conj(x))), conjugating on load and store.
 #include <cmath>
 #include <vector>
 
@@ -87,37 +89,50 @@ __device__ __forceinline__ void dft8(float2 (&v)[8]) {
   v[7] = c_sub(e3, w3);
 }
 
-// One in-place Stockham pass of radix R over B transforms of length N = 2^logN
-// stored in shared memory at s[e*ES + t*TS].  blockDim.x == N*B/8; each thread
-// does 8/R butterflies.  Ns = product of the radices of the previous passes.
+// Stockham passes over B = 2^logB transforms of length N = 2^logN with
+// blockDim.x == N*B/8: pass p of radix R has each thread do 8/R butterflies
+// b = tid + q*blockDim.x, each on transform t and index j in [0, N/R), with
+// inputs at positions j + r*N/R and outputs at ((j - k)*R + k) + r*Ns, k = j mod
+// Ns (Ns = product of the earlier radices).  The first pass (radix 8) takes its
+// inputs from registers and the last pass leaves its outputs in registers, so
+// the caller loads and stores global memory directly; the passes in between
+// exchange through shared memory, element (t, e) at s[pad(t*TS + e*ES)] with
+// one padding slot per 16 elements against bank conflicts.  Radix 8 passes,
+// then one radix 4 or 2 pass for the remaining factor.
+__device__ __forceinline__ int spad(int i) { return i + (i >> 4); }
+__host__ __device__ inline size_t fft_smem_elems(int logN, int logB) {
+  const size_t n = (size_t)1 << (logN + logB);
+  return n + (n >> 4) + 1;
+}
+__device__ __forceinline__ int num_passes(int logN) { return logN / 3 + (logN % 3 ? 1 : 0); }
+__device__ __forceinline__ int last_radix(int logN) { return logN % 3 == 0 ? 8 : (logN % 3 == 2 ? 4 : 2); }
+
 template <int R>
-__device__ __forceinline__ void fft_pass(float2* s, int logN, int logB, int ES, int TS, bool t_fast, int Ns,
-                                         const float2* __restrict__ tw) {
-  constexpr int PER = 8 / R;
+__device__ __forceinline__ void bfly_tj(int q, int logN, int logB, bool t_fast, int& t, int& j) {
   constexpr int LR = R == 8 ? 3 : R == 4 ? 2 : 1;
-  const int nthr = blockDim.x, tid = threadIdx.x;
+  const int b = threadIdx.x + q * blockDim.x;
   const int logNb = logN - LR;
-  const int nb = 1 << logNb;
-  const int N = 1 << logN;
-  float2 v[8];
-  int out_base[PER];
+  if (t_fast) {
+    t = b & ((1 << logB) - 1);
+    j = b >> logB;
+  } else {
+    t = b >> logNb;
+    j = b & ((1 << logNb) - 1);
+  }
+}
+
+// twiddles and DFTs of the thread's butterflies, slot q*R + r = input r of butterfly q
+template <int R>
+__device__ __forceinline__ void pass_compute(float2 (&v)[8], int logN, int logB, bool t_fast, int Ns,
+                                             const float2* __restrict__ tw) {
+  constexpr int PER = 8 / R;
 #pragma unroll
   for (int q = 0; q < PER; ++q) {
-    const int b = tid + q * nthr;
-    int t, j;
-    if (t_fast) {
-      t = b & ((1 << logB) - 1);
-      j = b >> logB;
-    } else {
-      t = b >> logNb;
-      j = b & (nb - 1);
-    }
-    const int k = j & (Ns - 1);
-    const float2* src = s + t * TS;
-#pragma unroll
-    for (int r = 0; r < R; ++r) v[q * R + r] = src[(j + r * nb) * ES];
     if (Ns > 1) {
-      const int step = N / (Ns * R);
+      int t, j;
+      bfly_tj<R>(q, logN, logB, t_fast, t, j);
+      const int k = j & (Ns - 1);
+      const int step = (1 << logN) / (Ns * R);
 #pragma unroll
       for (int r = 1; r < R; ++r) v[q * R + r] = c_mul(v[q * R + r], __ldg(&tw[r * k * step]));
     }
@@ -128,28 +143,77 @@ __device__ __forceinline__ void fft_pass(float2* s, int logN, int logB, int ES, 
     } else {
       dft2(v[q * 2 + 0], v[q * 2 + 1]);
     }
-    out_base[q] = t * TS + (((j - k) * R) + k) * ES;  // idxD = (j/Ns)*Ns*R + k
   }
-  __syncthreads();
-#pragma unroll
-  for (int q = 0; q < PER; ++q)
-#pragma unroll
-    for (int r = 0; r < R; ++r) s[out_base[q] + r * Ns * ES] = v[q * R + r];
-  __syncthreads();
 }
 
-// Forward FFT of B = 2^logB transforms of length 2^logN in shared memory.
-__device__ void block_fft(float2* s, int logN, int logB, int ES, int TS, bool t_fast, const float2* tw) {
-  int Ns = 1, rem = logN;
-  while (rem >= 3) {
-    fft_pass<8>(s, logN, logB, ES, TS, t_fast, Ns, tw);
-    Ns <<= 3;
-    rem -= 3;
+template <int R>
+__device__ __forceinline__ void pass_store(const float2 (&v)[8], float2* s, int logN, int logB, int ES, int TS,
+                                           bool t_fast, int Ns) {
+  constexpr int PER = 8 / R;
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    int t, j;
+    bfly_tj<R>(q, logN, logB, t_fast, t, j);
+    const int k = j & (Ns - 1);
+    const int base = t * TS + ((j - k) * R + k) * ES;
+#pragma unroll
+    for (int r = 0; r < R; ++r) s[spad(base + r * Ns * ES)] = v[q * R + r];
   }
-  if (rem == 2)
-    fft_pass<4>(s, logN, logB, ES, TS, t_fast, Ns, tw);
-  else if (rem == 1)
-    fft_pass<2>(s, logN, logB, ES, TS, t_fast, Ns, tw);
+}
+
+template <int R>
+__device__ __forceinline__ void pass_load(float2 (&v)[8], const float2* s, int logN, int logB, int ES, int TS,
+                                          bool t_fast) {
+  constexpr int PER = 8 / R;
+  const int nb = (1 << logN) / R;
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    int t, j;
+    bfly_tj<R>(q, logN, logB, t_fast, t, j);
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[q * R + r] = s[spad(t * TS + (j + r * nb) * ES)];
+  }
+}
+
+// Forward FFT.  On entry v[r] = element (t, j + r*N/8) with (t, j) = bfly_tj<8>(0);
+// on exit v[m] = element out_pos(m).
+__device__ __forceinline__ void block_fft_regs(float2 (&v)[8], float2* s, int logN, int logB, int ES, int TS,
+                                               bool t_fast, const float2* __restrict__ tw) {
+  const int np = num_passes(logN);
+  pass_compute<8>(v, logN, logB, t_fast, 1, tw);
+  int Ns = 1;
+  for (int i = 1; i < np; ++i) {
+    pass_store<8>(v, s, logN, logB, ES, TS, t_fast, Ns);  // only the last pass can have radix < 8
+    __syncthreads();
+    Ns <<= 3;
+    const int R = (i < np - 1) ? 8 : last_radix(logN);
+    if (R == 8) {
+      pass_load<8>(v, s, logN, logB, ES, TS, t_fast);
+      pass_compute<8>(v, logN, logB, t_fast, Ns, tw);
+    } else if (R == 4) {
+      pass_load<4>(v, s, logN, logB, ES, TS, t_fast);
+      pass_compute<4>(v, logN, logB, t_fast, Ns, tw);
+    } else {
+      pass_load<2>(v, s, logN, logB, ES, TS, t_fast);
+      pass_compute<2>(v, logN, logB, t_fast, Ns, tw);
+    }
+    __syncthreads();  // every thread has read before the next pass overwrites
+  }
+}
+
+// Position of output slot m after block_fft_regs: last pass radix R = last_radix,
+// butterfly q = m / R, r = m % R, e = j + r*N/R (k = j in the last pass).
+__device__ __forceinline__ void out_pos(int m, int logN, int logB, bool t_fast, int& t, int& e) {
+  const int R = num_passes(logN) == 1 ? 8 : last_radix(logN);
+  const int q = m / R, r = m - q * R;
+  int j;
+  if (R == 8)
+    bfly_tj<8>(q, logN, logB, t_fast, t, j);
+  else if (R == 4)
+    bfly_tj<4>(q, logN, logB, t_fast, t, j);
+  else
+    bfly_tj<2>(q, logN, logB, t_fast, t, j);
+  e = j + r * ((1 << logN) / R);
 }
 
 // ---------------------------------------------------------------- launch geometry
@@ -206,38 +270,46 @@ __global__ void __launch_bounds__(1024) k_rows(const __grid_constant__ RowArgs a
   const int logB = row_logB(logN);
   const int row0 = blockIdx.x << logB;
   const float sc = a.scale[f];
-  for (int i = threadIdx.x; i < (N << logB); i += blockDim.x) {
-    const int t = i >> logN, e = i & (N - 1);
+  // first-pass inputs straight from global memory: 8 independent loads per thread
+  float2 v[8];
+  {
+    int t, j;
+    bfly_tj<8>(0, logN, logB, false, t, j);
     const int row = row0 + t;
-    float2 v = make_float2(0.f, 0.f);
-    if (row < g.ny) {
-      if (IN == 0) {
-        const float* src = (const float*)a.src[f];
-        const float x = src[(size_t)(row + 1) * g.W + e + 1];
-        if (a.back[f]) store_ghosted(a.back[f], g, row, e, x);
-        v = make_float2(x * sc, 0.f * sc);
-      } else {
-        const float2* src = (const float2*)a.src[f];
-        v = src[(size_t)row * N + e];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int e = j + r * (N >> 3);
+      float2 x = make_float2(0.f, 0.f);
+      if (row < g.ny) {
+        if (IN == 0) {
+          const float* src = (const float*)a.src[f];
+          const float u = src[(size_t)(row + 1) * g.W + e + 1];
+          if (a.back[f]) store_ghosted(a.back[f], g, row, e, u);
+          x = make_float2(u * sc, 0.f * sc);
+        } else {
+          const float2* src = (const float2*)a.src[f];
+          x = src[(size_t)row * N + e];
+        }
       }
+      v[r] = INV ? c_conj(x) : x;
     }
-    sm[(t << logN) + e] = INV ? c_conj(v) : v;
   }
-  __syncthreads();
-  block_fft(sm, logN, logB, 1, N, false, tw);
-  for (int i = threadIdx.x; i < (N << logB); i += blockDim.x) {
-    const int t = i >> logN, e = i & (N - 1);
+  block_fft_regs(v, sm, logN, logB, 1, N, false, tw);
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    int t, e;
+    out_pos(m, logN, logB, false, t, e);
     const int row = row0 + t;
     if (row >= g.ny) continue;
-    float2 v = sm[(t << logN) + e];
-    if (INV) v = c_conj(v);
+    float2 x = v[m];
+    if (INV) x = c_conj(x);
     if (OUT == 0) {
       float2* dst = (float2*)a.dst[f];
-      dst[(size_t)row * N + e] = INV ? c_scale(v, sc) : v;
+      dst[(size_t)row * N + e] = INV ? c_scale(x, sc) : x;
     } else {
       // spatial = Re(ifft) * (1/(nx ny)); the CTA that owns row r also fills the
       // ghost cells that are images of row r
-      store_ghosted((float*)a.dst[f], g, row, e, v.x * sc);
+      store_ghosted((float*)a.dst[f], g, row, e, x.x * sc);
     }
   }
 }
@@ -255,17 +327,22 @@ __global__ void __launch_bounds__(1024) k_cols(const __grid_constant__ ColArgs a
   const int W = 1 << logW;
   const int x0 = blockIdx.x << logW;
   float2* d = a.data[f];
-  for (int i = threadIdx.x; i < (N << logW); i += blockDim.x) {
-    const int y = i >> logW, w = i & (W - 1);
-    float2 v = d[(size_t)y * g.nx + x0 + w];
-    sm[i] = INV ? c_conj(v) : v;  // sm[y*W + w]
+  float2 v[8];
+  {
+    int t, j;
+    bfly_tj<8>(0, logN, logW, true, t, j);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const float2 x = d[(size_t)(j + r * (N >> 3)) * g.nx + x0 + t];
+      v[r] = INV ? c_conj(x) : x;
+    }
   }
-  __syncthreads();
-  block_fft(sm, logN, logW, W, 1, true, tw);
-  for (int i = threadIdx.x; i < (N << logW); i += blockDim.x) {
-    const int y = i >> logW, w = i & (W - 1);
-    float2 v = sm[i];
-    d[(size_t)y * g.nx + x0 + w] = INV ? c_conj(v) : v;
+  block_fft_regs(v, sm, logN, logW, W, 1, true, tw);
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    int t, y;
+    out_pos(m, logN, logW, true, t, y);
+    d[(size_t)y * g.nx + x0 + t] = INV ? c_conj(v[m]) : v[m];
   }
 }
 
@@ -435,6 +512,26 @@ __host__ __device__ inline size_t filter_fused_smem_floats(int npass) {
   const size_t ew = FILT_TX + 2 * h, eh = FILT_TY + 2 * h;
   return 2 * ew * eh + (ew + 2) * (eh + 2);
 }
+// Walk the cells of a w x h region, 256 threads, row by row without a division
+// per cell: thread i starts at cell i and advances by 256 cells.
+struct RegionWalk {
+  int r, q, dr, dq, w;
+  __device__ RegionWalk(int w_) : w(w_) {
+    r = threadIdx.x / w;
+    q = threadIdx.x - r * w;
+    dr = 256 / w;
+    dq = 256 - dr * w;
+  }
+  __device__ void next() {
+    q += dq;
+    r += dr;
+    if (q >= w) {
+      q -= w;
+      ++r;
+    }
+  }
+};
+
 __global__ void __launch_bounds__(256) k_filter_fused(const __grid_constant__ ConstFieldList S,
                                                       const __grid_constant__ FieldList D, Grid g, int npass) {
   extern __shared__ float fs[];
@@ -451,23 +548,21 @@ __global__ void __launch_bounds__(256) k_filter_fused(const __grid_constant__ Co
   const bool inner = ex0 >= 1 && ey0 >= 1 && ex0 + EW - 1 <= nx && ey0 + EH - 1 <= ny;
   if (inner) {  // the frame and its one-cell border are plain array cells
     const int RW = EW + 2, RH = EH + 2;
-    for (int i = threadIdx.x; i < RW * RH; i += blockDim.x) {
-      const int r = i / RW, q = i - r * RW;
-      raw[i] = in[(size_t)(ey0 - 1 + r) * W + (ex0 - 1 + q)];
-    }
+    RegionWalk it(RW);
+    for (; it.r < RH; it.next()) raw[it.r * RW + it.q] = in[(size_t)(ey0 - 1 + it.r) * W + (ex0 - 1 + it.q)];
     __syncthreads();
-    for (int i = threadIdx.x; i < EW * EH; i += blockDim.x) {
-      const int r = i / EW, q = i - r * EW;
-      const float* up = raw + r * RW + q;
-      s0[i] = binomial9(up, up + RW, up + 2 * RW);
+    RegionWalk jt(EW);
+    for (; jt.r < EH; jt.next()) {
+      const float* up = raw + jt.r * RW + jt.q;
+      s0[jt.r * EW + jt.q] = binomial9(up, up + RW, up + 2 * RW);
     }
   } else {  // near the domain edge: the periodic image of each frame cell, raw ghosts included
-    for (int i = threadIdx.x; i < EW * EH; i += blockDim.x) {
-      const int r = i / EW, q = i - r * EW;
-      const int yy = (((ey0 + r - 1) % ny) + ny) % ny + 1;
-      const int xx = (((ex0 + q - 1) % nx) + nx) % nx + 1;
+    RegionWalk it(EW);
+    for (; it.r < EH; it.next()) {
+      const int yy = (((ey0 + it.r - 1) % ny) + ny) % ny + 1;
+      const int xx = (((ex0 + it.q - 1) % nx) + nx) % nx + 1;
       const float* md = in + (size_t)yy * W + xx - 1;
-      s0[i] = binomial9(md - W, md, md + W);
+      s0[it.r * EW + it.q] = binomial9(md - W, md, md + W);
     }
   }
   __syncthreads();
@@ -475,9 +570,9 @@ __global__ void __launch_bounds__(256) k_filter_fused(const __grid_constant__ Co
   float* dst = s1;
   for (int p = 2; p <= npass; ++p) {
     const int m = p - 1;  // frame cells [m, EW - m) x [m, EH - m)
-    const int w = EW - 2 * m, hh = EH - 2 * m;
-    for (int i = threadIdx.x; i < w * hh; i += blockDim.x) {
-      const int r = i / w + m, q = i % w + m;
+    RegionWalk it(EW - 2 * m);
+    for (; it.r < EH - 2 * m; it.next()) {
+      const int r = it.r + m, q = it.q + m;
       const float* up = src + (r - 1) * EW + (q - 1);
       dst[r * EW + q] = binomial9(up, up + EW, up + 2 * EW);
     }
@@ -486,10 +581,10 @@ __global__ void __launch_bounds__(256) k_filter_fused(const __grid_constant__ Co
     src = dst;
     dst = t;
   }
-  for (int i = threadIdx.x; i < FILT_TX * FILT_TY; i += blockDim.x) {
-    const int r = i / FILT_TX, q = i - r * FILT_TX;
-    const int yy = y0 + r, xx = x0 + q;
-    if (yy <= ny && xx <= nx) out[(size_t)yy * W + xx] = src[(r + h) * EW + (q + h)];
+  RegionWalk it(FILT_TX);
+  for (; it.r < FILT_TY; it.next()) {
+    const int yy = y0 + it.r, xx = x0 + it.q;
+    if (yy <= ny && xx <= nx) out[(size_t)yy * W + xx] = src[(it.r + h) * EW + (it.q + h)];
   }
 }
 
@@ -557,7 +652,7 @@ template <int IN, int OUT, bool INV>
 static void launch_rows(const Grid& g, const RowArgs& a, int nf, const float2* tw, cudaStream_t st) {
   const int logB = row_logB(g.log2nx);
   const int threads = std::max(1, (g.nx << logB) / 8);
-  const size_t smem = sizeof(float2) * ((size_t)g.nx << logB);
+  const size_t smem = sizeof(float2) * fft_smem_elems(g.log2nx, logB);
   const int blocks = (g.ny + (1 << logB) - 1) >> logB;
   k_rows<IN, OUT, INV><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
 }
@@ -566,7 +661,7 @@ template <bool INV>
 static void launch_cols(const Grid& g, const ColArgs& a, int nf, const float2* tw, cudaStream_t st) {
   const int logW = col_logW(g.log2ny, g.log2nx);
   const int threads = std::max(1, (g.ny << logW) / 8);
-  const size_t smem = sizeof(float2) * ((size_t)g.ny << logW);
+  const size_t smem = sizeof(float2) * fft_smem_elems(g.log2ny, logW);
   const int blocks = g.nx >> logW;
   k_cols<INV><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
 }

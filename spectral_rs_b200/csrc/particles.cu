@@ -313,8 +313,11 @@ __host__ __device__ inline size_t eb_floats(int TX, int TY) { return (size_t)6 *
 constexpr int QCAP = 64;     // entries per queue
 constexpr int QWORDS = 7;    // words per entry
 constexpr int QWARP = 2 * QWORDS * QCAP;  // floats per warp (J queue + mover queue)
-__host__ __device__ inline size_t slot_smem_floats(int TX, int TY, bool push, bool move) {
-  const size_t win = move ? 5 * (size_t)(TX + 4) * (TY + 4) : 0;
+// Deposit window planes: Jx, Jy, Jz, rho, dens, then (compensated sums) the
+// compensation terms of Jx, Jy, Jz.
+__host__ __device__ inline int win_planes(bool move, bool comp) { return move ? (comp ? 8 : 5) : 0; }
+__host__ __device__ inline size_t slot_smem_floats(int TX, int TY, bool push, bool move, bool comp = false) {
+  const size_t win = (size_t)win_planes(move, comp) * (TX + 4) * (TY + 4);
   const size_t eb = push ? eb_floats(TX, TY) : 0;
   const size_t q = move ? (size_t)(TX * TY / 32) * QWARP : 0;
   return win + eb + q;
@@ -364,7 +367,7 @@ __device__ __noinline__ void drain_m_fn(const StepArgs& a, const SpeciesArgs& S,
 #ifndef SPX_SLOT_MIN_BLOCKS
 #define SPX_SLOT_MIN_BLOCKS 2  // resident 256-thread CTAs per SM the register budget is sized for
 #endif
-template <bool PUSH, bool MOVE>
+template <bool PUSH, bool MOVE, bool COMP = false>
 __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, float* smem) {
   const int TC = a.TX * a.TY;
   const int tx = tile % a.NTX, ty = tile / a.NTX;
@@ -382,16 +385,17 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
   float* wjz = win + 2 * WN;
   float* wrho = win + 3 * WN;
   float* wdens = win + 4 * WN;
+  constexpr int NWP = MOVE ? (COMP ? 8 : 5) : 0;  // deposit window planes
   // E/B window: tile + 1 cell
   const int EX = a.TX + 2, EY = a.TY + 2;
-  float4* eb4 = reinterpret_cast<float4*>(smem + (MOVE ? 5 * WN : 0));  // 16-byte aligned: 5*WN is a multiple of 4
+  float4* eb4 = reinterpret_cast<float4*>(smem + NWP * WN);  // 16-byte aligned: WN is a multiple of 4
   float2* eb2 = reinterpret_cast<float2*>(eb4 + EX * EY);
-  float* after_eb = smem + (MOVE ? 5 * WN : 0) + (PUSH ? 6 * EX * EY : 0);
+  float* after_eb = smem + NWP * WN + (PUSH ? 6 * EX * EY : 0);
   float* qbase = after_eb + warp * QWARP;
   float* qj = qbase;                   // [QWORDS][QCAP]
   float* qm = qbase + QWORDS * QCAP;   // [QWORDS][QCAP]
   if (MOVE)
-    for (int i = c; i < 5 * WN; i += TC) win[i] = 0.f;
+    for (int i = c; i < NWP * WN; i += TC) win[i] = 0.f;
   if (PUSH) {
     for (int i = c; i < EY * EX; i += TC) {
       const int r = i / EX, q = i - r * EX;
@@ -404,10 +408,14 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
   const int ebo = ly * EX + lx;  // top-left of this cell's 3x3 neighbourhood
   float2 accJxy[9];
   float accJz[9];
+  float2 cmpJxy[9];  // compensation terms (COMP): the low-order bits the running sums lost
+  float cmpJz[9];
 #pragma unroll
   for (int k = 0; k < 9; ++k) {
     accJxy[k] = make_float2(0.f, 0.f);
     accJz[k] = 0.f;
+    cmpJxy[k] = make_float2(0.f, 0.f);
+    cmpJz[k] = 0.f;
   }
   const size_t gc = (size_t)tile * TC + c;
   const float half_dt = 0.5f * a.p.dt;
@@ -543,8 +551,19 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
             const float2 vxy = make_float2(vx, vy);
 #pragma unroll
             for (int k = 0; k < 9; ++k) {
-              accJxy[k] = fma2(bc2(w[k]), vxy, accJxy[k]);
-              accJz[k] = __fmaf_rn(w[k], vz, accJz[k]);
+              if (COMP) {  // Kahan summation: y = w v - comp; t = acc + y; comp = (t - acc) - y
+                const float2 y = fma2(bc2(w[k]), vxy, make_float2(-cmpJxy[k].x, -cmpJxy[k].y));
+                const float2 t = add2(accJxy[k], y);
+                cmpJxy[k] = sub2(sub2(t, accJxy[k]), y);
+                accJxy[k] = t;
+                const float yz = __fmaf_rn(w[k], vz, -cmpJz[k]);
+                const float tz = __fadd_rn(accJz[k], yz);
+                cmpJz[k] = __fsub_rn(__fsub_rn(tz, accJz[k]), yz);
+                accJz[k] = tz;
+              } else {
+                accJxy[k] = fma2(bc2(w[k]), vxy, accJxy[k]);
+                accJz[k] = __fmaf_rn(w[k], vz, accJz[k]);
+              }
             }
           } else {
             jxc = ix;
@@ -637,12 +656,18 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
         atomicAdd(wjx + bl + r * WX + k, accJxy[r * 3 + k].x);
         atomicAdd(wjy + bl + r * WX + k, accJxy[r * 3 + k].y);
         atomicAdd(wjz + bl + r * WX + k, accJz[r * 3 + k]);
+        if (COMP) {  // the compensation travels with the tile flush
+          atomicAdd(win + 5 * WN + bl + r * WX + k, -cmpJxy[r * 3 + k].x);
+          atomicAdd(win + 6 * WN + bl + r * WX + k, -cmpJxy[r * 3 + k].y);
+          atomicAdd(win + 7 * WN + bl + r * WX + k, -cmpJz[r * 3 + k]);
+        }
       }
   }
   __syncthreads();
   // window -> global (clipped to the ghosted grid)
   for (int i = c; i < 5 * WN; i += TC) {
-    const float v = win[i];
+    float v = win[i];
+    if (COMP && i < 3 * WN) v += win[i + 5 * WN];  // one rounding of sum + compensation
     if (v == 0.f) continue;
     const int plane = i / WN, k = i - plane * WN;
     const int wy = k / WX, wx = k - wy * WX;
@@ -658,6 +683,13 @@ template <bool PUSH, bool MOVE>
 __global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS) k_slot(const __grid_constant__ StepArgs a) {
   extern __shared__ float smem[];
   slot_tile<PUSH, MOVE>(a, blockIdx.x, smem);
+}
+
+// Compensated current sums: the extra registers allow one 256-thread CTA per SM.
+template <bool PUSH>
+__global__ void __launch_bounds__(256, 1) k_slot_comp(const __grid_constant__ StepArgs a) {
+  extern __shared__ float smem[];
+  slot_tile<PUSH, true, true>(a, blockIdx.x, smem);
 }
 
 // Many simulations: persistent CTAs take (simulation, tile) items from a work
@@ -824,7 +856,8 @@ static SpeciesArgs species_args(Species& sp) {
 void slot_set_kernel_attributes() {
   for (const void* f : {(const void*)k_slot<true, true>, (const void*)k_slot<true, false>,
                         (const void*)k_slot<false, true>, (const void*)k_slot_batch<true, true>,
-                        (const void*)k_slot_batch<true, false>, (const void*)k_slot_batch<false, true>})
+                        (const void*)k_slot_batch<true, false>, (const void*)k_slot_batch<false, true>,
+                        (const void*)k_slot_comp<true>, (const void*)k_slot_comp<false>})
     SPX_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
 }
 
@@ -847,8 +880,13 @@ int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysPar
     if (move) SPX_CUDA_TRY(cudaMemsetAsync(sp[s].slot.ocount + (sp[s].slot.ocur ^ 1), 0, sizeof(uint32_t), st));
   }
   const int TC = pg.TC();
-  const size_t smem = slot_smem_floats(pg.TX, pg.TY, push, move) * sizeof(float);
-  if (push && move)
+  const bool comp = pp.compensated && move;
+  const size_t smem = slot_smem_floats(pg.TX, pg.TY, push, move, comp) * sizeof(float);
+  if (comp && push)
+    k_slot_comp<true><<<pg.ntiles(), TC, smem, st>>>(a);
+  else if (comp)
+    k_slot_comp<false><<<pg.ntiles(), TC, smem, st>>>(a);
+  else if (push && move)
     k_slot<true, true><<<pg.ntiles(), TC, smem, st>>>(a);
   else if (push)
     k_slot<true, false><<<pg.ntiles(), TC, smem, st>>>(a);

@@ -77,6 +77,7 @@ struct ParticleGeom {
 struct PhysParams {
   float dt, c, csqinv;
   int periodic_x, left_wall, wall_loc, delta;
+  int compensated;  // compensated (Kahan) current sums in the split-path kernel
 };
 
 struct FieldPtrs {

@@ -23,13 +23,28 @@ from .config import Config
 from .init import species_arrays
 
 
+def _tile_choice(cfg, tile):
+    """(tile_x, tile_y) for spx_params: explicit, autotuned, or from the config (0 = library rule)."""
+    p = cfg.params
+    if tile is None:
+        return p.tile_x, p.tile_y
+    if tile == "auto":
+        from .tune import autotune_tiles
+        crop = (min(p.size_x, 1024), min(p.size_y, 256)) if p.periodic_x else None
+        return autotune_tiles(p, cfg.species_list(), crop=crop)[0]
+    return int(tile[0]), int(tile[1])
+
+
 class Sim:
     """Owns one device context (``spx_ctx``)."""
 
-    def __init__(self, cfg: Config, path=None):
+    def __init__(self, cfg: Config, path=None, tile=None):
+        """path: "split" / "plain" overrides the config; tile: (tx, ty), or "auto" for the
+        autotuner (spectral_rs_b200.tune), or None for the config's / the library's choice."""
         self.lib = _lib.load()
         self.config = cfg
         p = cfg.params
+        tx, ty = _tile_choice(cfg, tile)
         self.t = 0
         self.t_final = cfg.setup.t_final
         self.size_x, self.size_y, self.delta = p.size_x, p.size_y, p.delta
@@ -41,7 +56,8 @@ class Sim:
             gamma_inj=p.gamma_inj, n_pass=p.n_pass, periodic_x=1 if p.periodic_x else 0,
             left_wall=1 if p.left_wall else 0,
             path=_lib.PATH_PLAIN if (path or p.path) == "plain" else _lib.PATH_SPLIT,
-            tile_x=p.tile_x, tile_y=p.tile_y, slot_capacity=p.slot_capacity, device=0)
+            tile_x=tx, tile_y=ty, slot_capacity=p.slot_capacity, device=0,
+            compensated=1 if p.compensated else 0)
         self._ctx = ctypes.c_void_p()
         _lib.check(self.lib.spx_create(ctypes.byref(prm), ctypes.byref(self._ctx)))
         self.flds = Flds(self)
@@ -271,15 +287,22 @@ class Batch:
     """Independent simulations advanced together (spx_batch_*): one persistent
     particle launch over all (simulation, tile) items and one CUDA graph per step."""
 
-    def __init__(self, cfgs):
+    def __init__(self, cfgs, tile=None):
+        """tile: (tx, ty) for every member, "auto" (tuned on the member with the most
+        particles), or None (the configs' / the library's choice)."""
         self.lib = _lib.load()
         prms = (_lib.SpxParams * len(cfgs))()
+        shape = None
+        if tile is not None:
+            big = max(cfgs, key=lambda c: sum(s.ppc for s in c.species_list()) * c.params.size_x * c.params.size_y)
+            shape = _tile_choice(big, tile)
         for i, cfg in enumerate(cfgs):
             p = cfg.params
+            tx, ty = shape if shape else (p.tile_x, p.tile_y)
             prms[i] = _lib.SpxParams(
                 size_x=p.size_x, size_y=p.size_y, delta=p.delta, dt=p.dt, c=p.c, dens=p.dens,
                 gamma_inj=p.gamma_inj, n_pass=p.n_pass, periodic_x=1 if p.periodic_x else 0,
-                left_wall=1 if p.left_wall else 0, path=_lib.PATH_SPLIT, tile_x=p.tile_x, tile_y=p.tile_y,
+                left_wall=1 if p.left_wall else 0, path=_lib.PATH_SPLIT, tile_x=tx, tile_y=ty,
                 slot_capacity=p.slot_capacity, device=0)
         self._b = ctypes.c_void_p()
         code = self.lib.spx_batch_create(len(cfgs), prms, ctypes.byref(self._b))

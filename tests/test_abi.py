@@ -29,10 +29,20 @@ def test_library_exports_every_declared_symbol():
     assert exported == declared()
 
 
-def test_params_struct_layout_matches_header():
-    # the ctypes mirror must have the C struct's size: 3 u64 + 2 f32 + u32 + f32 + u32 + 7 i32 = 72 bytes
+def test_params_struct_layout_matches_header(tmp_path):
+    # the ctypes mirror must match the C struct field by field: compile the header and compare offsets
     from spectral_rs_b200 import _lib
-    assert ctypes.sizeof(_lib.SpxParams) == 72
+    names = [f[0] for f in _lib.SpxParams._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text("#include <stdio.h>\n#include <stddef.h>\n#include \"spectral_gpu.h\"\nint main(void) {\n"
+                   + f'  printf("%zu\\n", sizeof(spx_params));\n'
+                   + "".join(f'  printf("%zu\\n", offsetof(spx_params, {n}));\n' for n in names)
+                   + "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert got[0] == ctypes.sizeof(_lib.SpxParams)
+    assert got[1:] == [getattr(_lib.SpxParams, n).offset for n in names]
 
 
 def test_errors_without_device_are_reported_not_crashing():

@@ -1,8 +1,9 @@
 """Precision study (symmetric two-stream electron beams): GPU FP32 against the FP64 oracle.
 
 tests/golden/two_stream_energy.json holds the field-energy history of the
-FP64 and FP32 oracle runs (tests/golden/make_two_stream.py).  The GPU split and
-plain paths start from the same seeded particles and run the same 2000 steps.
+FP64 and FP32 oracle runs (tests/golden/make_two_stream.py).  The GPU split path
+(with plain and with compensated current sums) and the plain path start from the
+same seeded particles and run the same 2000 steps.
 Reported (printed with -s): the linear growth rate of the field energy and the
 relative field-energy error against FP64 over time.  The instability amplifies
 rounding differences exponentially, so after saturation the runs decorrelate;
@@ -30,7 +31,9 @@ def _run_gpu(path):
         study = json.load(f)["study"]
     mts.STUDY.update(study)
     p, bs = mts.beams(study)
-    with Sim(Config(p, Setup(study["steps"]), Output(False, False, 1, 1, 1, 1)), path=path) as sim:
+    p.compensated = path == "split_compensated"
+    with Sim(Config(p, Setup(study["steps"]), Output(False, False, 1, 1, 1, 1)),
+             path="plain" if path == "plain" else "split") as sim:
         for a in bs:
             sim.add_species(-1.0, 1.0, study["vth"], a["ix"], a["iy"], a["dx"], a["dy"], a["px"], a["py"], a["pz"],
                             a["psa"])
@@ -56,7 +59,7 @@ def ref():
         return json.load(f)
 
 
-@pytest.mark.parametrize("path", ["split", "plain"])
+@pytest.mark.parametrize("path", ["split", "split_compensated", "plain"])
 def test_two_stream_energy_vs_fp64(ref, path):
     e_gpu, study = _run_gpu(path)
     e64 = np.array(ref["fp64"]["E"])
