@@ -83,6 +83,8 @@ def params(w, **over):
              vth=sp[0]["vth"], periodic_x=w["periodic_x"], left_wall=w["left_wall"])
     if w.get("tile"):
         d["tile_x"], d["tile_y"] = w["tile"]
+    if w.get("compensated"):
+        d["compensated"] = True
     d.update(over)
     return Params(**d)
 
@@ -262,8 +264,11 @@ def e2e_run(w, steps, seed):
     for sp, a in host:
         sim.add_species(sp["q"], sp["m"], sp["vth"], a["ix"], a["iy"], a["dx"], a["dy"], a["px"], a["py"], a["pz"],
                         a["psa"])
+    t1 = time.perf_counter()
     sim.prepare()
+    t2 = time.perf_counter()
     sim.step(steps)
+    t3 = time.perf_counter()
     out = [sim.flds.spatial(name, with_ghosts=False) for name in
            ("Jx", "Jy", "Jz", "Ex", "Ey", "Ez", "Bx", "By", "Bz", "Dens")]
     d = sim.diag()
@@ -273,6 +278,7 @@ def e2e_run(w, steps, seed):
     sim.close()
     return {"value": n * steps / dt, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d / steps,
             "d2h_bytes_per_step": d2h / steps, "wall_s": dt,
+            "split_s": {"upload": t1 - t0, "prepare": t2 - t1, "steps": t3 - t2, "readback": t0 + dt - t3},
             "scope": "host arrays -> spx_add_species x2 -> spx_prepare -> spx_step(K) -> 10 fields + diag to host"}
 
 
@@ -327,6 +333,12 @@ def run_gpu(args, w):
     achieved = alg_bytes / (kern_ms / 1e3) / 1e9
     traffic = traffic_per_launch(n_particles, cells)
 
+    # end to end through the public API, next on the clean device; rank 0 only (the pinned
+    # host copy of the workload is 21 GB per rank)
+    e2e = e2e_run(w, args.steps, seed) if rank == 0 and not args.no_e2e else None
+    if e2e is not None:
+        e2e["ranks_measured"] = 1
+
     plain = None
     if not args.no_plain and rank == 0:
         ps = make_sim(w, "plain", seed)
@@ -346,13 +358,10 @@ def run_gpu(args, w):
                  "path": "plain FP32 (global x = ix + dx, per-phase kernels, global atomics, no sort)"}
 
     cpu = None
-    e2e = None
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, cores, sample, _ = oracle_crop_rate(w, args.cpu_seconds)
         cpu = {"value": rate, "unit": "particle-steps/s", "cores": cores, "kind": "port",
                "sample": sample + " (C++ restatement of the reference CPU path, OpenMP push/FFT, serial deposit)"}
-    if rank == 0 and not args.no_e2e:
-        e2e = e2e_run(w, args.steps, seed)
 
     if rank == 0:
         line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
@@ -493,6 +502,9 @@ def main():
     ap.add_argument("--small", action="store_true", help="1/16 of the workload (quick checks)")
     ap.add_argument("--workload", default="thermal", choices=sorted(WORKLOADS) + ["ensemble"])
     ap.add_argument("--tile", default=None, help="split-path tile shape TXxTY (default: the library's choice)")
+    ap.add_argument("--compensated", action="store_true", help="Kahan-compensated current sums (split path)")
+    ap.add_argument("--ppc", type=int, default=None,
+                    help="particles per cell of every species (field-phase profiling on the full grid)")
     ap.add_argument("--ensemble", type=int, default=64, help="members of the batched ensemble")
     args = ap.parse_args()
     if args.workload == "ensemble":
@@ -504,6 +516,12 @@ def main():
         w.update(size_x=sx, size_y=sy, name=f"{w['name']}_small_{sx}x{sy}")
     if args.tile:
         w["tile"] = tuple(int(v) for v in args.tile.lower().split("x"))
+    if args.compensated:
+        w["compensated"] = True
+        w["name"] += "_compensated"
+    if args.ppc:
+        w["species"] = [dict(sp, ppc=args.ppc) for sp in w["species"]]
+        w["name"] += f"_ppc{args.ppc}"
     if args.impl == "reference":
         run_reference(args, w)
     else:
