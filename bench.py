@@ -261,9 +261,12 @@ def e2e_run(w, steps, seed):
     sim = Sim(cfg)
     h2d = sum(a["ix"].nbytes + a["iy"].nbytes + 6 * a["dx"].nbytes for (_, a) in host)
     t0 = time.perf_counter()
+    per_species = []
     for sp, a in host:
+        ts = time.perf_counter()
         sim.add_species(sp["q"], sp["m"], sp["vth"], a["ix"], a["iy"], a["dx"], a["dy"], a["px"], a["py"], a["pz"],
                         a["psa"])
+        per_species.append(time.perf_counter() - ts)
     t1 = time.perf_counter()
     sim.prepare()
     t2 = time.perf_counter()
@@ -278,7 +281,8 @@ def e2e_run(w, steps, seed):
     sim.close()
     return {"value": n * steps / dt, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d / steps,
             "d2h_bytes_per_step": d2h / steps, "wall_s": dt,
-            "split_s": {"upload": t1 - t0, "prepare": t2 - t1, "steps": t3 - t2, "readback": t0 + dt - t3},
+            "split_s": {"upload": t1 - t0, "upload_per_species": per_species, "prepare": t2 - t1, "steps": t3 - t2,
+                        "readback": t0 + dt - t3},
             "scope": "host arrays -> spx_add_species x2 -> spx_prepare -> spx_step(K) -> 10 fields + diag to host"}
 
 

@@ -171,7 +171,7 @@ SPX_API int spx_diag(spx_ctx* ctx, double* out5);
  * Fft2D methods, used by the known-answer tests): op 0 = deposit_ghosts,
  * 1 = update_ghosts, 2 = n_pass x binomial_filter_2_d (one kernel per pass),
  * 3 = the same through the fused n-pass kernel of spx_fields_update
- * (1 <= n_pass <= 27).  In/out in place. */
+ * (1 <= n_pass <= 16).  In/out in place. */
 SPX_API int spx_field_op(uint64_t size_x, uint64_t size_y, int32_t op, uint32_t n_pass, float* spatial_with_ghosts);
 /* Fft2D::fft / inv_fft (src/flds/fft_2d.rs:91-172) on a size_y*size_x
  * interleaved complex array, in place; inverse includes the 1/(nx*ny) scale.

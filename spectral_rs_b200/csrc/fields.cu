@@ -484,7 +484,10 @@ __global__ void k_filter(const __grid_constant__ ConstFieldList S, const __grid_
   out[r * W + c] = v;
 }
 
-constexpr int FILT_TX = 64, FILT_TY = 16;  // output tile of the fused filter
+// Fused filter geometry: the extended frame of a tile is 64 columns wide (one
+// per lane of a 64-thread row group; 4 row groups = 256 threads), the output
+// tile is 64 - 2h columns by FILT_TY rows, h = n_pass - 1 (up to 15).
+constexpr int FILT_EW = 64, FILT_TY = 32, FILT_MAX_PASS = 16;
 
 // binomial_filter_2_d's stencil at the cell whose 3x3 neighbourhood rows start
 // at up, md, dn (left column): reference summation order, no contraction.
@@ -505,32 +508,35 @@ __device__ __forceinline__ float binomial9(const float* up, const float* md, con
 // after another, each followed by update_ghosts, src/flds/mod.rs:90-94).  Pass
 // 1 reads the raw ghosted input around each cell's periodic image; after it
 // every neighbour is a periodic image, so passes 2..n run on a shared-memory
-// tile whose halo shrinks by one cell per pass.  Writes the interior of `out`;
-// each value is computed exactly as the separate passes compute it.
+// frame whose halo shrinks by one cell per pass.  Each lane owns one column of
+// the frame and walks a chunk of rows keeping the last two rows of its 3x3
+// neighbourhood in registers (3 shared loads per cell).  Writes the interior of
+// `out`; each value is computed exactly as the separate passes compute it.
 __host__ __device__ inline size_t filter_fused_smem_floats(int npass) {
   const int h = npass - 1;
-  const size_t ew = FILT_TX + 2 * h, eh = FILT_TY + 2 * h;
-  return 2 * ew * eh + (ew + 2) * (eh + 2);
+  const size_t eh = FILT_TY + 2 * h;
+  return 2 * (size_t)FILT_EW * eh + (FILT_EW + 2) * (eh + 2);
 }
-// Walk the cells of a w x h region, 256 threads, row by row without a division
-// per cell: thread i starts at cell i and advances by 256 cells.
-struct RegionWalk {
-  int r, q, dr, dq, w;
-  __device__ RegionWalk(int w_) : w(w_) {
-    r = threadIdx.x / w;
-    q = threadIdx.x - r * w;
-    dr = 256 / w;
-    dq = 256 - dr * w;
+
+// One pass over frame rows [r0, r1) of column q (src row pitch sp; the 3x3
+// neighbourhood of frame cell (r, q) is src[(r - 1 + dr) * sp + q - 1 + dq]).
+__device__ __forceinline__ void filter_column(const float* src, int sp, float* dst, int dp, int q, int r0, int r1) {
+  if (r0 >= r1) return;
+  const float* s = src + q - 1;
+  float a0 = s[(r0 - 1) * sp], a1 = s[(r0 - 1) * sp + 1], a2 = s[(r0 - 1) * sp + 2];
+  float b0 = s[r0 * sp], b1 = s[r0 * sp + 1], b2 = s[r0 * sp + 2];
+  for (int r = r0; r < r1; ++r) {
+    const float c0 = s[(r + 1) * sp], c1 = s[(r + 1) * sp + 1], c2 = s[(r + 1) * sp + 2];
+    const float up[3] = {a0, a1, a2}, md[3] = {b0, b1, b2}, dn[3] = {c0, c1, c2};
+    dst[r * dp + q] = binomial9(up, md, dn);
+    a0 = b0;
+    a1 = b1;
+    a2 = b2;
+    b0 = c0;
+    b1 = c1;
+    b2 = c2;
   }
-  __device__ void next() {
-    q += dq;
-    r += dr;
-    if (q >= w) {
-      q -= w;
-      ++r;
-    }
-  }
-};
+}
 
 __global__ void __launch_bounds__(256) k_filter_fused(const __grid_constant__ ConstFieldList S,
                                                       const __grid_constant__ FieldList D, Grid g, int npass) {
@@ -539,30 +545,38 @@ __global__ void __launch_bounds__(256) k_filter_fused(const __grid_constant__ Co
   float* out = D.f[blockIdx.z];
   const int W = g.W, nx = g.nx, ny = g.ny;
   const int h = npass - 1;
-  const int EW = FILT_TX + 2 * h, EH = FILT_TY + 2 * h;
-  const int x0 = blockIdx.x * FILT_TX + 1, y0 = blockIdx.y * FILT_TY + 1;  // first interior cell of the tile
-  const int ex0 = x0 - h, ey0 = y0 - h;                                    // origin of the extended frame
+  const int TW = FILT_EW - 2 * h;                // output tile width
+  const int EW = FILT_EW, EH = FILT_TY + 2 * h;  // frame
+  const int x0 = blockIdx.x * TW + 1, y0 = blockIdx.y * FILT_TY + 1;  // first interior cell of the tile
+  const int ex0 = x0 - h, ey0 = y0 - h;                               // origin of the frame
+  const int q = threadIdx.x & 63, grp = threadIdx.x >> 6;
   float* s0 = fs;
   float* s1 = fs + EW * EH;
   float* raw = fs + 2 * EW * EH;
   const bool inner = ex0 >= 1 && ey0 >= 1 && ex0 + EW - 1 <= nx && ey0 + EH - 1 <= ny;
-  if (inner) {  // the frame and its one-cell border are plain array cells
+  // rows [lo, hi) of a region split into 4 chunks, one per row group
+  auto chunk = [&](int lo, int hi, int& r0, int& r1) {
+    const int n = (hi - lo + 3) >> 2;
+    r0 = min(hi, lo + grp * n);
+    r1 = min(hi, r0 + n);
+  };
+  if (inner) {  // the frame and its one-cell border are plain array cells: raw (EW+2) x (EH+2)
     const int RW = EW + 2, RH = EH + 2;
-    RegionWalk it(RW);
-    for (; it.r < RH; it.next()) raw[it.r * RW + it.q] = in[(size_t)(ey0 - 1 + it.r) * W + (ex0 - 1 + it.q)];
-    __syncthreads();
-    RegionWalk jt(EW);
-    for (; jt.r < EH; jt.next()) {
-      const float* up = raw + jt.r * RW + jt.q;
-      s0[jt.r * EW + jt.q] = binomial9(up, up + RW, up + 2 * RW);
+    for (int r = grp; r < RH; r += 4) {
+      const float* row = in + (size_t)(ey0 - 1 + r) * W + (ex0 - 1);
+      raw[r * RW + q] = row[q];
+      if (q < 2) raw[r * RW + 64 + q] = row[64 + q];
     }
+    __syncthreads();
+    int r0, r1;
+    chunk(0, EH, r0, r1);
+    filter_column(raw + RW + 1, RW, s0, EW, q, r0, r1);  // frame cell (r, q) = raw cell (r + 1, q + 1)
   } else {  // near the domain edge: the periodic image of each frame cell, raw ghosts included
-    RegionWalk it(EW);
-    for (; it.r < EH; it.next()) {
-      const int yy = (((ey0 + it.r - 1) % ny) + ny) % ny + 1;
-      const int xx = (((ex0 + it.q - 1) % nx) + nx) % nx + 1;
+    const int xx = (((ex0 + q - 1) % nx) + nx) % nx + 1;
+    for (int r = grp; r < EH; r += 4) {
+      const int yy = (((ey0 + r - 1) % ny) + ny) % ny + 1;
       const float* md = in + (size_t)yy * W + xx - 1;
-      s0[it.r * EW + it.q] = binomial9(md - W, md, md + W);
+      s0[r * EW + q] = binomial9(md - W, md, md + W);
     }
   }
   __syncthreads();
@@ -570,21 +584,22 @@ __global__ void __launch_bounds__(256) k_filter_fused(const __grid_constant__ Co
   float* dst = s1;
   for (int p = 2; p <= npass; ++p) {
     const int m = p - 1;  // frame cells [m, EW - m) x [m, EH - m)
-    RegionWalk it(EW - 2 * m);
-    for (; it.r < EH - 2 * m; it.next()) {
-      const int r = it.r + m, q = it.q + m;
-      const float* up = src + (r - 1) * EW + (q - 1);
-      dst[r * EW + q] = binomial9(up, up + EW, up + 2 * EW);
-    }
+    int r0, r1;
+    chunk(m, EH - m, r0, r1);
+    if (q >= m && q < EW - m) filter_column(src, EW, dst, EW, q, r0, r1);
     __syncthreads();
     float* t = src;
     src = dst;
     dst = t;
   }
-  RegionWalk it(FILT_TX);
-  for (; it.r < FILT_TY; it.next()) {
-    const int yy = y0 + it.r, xx = x0 + it.q;
-    if (yy <= ny && xx <= nx) out[(size_t)yy * W + xx] = src[(it.r + h) * EW + (it.q + h)];
+  if (q >= h && q < h + TW) {
+    const int xx = x0 + q - h;
+    if (xx <= nx)
+      for (int r = grp; r < FILT_TY; r += 4) {
+        const int yy = y0 + r;
+        if (yy > ny) break;
+        out[(size_t)yy * W + xx] = src[(r + h) * EW + q];
+      }
   }
 }
 
@@ -609,9 +624,7 @@ void launch_update_ghosts(const Grid& g, float* const* fields, int nf, cudaStrea
   k_update_ghosts<<<dim3((nper + 255) / 256, nf), 256, 0, st>>>(L, g);
 }
 
-bool filter_fused_fits(uint32_t npass) {
-  return npass >= 1 && filter_fused_smem_floats((int)npass) * sizeof(float) <= 96 * 1024;
-}
+bool filter_fused_fits(uint32_t npass) { return npass >= 1 && npass <= (uint32_t)FILT_MAX_PASS; }
 
 void launch_filter_fused(const Grid& g, float* const* src, float* const* dst, int nf, uint32_t npass,
                          cudaStream_t st) {
@@ -622,7 +635,8 @@ void launch_filter_fused(const Grid& g, float* const* src, float* const* dst, in
     D.f[i] = dst[i];
   }
   const size_t smem = filter_fused_smem_floats((int)npass) * sizeof(float);
-  dim3 grd((g.nx + FILT_TX - 1) / FILT_TX, (g.ny + FILT_TY - 1) / FILT_TY, nf);
+  const int tw = FILT_EW - 2 * ((int)npass - 1);
+  dim3 grd((g.nx + tw - 1) / tw, (g.ny + FILT_TY - 1) / FILT_TY, nf);
   k_filter_fused<<<grd, 256, smem, st>>>(S, D, g, (int)npass);
 }
 

@@ -49,13 +49,13 @@ def test_gpu_filter_raw_ghosts_bit_exact(nx, ny):
     assert np.array_equal(_lib().field_op(nx, ny, 0, x), orc.field_op(nx, ny, 0, x, dtype=np.float32))
 
 
-@pytest.mark.parametrize("nx,ny", [(24, 12), (8, 8), (64, 16), (200, 40), (512, 64), (4096, 32)])
+@pytest.mark.parametrize("nx,ny", [(24, 12), (8, 8), (64, 16), (200, 40), (512, 64), (4096, 32), (1024, 256)])
 def test_gpu_fused_filter_bit_exact(nx, ny):
     # all passes in one kernel (the Flds::update path): identical to the passes one by one,
     # the first one reading the raw ghost frame; tiles inside the grid and tiles at its edges
     rng = np.random.default_rng(nx + 13 * ny)
     x = rng.standard_normal((ny + 2) * (nx + 2)).astype(np.float32)
-    for npass in (1, 2, 4, 8):
+    for npass in (1, 2, 4, 8, 16):
         assert np.array_equal(_lib().field_op(nx, ny, 3, x, n_pass=npass),
                               orc.field_op(nx, ny, 2, x, n_pass=npass, dtype=np.float32)), npass
 
