@@ -299,6 +299,12 @@ def run_gpu(args, w):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     seed = rank_seed(args.seed, rank)
 
+    # end to end through the public API, first, on the clean device; rank 0 only (the pinned
+    # host copy of the workload is 21 GB per rank)
+    e2e = e2e_run(w, args.steps, seed) if rank == 0 and not args.no_e2e else None
+    if e2e is not None:
+        e2e["ranks_measured"] = 1
+
     sim = make_sim(w, "split", seed)
     n_particles = sum(len(p) for p in sim.prtls)
     cells = w["size_x"] * w["size_y"]
@@ -337,11 +343,6 @@ def run_gpu(args, w):
     achieved = alg_bytes / (kern_ms / 1e3) / 1e9
     traffic = traffic_per_launch(n_particles, cells)
 
-    # end to end through the public API, next on the clean device; rank 0 only (the pinned
-    # host copy of the workload is 21 GB per rank)
-    e2e = e2e_run(w, args.steps, seed) if rank == 0 and not args.no_e2e else None
-    if e2e is not None:
-        e2e["ranks_measured"] = 1
 
     plain = None
     if not args.no_plain and rank == 0:

@@ -223,9 +223,12 @@ __host__ __device__ inline int row_logB(int logN) {
   return lb < 0 ? 0 : lb;
 }
 // Column pass: strip of W = 2^logW columns, blockDim = Ny*W/8 threads (<= 1024).
+// 512 threads (two CTAs per SM at 64 registers) while the strip is at least 4
+// columns (32-byte row segments), else 1024 threads; >= 256 for short columns.
 __host__ __device__ inline int col_logW(int logNy, int logNx) {
-  int lw = logNy >= 7 ? 13 - logNy : 11 - logNy;  // <= 1024 threads, >= 256 for short columns
-  if (lw > 4 && logNy >= 7) lw = 4;               // 16 columns = 128 B row segments
+  int lw = logNy >= 7 ? 12 - logNy : 11 - logNy;
+  if (logNy >= 7 && lw < 2) lw = 13 - logNy;
+  if (lw > 4 && logNy >= 7) lw = 4;  // 16 columns = 128 B row segments
   if (lw < 0) lw = 0;
   if (lw > logNx) lw = logNx;
   return lw;
@@ -276,22 +279,27 @@ __global__ void __launch_bounds__(1024) k_rows(const __grid_constant__ RowArgs a
     int t, j;
     bfly_tj<8>(0, logN, logB, false, t, j);
     const int row = row0 + t;
+    if (IN == 0) {
+      // all 8 loads first, then the write-back stores (which may not be reordered above them)
+      const float* __restrict__ src = (const float*)a.src[f];
+      float u[8];
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const int e = j + r * (N >> 3);
-      float2 x = make_float2(0.f, 0.f);
-      if (row < g.ny) {
-        if (IN == 0) {
-          const float* src = (const float*)a.src[f];
-          const float u = src[(size_t)(row + 1) * g.W + e + 1];
-          if (a.back[f]) store_ghosted(a.back[f], g, row, e, u);
-          x = make_float2(u * sc, 0.f * sc);
-        } else {
-          const float2* src = (const float2*)a.src[f];
-          x = src[(size_t)row * N + e];
-        }
+      for (int r = 0; r < 8; ++r) u[r] = row < g.ny ? src[(size_t)(row + 1) * g.W + j + r * (N >> 3) + 1] : 0.f;
+      if (a.back[f] && row < g.ny)
+#pragma unroll
+        for (int r = 0; r < 8; ++r) store_ghosted(a.back[f], g, row, j + r * (N >> 3), u[r]);
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const float2 x = make_float2(u[r] * sc, 0.f * sc);
+        v[r] = INV ? c_conj(x) : x;
       }
-      v[r] = INV ? c_conj(x) : x;
+    } else {
+      const float2* __restrict__ src = (const float2*)a.src[f];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const float2 x = row < g.ny ? src[(size_t)row * N + j + r * (N >> 3)] : make_float2(0.f, 0.f);
+        v[r] = INV ? c_conj(x) : x;
+      }
     }
   }
   block_fft_regs(v, sm, logN, logB, 1, N, false, tw);
