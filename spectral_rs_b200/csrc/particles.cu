@@ -433,8 +433,9 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
     float* __restrict__ spz = S.pz + tb;
     uint32_t* __restrict__ stg = S.tag + tb;
     const int nlow = (int)S.nlow[gc], nin = (int)S.ain[gc];
-    const int wl = __reduce_max_sync(0xffffffffu, nlow);
-    const int rounds = wl + __reduce_max_sync(0xffffffffu, nin);
+    // each lane walks its low range and then its arrivals without a gap: the warp runs
+    // max(nlow + nin) rounds instead of max(nlow) + max(nin)
+    const int rounds = __reduce_max_sync(0xffffffffu, nlow + nin);
     const int KL = S.KL, rin = S.rin;
     int kept = 0;  // particles kept so far (moving steps): the next low-range slot
     const float q = S.charge, beta = S.beta, alpha = S.alpha;
@@ -444,12 +445,8 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
     int nq_j = 0, nq_m = 0;  // warp-uniform queue sizes
 
     auto slot_of = [&](int r, bool& act) -> int {
-      if (r < wl) {
-        act = r < nlow;
-        return r;
-      }
-      act = (r - wl) < nin;
-      return rin + (r - wl);
+      act = r < nlow + nin;
+      return r < nlow ? r : rin + (r - nlow);
     };
     // drain the J queue: deposit the stencils whose centre left the owner cell
     auto drain_j = [&]() {
