@@ -319,3 +319,42 @@ def test_device_init_statistics():
         assert abs(np.mean(st["py"])) < 0.01
         # every cell holds exactly ppc particles, in reference order
         assert np.all(np.bincount((st["iy"] - 1) * 64 + (st["ix"] - 1)) == 16)
+
+
+def test_run_writes_the_reference_output_layout(tmp_path):
+    """run() with write_output: output/dat_NNNNN/{x,y,u,gam}.npy (species 0, every stride-th
+    particle) and flds/*.npy (interior, 1-D) at every output_interval (src/save/mod.rs:8-80).
+    The t = 0 dump follows the pre-loop move: positions bit-exact with the oracle, sources
+    within the deposit tolerance."""
+    import os
+    from spectral_rs_b200 import run
+    from spectral_rs_b200.config import Config, Setup, Output
+    from spectral_rs_b200.init import species_arrays
+    from spectral_rs_b200.save import SAVED_FIELDS
+    p = test_params(size_x=64, size_y=32, delta=0, c=3.0, dt=0.1, dens=8, periodic_x=True, n_pass=4,
+                    random_positions=True, seed=5, mass_ratio=16.0, vth=0.1, gamma_inj=1.0050378)
+    cfg = Config(p, Setup(10), Output(False, True, 1, 5, 3, 1))
+    out = str(tmp_path / "output")
+    run(cfg, out_dir=out)
+    assert sorted(os.listdir(out)) == ["dat_00000", "dat_00001", "dat_00002"]
+    o = orc.OracleSim.from_params(p, dtype=np.float32)
+    for k, spec in enumerate(cfg.species_list()):
+        a = species_arrays(p, spec, seed_offset=k)
+        o.add_species(spec.charge, spec.mass, spec.vth, a["ix"], a["iy"], a["dx"], a["dy"], a["px"], a["py"], a["pz"],
+                      a["psa"])
+    o.prepare()
+    r = o.state(0)
+    d0 = os.path.join(out, "dat_00000")
+    x = np.load(os.path.join(d0, "x.npy"))
+    assert x.dtype == np.float32 and len(x) == (len(r["ix"]) + 2) // 3
+    assert np.array_equal(x, (r["ix"].astype(np.float32) + r["dx"])[::3])
+    assert np.array_equal(np.load(os.path.join(d0, "y.npy")), (r["iy"].astype(np.float32) + r["dy"])[::3])
+    assert np.array_equal(np.load(os.path.join(d0, "u.npy")), (r["px"] / np.float32(p.c))[::3])
+    assert np.array_equal(np.load(os.path.join(d0, "gam.npy")), r["psa"][::3])
+    for name in SAVED_FIELDS:
+        f = np.load(os.path.join(d0, "flds", f"{name}.npy"))
+        assert f.shape == (p.size_x * p.size_y,) and f.dtype == np.float32
+        ref = o.spatial(name).reshape(p.size_y + 2, p.size_x + 2)[1:-1, 1:-1].reshape(-1)
+        assert np.max(np.abs(f - ref)) <= DEP_RTOL * max(float(np.max(np.abs(ref))), 1e-30) + 1e-30, name
+    for d in ("dat_00001", "dat_00002"):
+        assert len(np.load(os.path.join(out, d, "gam.npy"))) == len(x)
