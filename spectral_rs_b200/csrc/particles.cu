@@ -369,7 +369,21 @@ __device__ __noinline__ void drain_m_fn(const StepArgs& a, const SpeciesArgs& S,
 #ifndef SPX_SLOT_MIN_BLOCKS
 #define SPX_SLOT_MIN_BLOCKS 2  // resident 256-thread CTAs per SM the register budget is sized for
 #endif
-template <bool PUSH, bool MOVE, bool COMP = false>
+// apply_bc of a grid periodic in x as well as y (the reference's `periodic`
+// feature) when the kernel knows it at compile time.
+__device__ __forceinline__ void periodic_bc(int nx, int ny, int& ix, int& iy) {
+  if (iy < 1)
+    iy += ny;
+  else if (iy > ny)
+    iy -= ny;
+  if (ix < 1)
+    ix += nx;
+  else if (ix > nx)
+    ix -= nx;
+}
+
+// PX: the grid is periodic in x (compile time; the generic form reads a.p).
+template <bool PUSH, bool MOVE, bool COMP = false, bool PX = false>
 __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, float* smem) {
   const int TC = a.TX * a.TY;
   const int tx = tile % a.NTX, ty = tile / a.NTX;
@@ -535,7 +549,10 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
           const float c1 = half_dt * inv;
           // first half: position, boundaries, current (src/lib.rs:480-484)
           move_half(c1, px, py, ix, iy, dx, dy);
-          apply_bc(a.p, nx, ny, ix, iy, dx, px, a.derr);
+          if (PX)
+            periodic_bc(nx, ny, ix, iy);
+          else
+            apply_bc(a.p, nx, ny, ix, iy, dx, px, a.derr);
           {
             const float2 vxy = mul2(mul2(bc2(q), make_float2(px, py)), bc2(inv));
             vx = vxy.x;
@@ -572,7 +589,10 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
           }
           // second half: position, boundaries, density (src/lib.rs:486-488)
           move_half(c1, px, py, ix, iy, dx, dy);
-          apply_bc(a.p, nx, ny, ix, iy, dx, px, a.derr);
+          if (PX)
+            periodic_bc(nx, ny, ix, iy);
+          else
+            apply_bc(a.p, nx, ny, ix, iy, dx, px, a.derr);
           // a particle that stays but finds the low range full joins its own
           // cell's arrivals like a mover
           mover = ix != ox || iy != oy || kept >= KL;
@@ -678,17 +698,33 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
 }
 
 // One simulation: one CTA per tile.
-template <bool PUSH, bool MOVE>
+template <bool PUSH, bool MOVE, bool PX>
 __global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS) k_slot(const __grid_constant__ StepArgs a) {
   extern __shared__ float smem[];
-  slot_tile<PUSH, MOVE>(a, blockIdx.x, smem);
+  slot_tile<PUSH, MOVE, false, PX>(a, blockIdx.x, smem);
 }
 
 // Compensated current sums: the extra registers allow one 256-thread CTA per SM.
-template <bool PUSH>
+template <bool PUSH, bool PX>
 __global__ void __launch_bounds__(256, 1) k_slot_comp(const __grid_constant__ StepArgs a) {
   extern __shared__ float smem[];
-  slot_tile<PUSH, true, true>(a, blockIdx.x, smem);
+  slot_tile<PUSH, true, true, PX>(a, blockIdx.x, smem);
+}
+
+// the instantiation for (push, move, compensated, periodic in x)
+template <bool PX>
+static void launch_slot(bool push, bool move, bool comp, int grid, int threads, size_t smem, cudaStream_t st,
+                        const StepArgs& a) {
+  if (comp && push)
+    k_slot_comp<true, PX><<<grid, threads, smem, st>>>(a);
+  else if (comp)
+    k_slot_comp<false, PX><<<grid, threads, smem, st>>>(a);
+  else if (push && move)
+    k_slot<true, true, PX><<<grid, threads, smem, st>>>(a);
+  else if (push)
+    k_slot<true, false, PX><<<grid, threads, smem, st>>>(a);
+  else if (move)
+    k_slot<false, true, PX><<<grid, threads, smem, st>>>(a);
 }
 
 // Many simulations: persistent CTAs take (simulation, tile) items from a work
@@ -853,10 +889,13 @@ static SpeciesArgs species_args(Species& sp) {
 }
 
 void slot_set_kernel_attributes() {
-  for (const void* f : {(const void*)k_slot<true, true>, (const void*)k_slot<true, false>,
-                        (const void*)k_slot<false, true>, (const void*)k_slot_batch<true, true>,
-                        (const void*)k_slot_batch<true, false>, (const void*)k_slot_batch<false, true>,
-                        (const void*)k_slot_comp<true>, (const void*)k_slot_comp<false>})
+  for (const void* f : {(const void*)k_slot<true, true, false>, (const void*)k_slot<true, false, false>,
+                        (const void*)k_slot<false, true, false>, (const void*)k_slot<true, true, true>,
+                        (const void*)k_slot<true, false, true>, (const void*)k_slot<false, true, true>,
+                        (const void*)k_slot_batch<true, true>, (const void*)k_slot_batch<true, false>,
+                        (const void*)k_slot_batch<false, true>, (const void*)k_slot_comp<true, false>,
+                        (const void*)k_slot_comp<false, false>, (const void*)k_slot_comp<true, true>,
+                        (const void*)k_slot_comp<false, true>})
     SPX_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
 }
 
@@ -881,16 +920,10 @@ int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysPar
   const int TC = pg.TC();
   const bool comp = pp.compensated && move;
   const size_t smem = slot_smem_floats(pg.TX, pg.TY, push, move, comp) * sizeof(float);
-  if (comp && push)
-    k_slot_comp<true><<<pg.ntiles(), TC, smem, st>>>(a);
-  else if (comp)
-    k_slot_comp<false><<<pg.ntiles(), TC, smem, st>>>(a);
-  else if (push && move)
-    k_slot<true, true><<<pg.ntiles(), TC, smem, st>>>(a);
-  else if (push)
-    k_slot<true, false><<<pg.ntiles(), TC, smem, st>>>(a);
-  else if (move)
-    k_slot<false, true><<<pg.ntiles(), TC, smem, st>>>(a);
+  if (pp.periodic_x)
+    launch_slot<true>(push, move, comp, pg.ntiles(), TC, smem, st, a);
+  else
+    launch_slot<false>(push, move, comp, pg.ntiles(), TC, smem, st, a);
   ++launches;
   for (int s = 0; s < a.ns; ++s) {
     // the overflow fallback reads its count on the device; a small fixed grid covers it
