@@ -383,18 +383,20 @@ __device__ __forceinline__ void periodic_bc(int nx, int ny, int& ix, int& iy) {
 }
 
 // PX: the grid is periodic in x (compile time; the generic form reads a.p).
-template <bool PUSH, bool MOVE, bool COMP = false, bool PX = false>
+// T16: tiles of 16 x 16 cells (compile-time index arithmetic; else from a).
+template <bool PUSH, bool MOVE, bool COMP = false, bool PX = false, bool T16 = false>
 __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, float* smem) {
-  const int TC = a.TX * a.TY;
+  const int TXc = T16 ? 16 : a.TX, TYc = T16 ? 16 : a.TY, logTXc = T16 ? 4 : a.logTX;
+  const int TC = TXc * TYc;
   const int tx = tile % a.NTX, ty = tile / a.NTX;
   const int c = threadIdx.x;
   const int lane = c & 31, warp = c >> 5;
-  const int lx = c & (a.TX - 1), ly = c >> a.logTX;
-  const int ox = tx * a.TX + lx + 1, oy = ty * a.TY + ly + 1;  // owner cell (reference coords)
+  const int lx = c & (TXc - 1), ly = c >> logTXc;
+  const int ox = tx * TXc + lx + 1, oy = ty * TYc + ly + 1;  // owner cell (reference coords)
   const int W = a.g.W, nx = a.g.nx, ny = a.g.ny;
   // deposit window: tile + 2 cells
-  const int WX = a.TX + 4, WY = a.TY + 4, WN = WX * WY;
-  const int wx0 = tx * a.TX + 1 - 2, wy0 = ty * a.TY + 1 - 2;
+  const int WX = TXc + 4, WY = TYc + 4, WN = WX * WY;
+  const int wx0 = tx * TXc + 1 - 2, wy0 = ty * TYc + 1 - 2;
   float* win = smem;
   float* wjx = win;
   float* wjy = win + WN;
@@ -403,7 +405,7 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
   float* wdens = win + 4 * WN;
   constexpr int NWP = MOVE ? (COMP ? 8 : 5) : 0;  // deposit window planes
   // E/B window: tile + 1 cell
-  const int EX = a.TX + 2, EY = a.TY + 2;
+  const int EX = TXc + 2, EY = TYc + 2;
   float4* eb4 = reinterpret_cast<float4*>(smem + NWP * WN);  // 16-byte aligned: WN is a multiple of 4
   float2* eb2 = reinterpret_cast<float2*>(eb4 + EX * EY);
   float* after_eb = smem + NWP * WN + (PUSH ? 6 * EX * EY : 0);
@@ -415,7 +417,7 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
   if (PUSH) {
     for (int i = c; i < EY * EX; i += TC) {
       const int r = i / EX, q = i - r * EX;
-      const size_t g = (size_t)(ty * a.TY + r) * W + (tx * a.TX + q);
+      const size_t g = (size_t)(ty * TYc + r) * W + (tx * TXc + q);
       eb4[i] = make_float4(__ldg(a.f.E[0] + g), __ldg(a.f.E[1] + g), __ldg(a.f.E[2] + g), __ldg(a.f.B[0] + g));
       eb2[i] = make_float2(__ldg(a.f.B[1] + g), __ldg(a.f.B[2] + g));
     }
@@ -698,10 +700,10 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
 }
 
 // One simulation: one CTA per tile.
-template <bool PUSH, bool MOVE, bool PX>
+template <bool PUSH, bool MOVE, bool PX, bool T16>
 __global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS) k_slot(const __grid_constant__ StepArgs a) {
   extern __shared__ float smem[];
-  slot_tile<PUSH, MOVE, false, PX>(a, blockIdx.x, smem);
+  slot_tile<PUSH, MOVE, false, PX, T16>(a, blockIdx.x, smem);
 }
 
 // Compensated current sums: the extra registers allow one 256-thread CTA per SM.
@@ -711,8 +713,8 @@ __global__ void __launch_bounds__(256, 1) k_slot_comp(const __grid_constant__ St
   slot_tile<PUSH, true, true, PX>(a, blockIdx.x, smem);
 }
 
-// the instantiation for (push, move, compensated, periodic in x)
-template <bool PX>
+// the instantiation for (push, move, compensated, periodic in x, 16 x 16 tiles)
+template <bool PX, bool T16>
 static void launch_slot(bool push, bool move, bool comp, int grid, int threads, size_t smem, cudaStream_t st,
                         const StepArgs& a) {
   if (comp && push)
@@ -720,17 +722,17 @@ static void launch_slot(bool push, bool move, bool comp, int grid, int threads, 
   else if (comp)
     k_slot_comp<false, PX><<<grid, threads, smem, st>>>(a);
   else if (push && move)
-    k_slot<true, true, PX><<<grid, threads, smem, st>>>(a);
+    k_slot<true, true, PX, T16><<<grid, threads, smem, st>>>(a);
   else if (push)
-    k_slot<true, false, PX><<<grid, threads, smem, st>>>(a);
+    k_slot<true, false, PX, T16><<<grid, threads, smem, st>>>(a);
   else if (move)
-    k_slot<false, true, PX><<<grid, threads, smem, st>>>(a);
+    k_slot<false, true, PX, T16><<<grid, threads, smem, st>>>(a);
 }
 
 // Many simulations: persistent CTAs take (simulation, tile) items from a work
 // queue (an atomic counter over a list sorted by decreasing work), so uneven
 // grids and particle counts share one launch and balance across the SMs.
-template <bool PUSH, bool MOVE>
+template <bool PUSH, bool MOVE, bool T16>
 __global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS)
     k_slot_batch(const StepArgs* __restrict__ args, const int2* __restrict__ items, int nitems, int* counter) {
   extern __shared__ float smem[];
@@ -742,7 +744,7 @@ __global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS)
     __syncthreads();
     if (it >= nitems) break;
     const int2 item = items[it];
-    slot_tile<PUSH, MOVE>(args[item.x], item.y, smem);
+    slot_tile<PUSH, MOVE, false, false, T16>(args[item.x], item.y, smem);
     __syncthreads();  // the shared windows are reused by the next item
   }
 }
@@ -889,11 +891,16 @@ static SpeciesArgs species_args(Species& sp) {
 }
 
 void slot_set_kernel_attributes() {
-  for (const void* f : {(const void*)k_slot<true, true, false>, (const void*)k_slot<true, false, false>,
-                        (const void*)k_slot<false, true, false>, (const void*)k_slot<true, true, true>,
-                        (const void*)k_slot<true, false, true>, (const void*)k_slot<false, true, true>,
-                        (const void*)k_slot_batch<true, true>, (const void*)k_slot_batch<true, false>,
-                        (const void*)k_slot_batch<false, true>, (const void*)k_slot_comp<true, false>,
+  for (const void* f : {(const void*)k_slot<true, true, false, false>, (const void*)k_slot<true, false, false, false>,
+                        (const void*)k_slot<false, true, false, false>, (const void*)k_slot<true, true, true, false>,
+                        (const void*)k_slot<true, false, true, false>, (const void*)k_slot<false, true, true, false>,
+                        (const void*)k_slot<true, true, false, true>, (const void*)k_slot<true, false, false, true>,
+                        (const void*)k_slot<false, true, false, true>, (const void*)k_slot<true, true, true, true>,
+                        (const void*)k_slot<true, false, true, true>, (const void*)k_slot<false, true, true, true>,
+                        (const void*)k_slot_batch<true, true, false>, (const void*)k_slot_batch<true, false, false>,
+                        (const void*)k_slot_batch<false, true, false>, (const void*)k_slot_batch<true, true, true>,
+                        (const void*)k_slot_batch<true, false, true>, (const void*)k_slot_batch<false, true, true>,
+                        (const void*)k_slot_comp<true, false>,
                         (const void*)k_slot_comp<false, false>, (const void*)k_slot_comp<true, true>,
                         (const void*)k_slot_comp<false, true>})
     SPX_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
@@ -920,10 +927,15 @@ int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysPar
   const int TC = pg.TC();
   const bool comp = pp.compensated && move;
   const size_t smem = slot_smem_floats(pg.TX, pg.TY, push, move, comp) * sizeof(float);
-  if (pp.periodic_x)
-    launch_slot<true>(push, move, comp, pg.ntiles(), TC, smem, st, a);
+  const bool t16 = pg.TX == 16 && pg.TY == 16;
+  if (pp.periodic_x && t16)
+    launch_slot<true, true>(push, move, comp, pg.ntiles(), TC, smem, st, a);
+  else if (pp.periodic_x)
+    launch_slot<true, false>(push, move, comp, pg.ntiles(), TC, smem, st, a);
+  else if (t16)
+    launch_slot<false, true>(push, move, comp, pg.ntiles(), TC, smem, st, a);
   else
-    launch_slot<false>(push, move, comp, pg.ntiles(), TC, smem, st, a);
+    launch_slot<false, false>(push, move, comp, pg.ntiles(), TC, smem, st, a);
   ++launches;
   for (int s = 0; s < a.ns; ++s) {
     // the overflow fallback reads its count on the device; a small fixed grid covers it
@@ -997,7 +1009,8 @@ void slot_batch_build(SlotBatch& b, const std::vector<SlotBatchSim>& sims) {
   }
   const size_t smem = slot_smem_floats(sims[0].pg.TX, sims[0].pg.TY, true, true) * sizeof(float);
   int per_sm = 0;
-  SPX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_slot_batch<true, true>, sims[0].pg.TC(), smem));
+  SPX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_slot_batch<true, true, false>,
+                                                             sims[0].pg.TC(), smem));
   int dev = 0, nsm = 0;
   SPX_CUDA_TRY(cudaGetDevice(&dev));
   SPX_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -1012,12 +1025,19 @@ int slot_batch_step(SlotBatch& b, std::vector<SlotBatchSim>& sims, bool push, bo
   int launches = 0;
   k_batch_reset<<<(b.nsims + 255) / 256, 256, 0, st>>>(args, b.nsims, b.d_counter);
   ++launches;
-  if (push && move)
-    k_slot_batch<true, true><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
+  const bool t16 = sims[0].pg.TX == 16 && sims[0].pg.TY == 16;  // one tile shape for the whole batch
+  if (push && move && t16)
+    k_slot_batch<true, true, true><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
+  else if (push && move)
+    k_slot_batch<true, true, false><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
+  else if (push && t16)
+    k_slot_batch<true, false, true><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
   else if (push)
-    k_slot_batch<true, false><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
+    k_slot_batch<true, false, false><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
+  else if (t16)
+    k_slot_batch<false, true, true><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
   else
-    k_slot_batch<false, true><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
+    k_slot_batch<false, true, false><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
   ++launches;
   const dim3 og(16, b.nsims);
   if (push && move)
