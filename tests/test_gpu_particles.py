@@ -64,9 +64,14 @@ def _assert_moments_close(sim, o, names=("Jx", "Jy", "Jz", "Rho", "Dens"), rtol=
         assert err < rtol, (name, err)
 
 
+TILES = [(0, 0), (16, 16)]  # the library's choice for these small grids, and the 16x16 instantiation
+
+
+@pytest.mark.parametrize("tile", TILES)
 @pytest.mark.parametrize("periodic", [True, False])
-def test_boris_push_bit_exact(periodic):
-    cfg = _cfg(size_x=64, size_y=32, delta=6, c=4.5, dt=0.1, dens=8, periodic_x=periodic, left_wall=not periodic)
+def test_boris_push_bit_exact(periodic, tile):
+    cfg = _cfg(size_x=64, size_y=32, delta=6, c=4.5, dt=0.1, dens=8, periodic_x=periodic, left_wall=not periodic,
+               tile_x=tile[0], tile_y=tile[1])
     p = cfg.params
     specs = [(1.0, 16.0, 0.1, _species(p, 8, 0.1, 1.0050378, 1.0, 1)),
              (-1.0, 1.0, 0.1, _species(p, 8, 0.1, 1.0050378, 1.0, 2))]
@@ -79,9 +84,11 @@ def test_boris_push_bit_exact(periodic):
     sim.close()
 
 
+@pytest.mark.parametrize("tile", TILES)
 @pytest.mark.parametrize("periodic", [True, False])
-def test_move_and_deposit_bit_exact(periodic):
-    cfg = _cfg(size_x=64, size_y=32, delta=6, c=4.5, dt=0.1, dens=8, periodic_x=periodic, left_wall=not periodic)
+def test_move_and_deposit_bit_exact(periodic, tile):
+    cfg = _cfg(size_x=64, size_y=32, delta=6, c=4.5, dt=0.1, dens=8, periodic_x=periodic, left_wall=not periodic,
+               tile_x=tile[0], tile_y=tile[1])
     p = cfg.params
     specs = [(1.0, 16.0, 0.1, _species(p, 8, 0.1, 1.0050378, 1.0, 11)),
              (-1.0, 1.0, 0.3, _species(p, 8, 0.3, 1.2, 1.0, 12))]
@@ -175,11 +182,14 @@ def test_compensated_currents_track_fp64():
     assert errs[True] < 0.5 * errs[False]
 
 
-def test_fused_step_equals_per_phase_sequence():
+@pytest.mark.parametrize("tile", TILES)
+@pytest.mark.parametrize("periodic", [True, False])
+def test_fused_step_equals_per_phase_sequence(periodic, tile):
     """spx_step (push of step t fused with move+deposit of t+1, CUDA graphs) must
     equal the reference's sequence of per-phase calls on the same device."""
     from spectral_rs_b200 import Sim
-    cfg = _cfg(size_x=64, size_y=32, delta=0, c=4.5, dt=0.1, dens=8, periodic_x=True, n_pass=2)
+    cfg = _cfg(size_x=64, size_y=32, delta=0 if periodic else 6, c=3.0, dt=0.1, dens=8, periodic_x=periodic,
+               left_wall=not periodic, n_pass=2, tile_x=tile[0], tile_y=tile[1])
     p = cfg.params
     sp = [(1.0, 16.0, 0.1, _species(p, 8, 0.1, 1.0, 1.0, 31)), (-1.0, 1.0, 0.1, _species(p, 8, 0.1, 1.0, 1.0, 32))]
     fused = Sim(cfg)
