@@ -128,7 +128,7 @@ extern "C" int spx_create(const spx_params* p, spx_ctx** out) {
     tx = std::min(tx, c->g.nx);
     ty = std::min(ty, c->g.ny);
     if (!is_pow2(tx) || !is_pow2(ty) || tx * ty > 256 || tx * ty < 32) {
-      delete c;
+      spx_destroy(c);  // releases the stream and fields allocated above
       return fail(nullptr, SPX_ERR_ARG, "tile_x*tile_y must be a power-of-two product in [32, 256]");
     }
     c->pg.g = c->g;
