@@ -54,3 +54,9 @@ def test_errors_without_device_are_reported_not_crashing():
     code = lib.spx_create(ctypes.byref(prm), ctypes.byref(ctx))
     assert code == 1  # 24 is not a power of two: rejected before touching a device
     assert b"power-of-two" in lib.spx_last_error(None)
+
+
+def test_rust_binding_covers_the_header():
+    # INTEGRATION.md's extern "C" blocks declare every entry point of the header, no other
+    txt = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    assert sorted(set(re.findall(r"pub fn (spx_\w+)", txt))) == declared()
