@@ -164,18 +164,9 @@ __device__ __forceinline__ void move_half(float c1, float px, float py, int& ix,
 // apply_bc (src/prtls.rs:124-190) for one particle.  The reference asserts
 // max(ix) <= wall_loc + 1 and min(ix) > delta over the species before the wall
 // pass; here each particle checks itself and raises the device error word.
-__device__ __forceinline__ void apply_bc(const PhysParams& p, int nx, int ny, int& ix, int& iy, float& dx, float& px,
-                                         int* derr) {
-  if (iy < 1)
-    iy += ny;
-  else if (iy > ny)
-    iy -= ny;
-  if (p.periodic_x) {
-    if (ix < 1)
-      ix += nx;
-    else if (ix > nx)
-      ix -= nx;
-  } else {
+// the x part of apply_bc without the periodic feature: the reflecting wall
+__device__ __forceinline__ void wall_x(const PhysParams& p, int& ix, float& dx, float& px, int* derr) {
+  {
     if (ix > p.wall_loc + 1 || ix < p.delta + (p.left_wall ? 0 : 1)) atomicOr(derr, DERR_WALL);
     if (p.left_wall && ix <= p.delta + 1) {  // optional mirror image of the right wall
       if (ix == p.delta + 1) {
@@ -201,6 +192,22 @@ __device__ __forceinline__ void apply_bc(const PhysParams& p, int nx, int ny, in
       ix -= 1;
       px *= -1.0f;
     }
+  }
+}
+
+__device__ __forceinline__ void apply_bc(const PhysParams& p, int nx, int ny, int& ix, int& iy, float& dx, float& px,
+                                         int* derr) {
+  if (iy < 1)
+    iy += ny;
+  else if (iy > ny)
+    iy -= ny;
+  if (p.periodic_x) {
+    if (ix < 1)
+      ix += nx;
+    else if (ix > nx)
+      ix -= nx;
+  } else {
+    wall_x(p, ix, dx, px, derr);
   }
 }
 
@@ -382,9 +389,26 @@ __device__ __forceinline__ void periodic_bc(int nx, int ny, int& ix, int& iy) {
     ix -= nx;
 }
 
-// PX: the grid is periodic in x (compile time; the generic form reads a.p).
-// T16: tiles of 16 x 16 cells (compile-time index arithmetic; else from a).
-template <bool PUSH, bool MOVE, bool COMP = false, bool PX = false, bool T16 = false>
+// Boundary handling known at compile time: BC_ANY reads a.p, BC_PERIODIC is the
+// reference's `periodic` feature, BC_WALL the reflecting wall.
+enum : int { BC_ANY = 0, BC_PERIODIC = 1, BC_WALL = 2 };
+template <int BC>
+__device__ __forceinline__ void bc_of(const StepArgs& a, int nx, int ny, int& ix, int& iy, float& dx, float& px) {
+  if (BC == BC_PERIODIC) {
+    periodic_bc(nx, ny, ix, iy);
+  } else if (BC == BC_WALL) {
+    if (iy < 1)
+      iy += ny;
+    else if (iy > ny)
+      iy -= ny;
+    wall_x(a.p, ix, dx, px, a.derr);
+  } else {
+    apply_bc(a.p, nx, ny, ix, iy, dx, px, a.derr);
+  }
+}
+
+// BC: see bc_of.  T16: tiles of 16 x 16 cells (compile-time index arithmetic; else from a).
+template <bool PUSH, bool MOVE, bool COMP = false, int BC = BC_ANY, bool T16 = false>
 __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, float* smem) {
   const int TXc = T16 ? 16 : a.TX, TYc = T16 ? 16 : a.TY, logTXc = T16 ? 4 : a.logTX;
   const int TC = TXc * TYc;
@@ -551,10 +575,7 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
           const float c1 = half_dt * inv;
           // first half: position, boundaries, current (src/lib.rs:480-484)
           move_half(c1, px, py, ix, iy, dx, dy);
-          if (PX)
-            periodic_bc(nx, ny, ix, iy);
-          else
-            apply_bc(a.p, nx, ny, ix, iy, dx, px, a.derr);
+          bc_of<BC>(a, nx, ny, ix, iy, dx, px);
           {
             const float2 vxy = mul2(mul2(bc2(q), make_float2(px, py)), bc2(inv));
             vx = vxy.x;
@@ -591,10 +612,7 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
           }
           // second half: position, boundaries, density (src/lib.rs:486-488)
           move_half(c1, px, py, ix, iy, dx, dy);
-          if (PX)
-            periodic_bc(nx, ny, ix, iy);
-          else
-            apply_bc(a.p, nx, ny, ix, iy, dx, px, a.derr);
+          bc_of<BC>(a, nx, ny, ix, iy, dx, px);
           // a particle that stays but finds the low range full joins its own
           // cell's arrivals like a mover
           mover = ix != ox || iy != oy || kept >= KL;
@@ -700,39 +718,39 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
 }
 
 // One simulation: one CTA per tile.
-template <bool PUSH, bool MOVE, bool PX, bool T16>
+template <bool PUSH, bool MOVE, int BC, bool T16>
 __global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS) k_slot(const __grid_constant__ StepArgs a) {
   extern __shared__ float smem[];
-  slot_tile<PUSH, MOVE, false, PX, T16>(a, blockIdx.x, smem);
+  slot_tile<PUSH, MOVE, false, BC, T16>(a, blockIdx.x, smem);
 }
 
 // Compensated current sums: the extra registers allow one 256-thread CTA per SM.
-template <bool PUSH, bool PX>
+template <bool PUSH, int BC>
 __global__ void __launch_bounds__(256, 1) k_slot_comp(const __grid_constant__ StepArgs a) {
   extern __shared__ float smem[];
-  slot_tile<PUSH, true, true, PX>(a, blockIdx.x, smem);
+  slot_tile<PUSH, true, true, BC>(a, blockIdx.x, smem);
 }
 
-// the instantiation for (push, move, compensated, periodic in x, 16 x 16 tiles)
-template <bool PX, bool T16>
+// the instantiation for (push, move, compensated, boundaries, 16 x 16 tiles)
+template <int BC, bool T16>
 static void launch_slot(bool push, bool move, bool comp, int grid, int threads, size_t smem, cudaStream_t st,
                         const StepArgs& a) {
   if (comp && push)
-    k_slot_comp<true, PX><<<grid, threads, smem, st>>>(a);
+    k_slot_comp<true, BC><<<grid, threads, smem, st>>>(a);
   else if (comp)
-    k_slot_comp<false, PX><<<grid, threads, smem, st>>>(a);
+    k_slot_comp<false, BC><<<grid, threads, smem, st>>>(a);
   else if (push && move)
-    k_slot<true, true, PX, T16><<<grid, threads, smem, st>>>(a);
+    k_slot<true, true, BC, T16><<<grid, threads, smem, st>>>(a);
   else if (push)
-    k_slot<true, false, PX, T16><<<grid, threads, smem, st>>>(a);
+    k_slot<true, false, BC, T16><<<grid, threads, smem, st>>>(a);
   else if (move)
-    k_slot<false, true, PX, T16><<<grid, threads, smem, st>>>(a);
+    k_slot<false, true, BC, T16><<<grid, threads, smem, st>>>(a);
 }
 
 // Many simulations: persistent CTAs take (simulation, tile) items from a work
 // queue (an atomic counter over a list sorted by decreasing work), so uneven
 // grids and particle counts share one launch and balance across the SMs.
-template <bool PUSH, bool MOVE, bool T16>
+template <bool PUSH, bool MOVE, int BC, bool T16>
 __global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS)
     k_slot_batch(const StepArgs* __restrict__ args, const int2* __restrict__ items, int nitems, int* counter) {
   extern __shared__ float smem[];
@@ -744,7 +762,7 @@ __global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS)
     __syncthreads();
     if (it >= nitems) break;
     const int2 item = items[it];
-    slot_tile<PUSH, MOVE, false, false, T16>(args[item.x], item.y, smem);
+    slot_tile<PUSH, MOVE, false, BC, T16>(args[item.x], item.y, smem);
     __syncthreads();  // the shared windows are reused by the next item
   }
 }
@@ -890,20 +908,31 @@ static SpeciesArgs species_args(Species& sp) {
   return A;
 }
 
-void slot_set_kernel_attributes() {
-  for (const void* f : {(const void*)k_slot<true, true, false, false>, (const void*)k_slot<true, false, false, false>,
-                        (const void*)k_slot<false, true, false, false>, (const void*)k_slot<true, true, true, false>,
-                        (const void*)k_slot<true, false, true, false>, (const void*)k_slot<false, true, true, false>,
-                        (const void*)k_slot<true, true, false, true>, (const void*)k_slot<true, false, false, true>,
-                        (const void*)k_slot<false, true, false, true>, (const void*)k_slot<true, true, true, true>,
-                        (const void*)k_slot<true, false, true, true>, (const void*)k_slot<false, true, true, true>,
-                        (const void*)k_slot_batch<true, true, false>, (const void*)k_slot_batch<true, false, false>,
-                        (const void*)k_slot_batch<false, true, false>, (const void*)k_slot_batch<true, true, true>,
-                        (const void*)k_slot_batch<true, false, true>, (const void*)k_slot_batch<false, true, true>,
-                        (const void*)k_slot_comp<true, false>,
-                        (const void*)k_slot_comp<false, false>, (const void*)k_slot_comp<true, true>,
-                        (const void*)k_slot_comp<false, true>})
+template <int BC, bool T16>
+static void set_batch_attributes() {
+  for (const void* f : {(const void*)k_slot_batch<true, true, BC, T16>, (const void*)k_slot_batch<true, false, BC, T16>,
+                        (const void*)k_slot_batch<false, true, BC, T16>})
     SPX_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+}
+template <int BC, bool T16>
+static void set_single_attributes() {
+  for (const void* f : {(const void*)k_slot<true, true, BC, T16>, (const void*)k_slot<true, false, BC, T16>,
+                        (const void*)k_slot<false, true, BC, T16>, (const void*)k_slot_comp<true, BC>,
+                        (const void*)k_slot_comp<false, BC>})
+    SPX_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+}
+
+void slot_set_kernel_attributes() {
+  set_single_attributes<BC_PERIODIC, false>();
+  set_single_attributes<BC_PERIODIC, true>();
+  set_single_attributes<BC_WALL, false>();
+  set_single_attributes<BC_WALL, true>();
+  set_batch_attributes<BC_ANY, false>();
+  set_batch_attributes<BC_ANY, true>();
+  set_batch_attributes<BC_PERIODIC, false>();
+  set_batch_attributes<BC_PERIODIC, true>();
+  set_batch_attributes<BC_WALL, false>();
+  set_batch_attributes<BC_WALL, true>();
 }
 
 int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysParams& pp, const FieldPtrs& fp,
@@ -929,13 +958,13 @@ int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysPar
   const size_t smem = slot_smem_floats(pg.TX, pg.TY, push, move, comp) * sizeof(float);
   const bool t16 = pg.TX == 16 && pg.TY == 16;
   if (pp.periodic_x && t16)
-    launch_slot<true, true>(push, move, comp, pg.ntiles(), TC, smem, st, a);
+    launch_slot<BC_PERIODIC, true>(push, move, comp, pg.ntiles(), TC, smem, st, a);
   else if (pp.periodic_x)
-    launch_slot<true, false>(push, move, comp, pg.ntiles(), TC, smem, st, a);
+    launch_slot<BC_PERIODIC, false>(push, move, comp, pg.ntiles(), TC, smem, st, a);
   else if (t16)
-    launch_slot<false, true>(push, move, comp, pg.ntiles(), TC, smem, st, a);
+    launch_slot<BC_WALL, true>(push, move, comp, pg.ntiles(), TC, smem, st, a);
   else
-    launch_slot<false, false>(push, move, comp, pg.ntiles(), TC, smem, st, a);
+    launch_slot<BC_WALL, false>(push, move, comp, pg.ntiles(), TC, smem, st, a);
   ++launches;
   for (int s = 0; s < a.ns; ++s) {
     // the overflow fallback reads its count on the device; a small fixed grid covers it
@@ -1009,12 +1038,23 @@ void slot_batch_build(SlotBatch& b, const std::vector<SlotBatchSim>& sims) {
   }
   const size_t smem = slot_smem_floats(sims[0].pg.TX, sims[0].pg.TY, true, true) * sizeof(float);
   int per_sm = 0;
-  SPX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_slot_batch<true, true, false>,
+  SPX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_slot_batch<true, true, BC_ANY, false>,
                                                              sims[0].pg.TC(), smem));
   int dev = 0, nsm = 0;
   SPX_CUDA_TRY(cudaGetDevice(&dev));
   SPX_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   b.grid = std::max(1, std::min(b.nitems, std::max(per_sm, 1) * nsm));
+}
+
+template <int BC, bool T16>
+static void launch_batch(bool push, bool move, const SlotBatch& b, int TC, size_t smem, cudaStream_t st,
+                         const StepArgs* args) {
+  if (push && move)
+    k_slot_batch<true, true, BC, T16><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
+  else if (push)
+    k_slot_batch<true, false, BC, T16><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
+  else
+    k_slot_batch<false, true, BC, T16><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
 }
 
 int slot_batch_step(SlotBatch& b, std::vector<SlotBatchSim>& sims, bool push, bool move, cudaStream_t st) {
@@ -1026,18 +1066,21 @@ int slot_batch_step(SlotBatch& b, std::vector<SlotBatchSim>& sims, bool push, bo
   k_batch_reset<<<(b.nsims + 255) / 256, 256, 0, st>>>(args, b.nsims, b.d_counter);
   ++launches;
   const bool t16 = sims[0].pg.TX == 16 && sims[0].pg.TY == 16;  // one tile shape for the whole batch
-  if (push && move && t16)
-    k_slot_batch<true, true, true><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
-  else if (push && move)
-    k_slot_batch<true, true, false><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
-  else if (push && t16)
-    k_slot_batch<true, false, true><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
-  else if (push)
-    k_slot_batch<true, false, false><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
-  else if (t16)
-    k_slot_batch<false, true, true><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
+  bool all_periodic = true, all_wall = true;
+  for (auto& m : sims) {
+    all_periodic = all_periodic && m.pp.periodic_x;
+    all_wall = all_wall && !m.pp.periodic_x;
+  }
+  const int bc = all_periodic ? BC_PERIODIC : all_wall ? BC_WALL : BC_ANY;
+  if (bc == BC_PERIODIC)
+    t16 ? launch_batch<BC_PERIODIC, true>(push, move, b, TC, smem, st, args)
+        : launch_batch<BC_PERIODIC, false>(push, move, b, TC, smem, st, args);
+  else if (bc == BC_WALL)
+    t16 ? launch_batch<BC_WALL, true>(push, move, b, TC, smem, st, args)
+        : launch_batch<BC_WALL, false>(push, move, b, TC, smem, st, args);
   else
-    k_slot_batch<false, true, false><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
+    t16 ? launch_batch<BC_ANY, true>(push, move, b, TC, smem, st, args)
+        : launch_batch<BC_ANY, false>(push, move, b, TC, smem, st, args);
   ++launches;
   const dim3 og(16, b.nsims);
   if (push && move)
