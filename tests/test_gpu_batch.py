@@ -22,11 +22,18 @@ def _arrays(p, ppc, vth, gamma, seed):
     return dict(ix=ix, iy=iy, dx=dx, dy=dy, px=px, py=py, pz=pz, psa=psa)
 
 
-def test_batch_matches_single_simulations():
+def _member(kind, size_x, size_y, dens, n_pass):
+    if kind == "periodic":
+        return _cfg(size_x=size_x, size_y=size_y, delta=0, c=3.0, dt=0.1, dens=dens, periodic_x=True, n_pass=n_pass)
+    return _cfg(size_x=size_x, size_y=size_y, delta=6, c=3.0, dt=0.1, dens=dens, periodic_x=False, left_wall=True,
+                n_pass=n_pass)
+
+
+# mixed boundaries run the batch kernel's generic form, uniform ones its periodic / wall forms
+@pytest.mark.parametrize("kinds", [("periodic", "wall", "periodic"), ("periodic",) * 3, ("wall",) * 3])
+def test_batch_matches_single_simulations(kinds):
     from spectral_rs_b200 import Sim, Batch
-    cfgs = [_cfg(size_x=64, size_y=32, delta=0, c=4.5, dt=0.1, dens=8, periodic_x=True, n_pass=4),
-            _cfg(size_x=128, size_y=64, delta=6, c=4.5, dt=0.1, dens=4, periodic_x=False, left_wall=True, n_pass=2),
-            _cfg(size_x=32, size_y=32, delta=0, c=4.5, dt=0.1, dens=16, periodic_x=True, n_pass=4)]
+    cfgs = [_member(kinds[0], 64, 32, 8, 4), _member(kinds[1], 128, 64, 4, 2), _member(kinds[2], 32, 32, 16, 4)]
     species = []
     for k, cfg in enumerate(cfgs):
         p = cfg.params
