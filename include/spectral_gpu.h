@@ -104,6 +104,9 @@ SPX_API const char* spx_version(void);
  * the Prtl fields (src/prtls.rs:8-16).  `usize` cell indices cross as uint64.
  * psa (Lorentz factors) must equal sqrt(1 + |p|^2 / c^2) as the reference keeps
  * them (src/prtls.rs:237-249,440); the GPU recomputes it and does not store it.
+ * The arrays are host memory, pageable or page-locked (page-locked arrays are
+ * copied at the full host-link rate, in chunks of 2^22 particles); the call
+ * returns once they are no longer read.
  * The species id (0, 1, ...) is written to *species_out. */
 SPX_API int spx_add_species(spx_ctx* ctx, float charge, float mass, float vth, uint64_t n, const uint64_t* ix,
                     const uint64_t* iy, const float* dx, const float* dy, const float* px, const float* py,

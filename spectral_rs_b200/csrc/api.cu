@@ -154,6 +154,9 @@ extern "C" int spx_create(const spx_params* p, spx_ctx** out) {
     SPX_CUDA_TRY(cudaMalloc(&c->d_counts, c->pg.ncells() * sizeof(uint32_t)));
     slot_set_kernel_attributes();
     fields_set_kernel_attributes();
+    // the zero fills above ran on the legacy stream, which the context's
+    // non-blocking stream does not wait for
+    SPX_CUDA_TRY(cudaDeviceSynchronize());
   } catch (const spx::Error& e) {
     spx_destroy(c);
     return fail(nullptr, e.code, e.msg);
@@ -224,15 +227,8 @@ struct Capacity {
   int KL, H;
 };
 
-static Capacity choose_capacity(spx_ctx* c, uint64_t n) {
-  uint32_t mx = 0;
-  SPX_CUDA_TRY(cudaMemsetAsync(c->d_u32, 0, sizeof(uint32_t), c->st));
-  // max over the counts array
-  Species tmp;
-  tmp.slot.nlow = c->d_counts;
-  slot_max_occupancy(tmp, c->pg, c->d_u32, c->st);
-  SPX_CUDA_TRY(cudaMemcpyAsync(&mx, c->d_u32, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
-  SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+// Capacity for n particles whose fullest cell holds mx.
+static Capacity capacity_for(const spx_ctx* c, uint64_t n, uint32_t mx) {
   // exact low range and one arrival slot (tests: every step overflows)
   if (c->prm.slot_capacity < 0) return {std::max((int)mx, -c->prm.slot_capacity), 1};
   const double mean = (double)n / (double)c->pg.ncells();
@@ -248,6 +244,20 @@ static Capacity choose_capacity(spx_ctx* c, uint64_t n) {
   const int H = std::max(16, (KL + 3) / 4);
   return {KL, H};
 }
+
+// Largest per-cell count of c->d_counts.
+static uint32_t max_count(spx_ctx* c) {
+  uint32_t mx = 0;
+  SPX_CUDA_TRY(cudaMemsetAsync(c->d_u32, 0, sizeof(uint32_t), c->st));
+  Species tmp;
+  tmp.slot.nlow = c->d_counts;
+  slot_max_occupancy(tmp, c->pg, c->d_u32, c->st);
+  SPX_CUDA_TRY(cudaMemcpyAsync(&mx, c->d_u32, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
+  SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+  return mx;
+}
+
+static Capacity choose_capacity(spx_ctx* c, uint64_t n) { return capacity_for(c, n, max_count(c)); }
 
 static int finish_species(spx_ctx* c, Species& s, Staging& st, uint64_t n, const uint32_t* d_tag) {
   if (c->plain) {
@@ -286,19 +296,70 @@ __global__ void k_check_gamma(uint64_t n, const float* px, const float* py, cons
 }
 
 // Cell indices (1-based, usize in the reference) -> packed cell; the smallest
-// index of a particle outside the grid goes to *bad (initialised to ~0).
-__global__ void k_pack_check(uint64_t n, const uint64_t* ix, const uint64_t* iy, int nx, int ny, uint32_t* cell,
-                             uint32_t* bad) {
+// index (off + i) of a particle outside the grid goes to *bad (initialised to ~0).
+__global__ void k_pack_check(uint64_t n, uint64_t off, const uint64_t* ix, const uint64_t* iy, int nx, int ny,
+                             uint32_t* cell, uint32_t* bad) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t x = ix[i], y = iy[i];
     if (x < 1 || y < 1 || x > (uint64_t)nx || y > (uint64_t)ny) {
-      atomicMin(bad, (uint32_t)i);
+      atomicMin(bad, (uint32_t)(off + i));
       cell[i] = 1u | (1u << 16);
     } else {
       cell[i] = (uint32_t)x | ((uint32_t)y << 16);
     }
   }
 }
+
+// Upload of the caller's arrays: chunks of UPLOAD_CHUNK particles cross PCIe
+// through two device buffers on a copy stream while the context's stream
+// packs the previous chunk, so the copies run back to back at the link's rate.
+// Staging a whole species on the device instead (multi-GB allocations made and
+// released per species) cost more than the copies themselves.
+constexpr uint64_t UPLOAD_CHUNK = 1ull << 22;  // particles per chunk
+constexpr size_t UPLOAD_BYTES = 24;            // per particle and buffer: dx..pz + psa (>= ix + iy)
+struct UploadRing {
+  cudaStream_t cs = nullptr;
+  cudaEvent_t ready[2] = {nullptr, nullptr}, done[2] = {nullptr, nullptr};
+  unsigned char* buf[2] = {nullptr, nullptr};
+  explicit UploadRing(uint64_t n) {
+    const size_t bytes = UPLOAD_BYTES * std::max<uint64_t>(1, std::min(n, UPLOAD_CHUNK));
+    SPX_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; ++b) {
+      SPX_CUDA_TRY(cudaEventCreateWithFlags(&ready[b], cudaEventDisableTiming));
+      SPX_CUDA_TRY(cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming));
+      SPX_CUDA_TRY(cudaMalloc(&buf[b], bytes));
+    }
+  }
+  ~UploadRing() {
+    if (cs) cudaStreamSynchronize(cs);
+    for (int b = 0; b < 2; ++b) {
+      if (buf[b]) cudaFree(buf[b]);
+      if (ready[b]) cudaEventDestroy(ready[b]);
+      if (done[b]) cudaEventDestroy(done[b]);
+    }
+    if (cs) cudaStreamDestroy(cs);
+  }
+  // copy(off, m, buf, stream) queues the host-to-device copies of particles
+  // [off, off + m); use(off, m, buf) queues the kernels that consume them on st.
+  template <class Copy, class Use>
+  void run(uint64_t n, cudaStream_t st, Copy copy, Use use) {
+    // the first copies wait for everything already queued on st (a previous
+    // pass may still read the buffers)
+    SPX_CUDA_TRY(cudaEventRecord(done[0], st));
+    SPX_CUDA_TRY(cudaStreamWaitEvent(cs, done[0], 0));
+    uint64_t k = 0;
+    for (uint64_t off = 0; off < n; off += UPLOAD_CHUNK, ++k) {
+      const int b = (int)(k & 1);
+      const uint64_t m = std::min(UPLOAD_CHUNK, n - off);
+      if (k >= 2) SPX_CUDA_TRY(cudaStreamWaitEvent(cs, done[b], 0));
+      copy(off, m, buf[b], cs);
+      SPX_CUDA_TRY(cudaEventRecord(ready[b], cs));
+      SPX_CUDA_TRY(cudaStreamWaitEvent(st, ready[b], 0));
+      use(off, m, buf[b]);
+      SPX_CUDA_TRY(cudaEventRecord(done[b], st));
+    }
+  }
+};
 
 extern "C" int spx_add_species(spx_ctx* c, float charge, float mass, float vth, uint64_t n, const uint64_t* ix,
                                const uint64_t* iy, const float* dx, const float* dy, const float* px, const float* py,
@@ -318,42 +379,92 @@ extern "C" int spx_add_species(spx_ctx* c, float charge, float mass, float vth, 
     s.beta = (charge / mass) * 0.5f * c->prm.dt;
     s.alpha = (charge / mass) * 0.5f * c->prm.dt / c->prm.c;
     s.n = n;
-    Staging st;
-    st.alloc(n);
-    if (n) {  // cell indices checked and packed on the device (ix | iy << 16)
-      uint64_t* d_ixy = nullptr;
-      SPX_CUDA_TRY(cudaMallocAsync(&d_ixy, 2 * n * sizeof(uint64_t), c->st));
-      SPX_CUDA_TRY(cudaMemcpyAsync(d_ixy, ix, n * 8, cudaMemcpyHostToDevice, c->st));
-      SPX_CUDA_TRY(cudaMemcpyAsync(d_ixy + n, iy, n * 8, cudaMemcpyHostToDevice, c->st));
-      SPX_CUDA_TRY(cudaMemsetAsync(c->d_u32, 0xFF, sizeof(uint32_t), c->st));
-      k_pack_check<<<148 * 8, 256, 0, c->st>>>(n, d_ixy, d_ixy + n, c->g.nx, c->g.ny, st.cell, c->d_u32);
-      SPX_CUDA_TRY(cudaFreeAsync(d_ixy, c->st));
-      uint32_t bad = 0;
-      SPX_CUDA_TRY(cudaMemcpyAsync(&bad, c->d_u32, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
-      SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
-      if (bad != 0xFFFFFFFFu)
-        return fail(c, SPX_ERR_BOUNDS, "particle " + std::to_string(bad) + " outside the grid");
-    }
-    SPX_CUDA_TRY(cudaMemcpyAsync(st.dx, dx, n * 4, cudaMemcpyHostToDevice, c->st));
-    SPX_CUDA_TRY(cudaMemcpyAsync(st.dy, dy, n * 4, cudaMemcpyHostToDevice, c->st));
-    SPX_CUDA_TRY(cudaMemcpyAsync(st.px, px, n * 4, cudaMemcpyHostToDevice, c->st));
-    SPX_CUDA_TRY(cudaMemcpyAsync(st.py, py, n * 4, cudaMemcpyHostToDevice, c->st));
-    SPX_CUDA_TRY(cudaMemcpyAsync(st.pz, pz, n * 4, cudaMemcpyHostToDevice, c->st));
-    if (psa && n) {
-      float* d_psa = nullptr;
-      SPX_CUDA_TRY(cudaMallocAsync(&d_psa, n * 4, c->st));
-      SPX_CUDA_TRY(cudaMemcpyAsync(d_psa, psa, n * 4, cudaMemcpyHostToDevice, c->st));
-      k_check_gamma<<<148 * 8, 256, 0, c->st>>>(n, st.px, st.py, st.pz, d_psa, c->pp.csqinv, c->d_err);
-      SPX_CUDA_TRY(cudaFreeAsync(d_psa, c->st));
-      int h = 0;
-      SPX_CUDA_TRY(cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
-      SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
-      if (h & DERR_GAMMA) {
-        SPX_CUDA_TRY(cudaMemset(c->d_err, 0, sizeof(int)));
-        return fail(c, SPX_ERR_GAMMA, "psa differs from sqrt(1 + |p|^2/c^2); the GPU derives gamma from p");
+    UploadRing up(n);
+    uint32_t* cell = nullptr;  // packed cells of the whole species (ix | iy << 16)
+    SPX_CUDA_TRY(cudaMalloc(&cell, std::max<uint64_t>(n, 1) * 4));
+    struct Release {
+      uint32_t* p;
+      ~Release() { cudaFree(p); }
+    } cell_release{cell};
+    // pass 1: cell indices checked and packed on the device, occupancy per cell
+    SPX_CUDA_TRY(cudaMemsetAsync(c->d_u32, 0xFF, sizeof(uint32_t), c->st));
+    if (!c->plain) SPX_CUDA_TRY(cudaMemsetAsync(c->d_counts, 0, c->pg.ncells() * sizeof(uint32_t), c->st));
+    up.run(
+        n, c->st,
+        [&](uint64_t off, uint64_t m, unsigned char* b, cudaStream_t cs) {
+          SPX_CUDA_TRY(cudaMemcpyAsync(b, ix + off, m * 8, cudaMemcpyHostToDevice, cs));
+          SPX_CUDA_TRY(cudaMemcpyAsync(b + m * 8, iy + off, m * 8, cudaMemcpyHostToDevice, cs));
+        },
+        [&](uint64_t off, uint64_t m, unsigned char* b) {
+          const uint64_t* bx = reinterpret_cast<const uint64_t*>(b);
+          k_pack_check<<<148 * 4, 256, 0, c->st>>>(m, off, bx, bx + m, c->g.nx, c->g.ny, cell + off, c->d_u32);
+          if (!c->plain) slot_count(c->pg, m, cell + off, c->d_counts, c->st, false);
+        });
+    // the destination arrays are allocated while pass 1's copies run: the plain
+    // arrays, or (periodic grids) the slots for the occupancy of a uniform
+    // species, replaced below if the counts ask for more
+    auto release = [&]() {
+      slot_release(s);
+      for (float** p : {&s.plain.x, &s.plain.y, &s.plain.px, &s.plain.py, &s.plain.pz}) {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
       }
+    };
+    Capacity guess{0, 0};
+    if (c->plain) {
+      for (float** p : {&s.plain.x, &s.plain.y, &s.plain.px, &s.plain.py, &s.plain.pz})
+        SPX_CUDA_TRY(cudaMalloc(p, std::max<uint64_t>(n, 1) * 4));
+    } else if (c->prm.periodic_x) {
+      guess = capacity_for(c, n, (uint32_t)((n + c->pg.ncells() - 1) / c->pg.ncells()));
+      slot_allocate(s, c->pg, guess.KL, guess.H, n);
     }
-    finish_species(c, s, st, n, nullptr);
+    uint32_t bad = 0;
+    SPX_CUDA_TRY(cudaMemcpyAsync(&bad, c->d_u32, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
+    SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+    if (bad != 0xFFFFFFFFu) {
+      release();
+      return fail(c, SPX_ERR_BOUNDS, "particle " + std::to_string(bad) + " outside the grid");
+    }
+    // pass 2: offsets and momenta into their slots (or the plain arrays)
+    if (!c->plain) {
+      const Capacity cap = choose_capacity(c, n);
+      if (cap.KL != guess.KL || cap.H != guess.H) {
+        slot_release(s);
+        slot_allocate(s, c->pg, cap.KL, cap.H, n);
+      }
+      slot_scatter_begin(s, c->pg, c->d_counts, c->st);
+    }
+    up.run(
+        n, c->st,
+        [&](uint64_t off, uint64_t m, unsigned char* b, cudaStream_t cs) {
+          const float* src[6] = {dx, dy, px, py, pz, psa};
+          for (int f = 0; f < (psa ? 6 : 5); ++f)
+            SPX_CUDA_TRY(cudaMemcpyAsync(b + f * m * 4, src[f] + off, m * 4, cudaMemcpyHostToDevice, cs));
+        },
+        [&](uint64_t off, uint64_t m, unsigned char* b) {
+          const float* f = reinterpret_cast<const float*>(b);
+          if (psa) k_check_gamma<<<148 * 4, 256, 0, c->st>>>(m, f + 2 * m, f + 3 * m, f + 4 * m, f + 5 * m,
+                                                             c->pp.csqinv, c->d_err);
+          if (c->plain) {
+            k_plain_from_cells<<<148 * 4, 256, 0, c->st>>>(m, cell + off, f, f + m, s.plain.x + off, s.plain.y + off);
+            float* const mom[3] = {s.plain.px, s.plain.py, s.plain.pz};
+            for (int k = 0; k < 3; ++k)
+              SPX_CUDA_TRY(cudaMemcpyAsync(mom[k] + off, f + (2 + k) * m, m * 4, cudaMemcpyDeviceToDevice, c->st));
+          } else {
+            slot_scatter_chunk(s, c->pg, m, (uint32_t)off, cell + off, f, f + m, f + 2 * m, f + 3 * m, f + 4 * m,
+                               nullptr, c->d_counts, c->st);
+          }
+        });
+    if (!c->plain) slot_scatter_end(s, c->pg, c->d_counts, c->st);
+    SPX_CUDA_TRY(cudaGetLastError());
+    int h = 0;
+    SPX_CUDA_TRY(cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+    if (h & DERR_GAMMA) {
+      SPX_CUDA_TRY(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st));
+      release();
+      return fail(c, SPX_ERR_GAMMA, "psa differs from sqrt(1 + |p|^2/c^2); the GPU derives gamma from p");
+    }
     c->species.push_back(s);
     if (species_out) *species_out = (int32_t)c->species.size() - 1;
     invalidate_graphs(c);

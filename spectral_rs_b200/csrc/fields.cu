@@ -265,8 +265,13 @@ __device__ __forceinline__ void store_ghosted(float* dst, const Grid& g, int row
   }
 }
 
-template <int IN, int OUT, bool INV>
-__global__ void __launch_bounds__(1024) k_rows(const __grid_constant__ RowArgs a, Grid g, const float2* __restrict__ tw) {
+// Launch bounds of the transforms: a launch of at most 512 threads (every
+// transform of <= 4096 points) runs the SMALL instantiation, bounded to three
+// such CTAs per SM (40 registers); 8192-point transforms need 1024 threads.
+#define FFT_BOUNDS(SMALL) __launch_bounds__((SMALL) ? 512 : 1024, (SMALL) ? 3 : 1)
+
+template <int IN, int OUT, bool INV, bool SMALL>
+__global__ void FFT_BOUNDS(SMALL) k_rows(const __grid_constant__ RowArgs a, Grid g, const float2* __restrict__ tw) {
   extern __shared__ float2 sm[];
   const int f = blockIdx.y;
   const int logN = g.log2nx, N = g.nx;
@@ -326,8 +331,8 @@ __global__ void __launch_bounds__(1024) k_rows(const __grid_constant__ RowArgs a
 struct ColArgs {
   float2* data[8];
 };
-template <bool INV>
-__global__ void __launch_bounds__(1024) k_cols(const __grid_constant__ ColArgs a, Grid g, const float2* __restrict__ tw) {
+template <bool INV, bool SMALL>
+__global__ void FFT_BOUNDS(SMALL) k_cols(const __grid_constant__ ColArgs a, Grid g, const float2* __restrict__ tw) {
   extern __shared__ float2 sm[];
   const int f = blockIdx.y;
   const int logN = g.log2ny, N = g.ny;
@@ -663,11 +668,18 @@ void launch_filter_pass(const Grid& g, float* const* src, float* const* dst, int
 // Dynamic shared memory above 48 KB must be opted into once per kernel (on
 // every device that runs it; done when a context is created, never while a
 // stream is being captured).
-void fields_set_kernel_attributes() {
-  for (const void* f : {(const void*)k_rows<0, 0, false>, (const void*)k_rows<1, 0, false>,
-                        (const void*)k_rows<1, 0, true>, (const void*)k_rows<1, 1, true>, (const void*)k_cols<false>,
-                        (const void*)k_cols<true>, (const void*)k_filter_fused})
+template <bool SMALL>
+static void fft_set_kernel_attributes() {
+  for (const void* f : {(const void*)k_rows<0, 0, false, SMALL>, (const void*)k_rows<1, 0, false, SMALL>,
+                        (const void*)k_rows<1, 0, true, SMALL>, (const void*)k_rows<1, 1, true, SMALL>,
+                        (const void*)k_cols<false, SMALL>, (const void*)k_cols<true, SMALL>})
     SPX_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+}
+void fields_set_kernel_attributes() {
+  fft_set_kernel_attributes<false>();
+  fft_set_kernel_attributes<true>();
+  SPX_CUDA_TRY(cudaFuncSetAttribute((const void*)k_filter_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    96 * 1024));
 }
 
 template <int IN, int OUT, bool INV>
@@ -676,7 +688,10 @@ static void launch_rows(const Grid& g, const RowArgs& a, int nf, const float2* t
   const int threads = std::max(1, (g.nx << logB) / 8);
   const size_t smem = sizeof(float2) * fft_smem_elems(g.log2nx, logB);
   const int blocks = (g.ny + (1 << logB) - 1) >> logB;
-  k_rows<IN, OUT, INV><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
+  if (threads <= 512)
+    k_rows<IN, OUT, INV, true><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
+  else
+    k_rows<IN, OUT, INV, false><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
 }
 
 template <bool INV>
@@ -685,7 +700,10 @@ static void launch_cols(const Grid& g, const ColArgs& a, int nf, const float2* t
   const int threads = std::max(1, (g.ny << logW) / 8);
   const size_t smem = sizeof(float2) * fft_smem_elems(g.log2ny, logW);
   const int blocks = g.nx >> logW;
-  k_cols<INV><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
+  if (threads <= 512)
+    k_cols<INV, true><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
+  else
+    k_cols<INV, false><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
 }
 
 void FieldBuffers::allocate(const Grid& grid) {

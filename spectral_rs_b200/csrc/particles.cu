@@ -1111,8 +1111,9 @@ __global__ void k_count(uint64_t n, const uint32_t* cell, uint32_t* counts, int 
     atomicAdd(&counts[cell_gc(cell[i], TX, TY, logTX, logTY, NTX)], 1u);
 }
 
-__global__ void k_scatter(uint64_t n, const uint32_t* cell, const float* dx, const float* dy, const float* px,
-                          const float* py, const float* pz, const uint32_t* tag, uint32_t* cursor, float* odx,
+__global__ void k_scatter(uint64_t n, uint32_t tag0, const uint32_t* cell, const float* dx, const float* dy,
+                          const float* px, const float* py, const float* pz, const uint32_t* tag, uint32_t* cursor,
+                          float* odx,
                           float* ody, float* opx, float* opy, float* opz, uint32_t* otag, int K, int TX, int TY,
                           int logTX, int logTY, int NTX) {
   const int TC = TX * TY;
@@ -1127,29 +1128,46 @@ __global__ void k_scatter(uint64_t n, const uint32_t* cell, const float* dx, con
     opx[o] = px[i];
     opy[o] = py[i];
     opz[o] = pz[i];
-    otag[o] = tag ? tag[i] : (uint32_t)i;
+    otag[o] = tag ? tag[i] : tag0 + (uint32_t)i;
   }
 }
 
-void slot_count(const ParticleGeom& pg, uint64_t n, const uint32_t* cell, uint32_t* counts, cudaStream_t st) {
-  SPX_CUDA_TRY(cudaMemsetAsync(counts, 0, pg.ncells() * sizeof(uint32_t), st));
+void slot_count(const ParticleGeom& pg, uint64_t n, const uint32_t* cell, uint32_t* counts, cudaStream_t st,
+                bool reset) {
+  if (reset) SPX_CUDA_TRY(cudaMemsetAsync(counts, 0, pg.ncells() * sizeof(uint32_t), st));
   if (n) k_count<<<148 * 8, 256, 0, st>>>(n, cell, counts, pg.TX, pg.TY, pg.logTX, pg.logTY, pg.NTX);
+  SPX_CUDA_TRY(cudaGetLastError());
+}
+
+void slot_scatter_begin(Species& s, const ParticleGeom& pg, uint32_t* cursor, cudaStream_t st) {
+  s.slot.ocur = 0;
+  SPX_CUDA_TRY(cudaMemsetAsync(cursor, 0, pg.ncells() * sizeof(uint32_t), st));
+}
+
+void slot_scatter_chunk(Species& s, const ParticleGeom& pg, uint64_t n, uint32_t tag0, const uint32_t* cell,
+                        const float* dx, const float* dy, const float* px, const float* py, const float* pz,
+                        const uint32_t* tag, uint32_t* cursor, cudaStream_t st) {
+  SlotSpecies& S = s.slot;
+  if (n)
+    k_scatter<<<148 * 8, 256, 0, st>>>(n, tag0, cell, dx, dy, px, py, pz, tag, cursor, S.dx, S.dy, S.px, S.py, S.pz,
+                                       S.tag, S.K, pg.TX, pg.TY, pg.logTX, pg.logTY, pg.NTX);
+  SPX_CUDA_TRY(cudaGetLastError());
+}
+
+void slot_scatter_end(Species& s, const ParticleGeom& pg, uint32_t* cursor, cudaStream_t st) {
+  SlotSpecies& S = s.slot;
+  SPX_CUDA_TRY(cudaMemcpyAsync(S.nlow, cursor, pg.ncells() * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+  SPX_CUDA_TRY(cudaMemsetAsync(S.narr, 0, 2 * pg.ncells() * sizeof(uint32_t), st));
+  SPX_CUDA_TRY(cudaMemsetAsync(S.ocount, 0, 2 * sizeof(uint32_t), st));
   SPX_CUDA_TRY(cudaGetLastError());
 }
 
 void slot_scatter(Species& s, const ParticleGeom& pg, uint64_t n, const uint32_t* cell, const float* dx,
                   const float* dy, const float* px, const float* py, const float* pz, const uint32_t* tag,
                   uint32_t* cursor, cudaStream_t st) {
-  SlotSpecies& S = s.slot;
-  S.ocur = 0;
-  SPX_CUDA_TRY(cudaMemsetAsync(cursor, 0, pg.ncells() * sizeof(uint32_t), st));
-  if (n)
-    k_scatter<<<148 * 8, 256, 0, st>>>(n, cell, dx, dy, px, py, pz, tag, cursor, S.dx, S.dy, S.px, S.py, S.pz, S.tag,
-                                       S.K, pg.TX, pg.TY, pg.logTX, pg.logTY, pg.NTX);
-  SPX_CUDA_TRY(cudaMemcpyAsync(S.nlow, cursor, pg.ncells() * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
-  SPX_CUDA_TRY(cudaMemsetAsync(S.narr, 0, 2 * pg.ncells() * sizeof(uint32_t), st));
-  SPX_CUDA_TRY(cudaMemsetAsync(S.ocount, 0, 2 * sizeof(uint32_t), st));
-  SPX_CUDA_TRY(cudaGetLastError());
+  slot_scatter_begin(s, pg, cursor, st);
+  slot_scatter_chunk(s, pg, n, 0u, cell, dx, dy, px, py, pz, tag, cursor, st);
+  slot_scatter_end(s, pg, cursor, st);
 }
 
 __global__ void k_unpack(SpeciesArgs S, int TX, int TY, int logTX, int NTX, size_t ncells, uint32_t* ix,
@@ -1234,10 +1252,9 @@ void slot_allocate(Species& s, const ParticleGeom& pg, int KL, int H, uint64_t n
   SPX_CUDA_TRY(cudaMalloc(&S.py, cap * sizeof(float)));
   SPX_CUDA_TRY(cudaMalloc(&S.pz, cap * sizeof(float)));
   SPX_CUDA_TRY(cudaMalloc(&S.tag, cap * sizeof(uint32_t)));
+  // nlow, narr and ocount are set by slot_scatter_end, on the stream of the scatter
   SPX_CUDA_TRY(cudaMalloc(&S.nlow, pg.ncells() * sizeof(uint32_t)));
-  SPX_CUDA_TRY(cudaMemset(S.nlow, 0, pg.ncells() * sizeof(uint32_t)));
   SPX_CUDA_TRY(cudaMalloc(&S.narr, 2 * pg.ncells() * sizeof(uint32_t)));
-  SPX_CUDA_TRY(cudaMemset(S.narr, 0, 2 * pg.ncells() * sizeof(uint32_t)));
   S.ocap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(1u << 16, n / 32), 1u << 28);
   for (int b = 0; b < 2; ++b) {
     SPX_CUDA_TRY(cudaMalloc(&S.ocell[b], S.ocap * sizeof(uint32_t)));
@@ -1249,7 +1266,6 @@ void slot_allocate(Species& s, const ParticleGeom& pg, int KL, int H, uint64_t n
     SPX_CUDA_TRY(cudaMalloc(&S.otag[b], S.ocap * sizeof(uint32_t)));
   }
   SPX_CUDA_TRY(cudaMalloc(&S.ocount, 2 * sizeof(uint32_t)));
-  SPX_CUDA_TRY(cudaMemset(S.ocount, 0, 2 * sizeof(uint32_t)));
 }
 
 void slot_release(Species& s) {

@@ -93,14 +93,25 @@ enum : int { DERR_BOUNDS = 1, DERR_WALL = 2, DERR_OVERFLOW_LOST = 4, DERR_GAMMA 
 
 // --- split path ---------------------------------------------------------------
 // Storage for n particles with a low range of KL slots and arrival regions of
-// H slots per cell.
+// H slots per cell (its counters are set by slot_scatter_end).
 void slot_allocate(Species& s, const ParticleGeom& pg, int KL, int H, uint64_t n);
 void slot_release(Species& s);
-// Count particles per cell (for choosing K).  counts: ncells uint32 (zeroed inside).
-void slot_count(const ParticleGeom& pg, uint64_t n, const uint32_t* cell, uint32_t* counts, cudaStream_t st);
+// Count particles per cell (for choosing K).  counts: ncells uint32, zeroed
+// first unless reset is false (a later chunk of the same species).
+void slot_count(const ParticleGeom& pg, uint64_t n, const uint32_t* cell, uint32_t* counts, cudaStream_t st,
+                bool reset = true);
+// Place n particles into the slots allocated by slot_allocate (tags: tag[i],
+// or i when tag is null).  cursor: ncells uint32 scratch.
 void slot_scatter(Species& s, const ParticleGeom& pg, uint64_t n, const uint32_t* cell, const float* dx,
                   const float* dy, const float* px, const float* py, const float* pz, const uint32_t* tag,
                   uint32_t* cursor, cudaStream_t st);
+// The same in chunks: begin, then chunks of the species in any order (the
+// chunk's particles get tags tag0 + i when tag is null), then end.
+void slot_scatter_begin(Species& s, const ParticleGeom& pg, uint32_t* cursor, cudaStream_t st);
+void slot_scatter_chunk(Species& s, const ParticleGeom& pg, uint64_t n, uint32_t tag0, const uint32_t* cell,
+                        const float* dx, const float* dy, const float* px, const float* py, const float* pz,
+                        const uint32_t* tag, uint32_t* cursor, cudaStream_t st);
+void slot_scatter_end(Species& s, const ParticleGeom& pg, uint32_t* cursor, cudaStream_t st);
 // Download in reference order into device arrays indexed by tag.
 void slot_unpack(const Species& s, const ParticleGeom& pg, uint32_t* ix, uint32_t* iy, float* dx, float* dy,
                  float* px, float* py, float* pz, float* psa, float csqinv, cudaStream_t st);
