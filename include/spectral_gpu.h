@@ -106,7 +106,9 @@ SPX_API const char* spx_version(void);
  * them (src/prtls.rs:237-249,440); the GPU recomputes it and does not store it.
  * The arrays are host memory, pageable or page-locked (page-locked arrays are
  * copied at the full host-link rate, in chunks of 2^22 particles); the call
- * returns once they are no longer read.
+ * returns once they are no longer read.  The context keeps its upload scratch
+ * (4 B per particle of the largest species added, plus 2 x 96 MB) for later
+ * uploads; spx_destroy releases it (spx_batch_prepare for batch members).
  * The species id (0, 1, ...) is written to *species_out. */
 SPX_API int spx_add_species(spx_ctx* ctx, float charge, float mass, float vth, uint64_t n, const uint64_t* ix,
                     const uint64_t* iy, const float* dx, const float* dy, const float* px, const float* py,

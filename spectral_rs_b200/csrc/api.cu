@@ -16,6 +16,87 @@ struct StepGraph {
   int launches;  // kernel launches it holds
 };
 
+// Upload of the caller's arrays: chunks of UPLOAD_CHUNK particles cross PCIe
+// through two device buffers on a copy stream while the context's stream
+// packs the previous chunk, so the copies run back to back at the link's rate.
+// The buffers (and the packed cells of the species being added) are kept for
+// later uploads and released with the context: allocating and releasing
+// multi-GB staging per species cost more than the copies themselves, and a
+// release alone took up to 1.6 s on a busy device.
+constexpr uint64_t UPLOAD_CHUNK = 1ull << 22;  // particles per chunk
+constexpr size_t UPLOAD_BYTES = 24;            // per particle and buffer: dx..pz + psa (>= ix + iy)
+struct UploadRing {
+  cudaStream_t cs = nullptr;
+  cudaEvent_t ready[2] = {nullptr, nullptr}, done[2] = {nullptr, nullptr};
+  unsigned char* buf[2] = {nullptr, nullptr};
+  uint64_t chunk = 0;       // particles per buffer
+  uint32_t* cell = nullptr;  // packed cells (ix | iy << 16) of the species being added
+  uint64_t cell_n = 0;
+  // room for a species of n particles
+  void reserve(uint64_t n) {
+    if (!cs) {
+      SPX_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+      for (int b = 0; b < 2; ++b) {
+        SPX_CUDA_TRY(cudaEventCreateWithFlags(&ready[b], cudaEventDisableTiming));
+        SPX_CUDA_TRY(cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming));
+      }
+    }
+    const uint64_t m = std::max<uint64_t>(1, std::min(n, UPLOAD_CHUNK));
+    if (m > chunk) {
+      SPX_CUDA_TRY(cudaStreamSynchronize(cs));
+      chunk = 0;
+      for (int b = 0; b < 2; ++b) {
+        if (buf[b]) SPX_CUDA_TRY(cudaFree(buf[b]));
+        buf[b] = nullptr;
+        SPX_CUDA_TRY(cudaMalloc(&buf[b], UPLOAD_BYTES * m));
+      }
+      chunk = m;
+    }
+    if (std::max<uint64_t>(n, 1) > cell_n) {
+      if (cell) SPX_CUDA_TRY(cudaFree(cell));
+      cell = nullptr;
+      cell_n = 0;
+      SPX_CUDA_TRY(cudaMalloc(&cell, std::max<uint64_t>(n, 1) * 4));
+      cell_n = std::max<uint64_t>(n, 1);
+    }
+  }
+  void release() {
+    if (cs) cudaStreamSynchronize(cs);
+    for (int b = 0; b < 2; ++b) {
+      if (buf[b]) cudaFree(buf[b]);
+      if (ready[b]) cudaEventDestroy(ready[b]);
+      if (done[b]) cudaEventDestroy(done[b]);
+      buf[b] = nullptr;
+      ready[b] = done[b] = nullptr;
+    }
+    if (cell) cudaFree(cell);
+    if (cs) cudaStreamDestroy(cs);
+    cs = nullptr;
+    cell = nullptr;
+    chunk = cell_n = 0;
+  }
+  // copy(off, m, buf, stream) queues the host-to-device copies of particles
+  // [off, off + m); use(off, m, buf) queues the kernels that consume them on st.
+  template <class Copy, class Use>
+  void run(uint64_t n, cudaStream_t st, Copy copy, Use use) {
+    // the first copies wait for everything already queued on st (a previous
+    // pass may still read the buffers)
+    SPX_CUDA_TRY(cudaEventRecord(done[0], st));
+    SPX_CUDA_TRY(cudaStreamWaitEvent(cs, done[0], 0));
+    uint64_t k = 0;
+    for (uint64_t off = 0; off < n; off += chunk, ++k) {
+      const int b = (int)(k & 1);
+      const uint64_t m = std::min(chunk, n - off);
+      if (k >= 2) SPX_CUDA_TRY(cudaStreamWaitEvent(cs, done[b], 0));
+      copy(off, m, buf[b], cs);
+      SPX_CUDA_TRY(cudaEventRecord(ready[b], cs));
+      SPX_CUDA_TRY(cudaStreamWaitEvent(st, ready[b], 0));
+      use(off, m, buf[b]);
+      SPX_CUDA_TRY(cudaEventRecord(done[b], st));
+    }
+  }
+};
+
 struct spx_ctx {
   spx_params prm{};
   Grid g{};
@@ -41,6 +122,7 @@ struct spx_ctx {
   float last_timing[4] = {0, 0, 0, 0};
   uint64_t last_launches = 0;
   uint64_t repacks = 0, last_overflow = 0, last_max_occ = 0;
+  UploadRing up;  // spx_add_species scratch
 };
 
 static std::string g_create_err;
@@ -175,6 +257,7 @@ extern "C" int spx_destroy(spx_ctx* c) {
       if (p) cudaFree(p);
   }
   c->fb.release();
+  c->up.release();
   for (void* p : {(void*)c->d_err, (void*)c->d_diag, (void*)c->d_u32, (void*)c->d_counts})
     if (p) cudaFree(p);
   for (auto e : c->ev) cudaEventDestroy(e);
@@ -310,57 +393,6 @@ __global__ void k_pack_check(uint64_t n, uint64_t off, const uint64_t* ix, const
   }
 }
 
-// Upload of the caller's arrays: chunks of UPLOAD_CHUNK particles cross PCIe
-// through two device buffers on a copy stream while the context's stream
-// packs the previous chunk, so the copies run back to back at the link's rate.
-// Staging a whole species on the device instead (multi-GB allocations made and
-// released per species) cost more than the copies themselves.
-constexpr uint64_t UPLOAD_CHUNK = 1ull << 22;  // particles per chunk
-constexpr size_t UPLOAD_BYTES = 24;            // per particle and buffer: dx..pz + psa (>= ix + iy)
-struct UploadRing {
-  cudaStream_t cs = nullptr;
-  cudaEvent_t ready[2] = {nullptr, nullptr}, done[2] = {nullptr, nullptr};
-  unsigned char* buf[2] = {nullptr, nullptr};
-  explicit UploadRing(uint64_t n) {
-    const size_t bytes = UPLOAD_BYTES * std::max<uint64_t>(1, std::min(n, UPLOAD_CHUNK));
-    SPX_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-    for (int b = 0; b < 2; ++b) {
-      SPX_CUDA_TRY(cudaEventCreateWithFlags(&ready[b], cudaEventDisableTiming));
-      SPX_CUDA_TRY(cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming));
-      SPX_CUDA_TRY(cudaMalloc(&buf[b], bytes));
-    }
-  }
-  ~UploadRing() {
-    if (cs) cudaStreamSynchronize(cs);
-    for (int b = 0; b < 2; ++b) {
-      if (buf[b]) cudaFree(buf[b]);
-      if (ready[b]) cudaEventDestroy(ready[b]);
-      if (done[b]) cudaEventDestroy(done[b]);
-    }
-    if (cs) cudaStreamDestroy(cs);
-  }
-  // copy(off, m, buf, stream) queues the host-to-device copies of particles
-  // [off, off + m); use(off, m, buf) queues the kernels that consume them on st.
-  template <class Copy, class Use>
-  void run(uint64_t n, cudaStream_t st, Copy copy, Use use) {
-    // the first copies wait for everything already queued on st (a previous
-    // pass may still read the buffers)
-    SPX_CUDA_TRY(cudaEventRecord(done[0], st));
-    SPX_CUDA_TRY(cudaStreamWaitEvent(cs, done[0], 0));
-    uint64_t k = 0;
-    for (uint64_t off = 0; off < n; off += UPLOAD_CHUNK, ++k) {
-      const int b = (int)(k & 1);
-      const uint64_t m = std::min(UPLOAD_CHUNK, n - off);
-      if (k >= 2) SPX_CUDA_TRY(cudaStreamWaitEvent(cs, done[b], 0));
-      copy(off, m, buf[b], cs);
-      SPX_CUDA_TRY(cudaEventRecord(ready[b], cs));
-      SPX_CUDA_TRY(cudaStreamWaitEvent(st, ready[b], 0));
-      use(off, m, buf[b]);
-      SPX_CUDA_TRY(cudaEventRecord(done[b], st));
-    }
-  }
-};
-
 extern "C" int spx_add_species(spx_ctx* c, float charge, float mass, float vth, uint64_t n, const uint64_t* ix,
                                const uint64_t* iy, const float* dx, const float* dy, const float* px, const float* py,
                                const float* pz, const float* psa, int32_t* species_out) {
@@ -379,13 +411,9 @@ extern "C" int spx_add_species(spx_ctx* c, float charge, float mass, float vth, 
     s.beta = (charge / mass) * 0.5f * c->prm.dt;
     s.alpha = (charge / mass) * 0.5f * c->prm.dt / c->prm.c;
     s.n = n;
-    UploadRing up(n);
-    uint32_t* cell = nullptr;  // packed cells of the whole species (ix | iy << 16)
-    SPX_CUDA_TRY(cudaMalloc(&cell, std::max<uint64_t>(n, 1) * 4));
-    struct Release {
-      uint32_t* p;
-      ~Release() { cudaFree(p); }
-    } cell_release{cell};
+    UploadRing& up = c->up;
+    up.reserve(n);
+    uint32_t* const cell = up.cell;
     // pass 1: cell indices checked and packed on the device, occupancy per cell
     SPX_CUDA_TRY(cudaMemsetAsync(c->d_u32, 0xFF, sizeof(uint32_t), c->st));
     if (!c->plain) SPX_CUDA_TRY(cudaMemsetAsync(c->d_counts, 0, c->pg.ncells() * sizeof(uint32_t), c->st));
@@ -1183,6 +1211,7 @@ extern "C" int spx_batch_prepare(spx_batch* b) {
     spx_ctx* c = b->sims[i];
     if (c->species.empty()) return bfail(b, SPX_ERR_STATE, "simulation " + std::to_string(i) + " has no species");
     if (int rc = spx_prepare(c)) return bfail(b, rc, "simulation " + std::to_string(i) + ": " + c->err);
+    c->up.release();  // a batch holds many contexts: no upload scratch kept per member
   }
   try {
     b->sb.release();
