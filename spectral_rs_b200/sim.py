@@ -176,10 +176,15 @@ class Flds:
     def __init__(self, sim):
         self.sim = sim
 
-    def spatial(self, name, with_ghosts=True):
+    def spatial(self, name, with_ghosts=True, out=None):
+        """Field `name` as a float32 (rows, cols) array, into `out` when given
+        (C-contiguous float32 of that shape, e.g. a reused or page-locked buffer)."""
         s = self.sim
         shape = (s.size_y + 2, s.size_x + 2) if with_ghosts else (s.size_y, s.size_x)
-        out = np.empty(shape, dtype=np.float32)
+        if out is None:
+            out = np.empty(shape, dtype=np.float32)
+        elif out.shape != shape or out.dtype != np.float32 or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"out must be a C-contiguous float32 array of shape {shape}")
         s._chk(s.lib.spx_get_field(s._ctx, _lib.FIELD_IDS[name], 1 if with_ghosts else 0, _lib.ptr(out)))
         return out
 
