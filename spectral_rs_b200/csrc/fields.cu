@@ -121,18 +121,20 @@ __device__ __forceinline__ void bfly_tj(int q, int logN, int logB, bool t_fast, 
   }
 }
 
-// twiddles and DFTs of the thread's butterflies, slot q*R + r = input r of butterfly q
+// twiddles and DFTs of the thread's butterflies, slot q*R + r = input r of butterfly q;
+// Ns = 2^logNs (all index arithmetic is on powers of two: shifts and masks)
 template <int R>
-__device__ __forceinline__ void pass_compute(float2 (&v)[8], int logN, int logB, bool t_fast, int Ns,
+__device__ __forceinline__ void pass_compute(float2 (&v)[8], int logN, int logB, bool t_fast, int logNs,
                                              const float2* __restrict__ tw) {
   constexpr int PER = 8 / R;
+  constexpr int LR = R == 8 ? 3 : R == 4 ? 2 : 1;
 #pragma unroll
   for (int q = 0; q < PER; ++q) {
-    if (Ns > 1) {
+    if (logNs > 0) {
       int t, j;
       bfly_tj<R>(q, logN, logB, t_fast, t, j);
-      const int k = j & (Ns - 1);
-      const int step = (1 << logN) / (Ns * R);
+      const int k = j & ((1 << logNs) - 1);
+      const int step = 1 << (logN - logNs - LR);
 #pragma unroll
       for (int r = 1; r < R; ++r) v[q * R + r] = c_mul(v[q * R + r], __ldg(&tw[r * k * step]));
     }
@@ -148,16 +150,16 @@ __device__ __forceinline__ void pass_compute(float2 (&v)[8], int logN, int logB,
 
 template <int R>
 __device__ __forceinline__ void pass_store(const float2 (&v)[8], float2* s, int logN, int logB, int ES, int TS,
-                                           bool t_fast, int Ns) {
+                                           bool t_fast, int logNs) {
   constexpr int PER = 8 / R;
 #pragma unroll
   for (int q = 0; q < PER; ++q) {
     int t, j;
     bfly_tj<R>(q, logN, logB, t_fast, t, j);
-    const int k = j & (Ns - 1);
+    const int k = j & ((1 << logNs) - 1);
     const int base = t * TS + ((j - k) * R + k) * ES;
 #pragma unroll
-    for (int r = 0; r < R; ++r) s[spad(base + r * Ns * ES)] = v[q * R + r];
+    for (int r = 0; r < R; ++r) s[spad(base + ((r * ES) << logNs))] = v[q * R + r];
   }
 }
 
@@ -165,7 +167,8 @@ template <int R>
 __device__ __forceinline__ void pass_load(float2 (&v)[8], const float2* s, int logN, int logB, int ES, int TS,
                                           bool t_fast) {
   constexpr int PER = 8 / R;
-  const int nb = (1 << logN) / R;
+  constexpr int LR = R == 8 ? 3 : R == 4 ? 2 : 1;
+  const int nb = (1 << logN) >> LR;
 #pragma unroll
   for (int q = 0; q < PER; ++q) {
     int t, j;
@@ -180,22 +183,22 @@ __device__ __forceinline__ void pass_load(float2 (&v)[8], const float2* s, int l
 __device__ __forceinline__ void block_fft_regs(float2 (&v)[8], float2* s, int logN, int logB, int ES, int TS,
                                                bool t_fast, const float2* __restrict__ tw) {
   const int np = num_passes(logN);
-  pass_compute<8>(v, logN, logB, t_fast, 1, tw);
-  int Ns = 1;
+  pass_compute<8>(v, logN, logB, t_fast, 0, tw);
+  int logNs = 0;
   for (int i = 1; i < np; ++i) {
-    pass_store<8>(v, s, logN, logB, ES, TS, t_fast, Ns);  // only the last pass can have radix < 8
+    pass_store<8>(v, s, logN, logB, ES, TS, t_fast, logNs);  // only the last pass can have radix < 8
     __syncthreads();
-    Ns <<= 3;
+    logNs += 3;
     const int R = (i < np - 1) ? 8 : last_radix(logN);
     if (R == 8) {
       pass_load<8>(v, s, logN, logB, ES, TS, t_fast);
-      pass_compute<8>(v, logN, logB, t_fast, Ns, tw);
+      pass_compute<8>(v, logN, logB, t_fast, logNs, tw);
     } else if (R == 4) {
       pass_load<4>(v, s, logN, logB, ES, TS, t_fast);
-      pass_compute<4>(v, logN, logB, t_fast, Ns, tw);
+      pass_compute<4>(v, logN, logB, t_fast, logNs, tw);
     } else {
       pass_load<2>(v, s, logN, logB, ES, TS, t_fast);
-      pass_compute<2>(v, logN, logB, t_fast, Ns, tw);
+      pass_compute<2>(v, logN, logB, t_fast, logNs, tw);
     }
     __syncthreads();  // every thread has read before the next pass overwrites
   }
@@ -205,7 +208,8 @@ __device__ __forceinline__ void block_fft_regs(float2 (&v)[8], float2* s, int lo
 // butterfly q = m / R, r = m % R, e = j + r*N/R (k = j in the last pass).
 __device__ __forceinline__ void out_pos(int m, int logN, int logB, bool t_fast, int& t, int& e) {
   const int R = num_passes(logN) == 1 ? 8 : last_radix(logN);
-  const int q = m / R, r = m - q * R;
+  const int LR = R == 8 ? 3 : R == 4 ? 2 : 1;
+  const int q = m >> LR, r = m & (R - 1);
   int j;
   if (R == 8)
     bfly_tj<8>(q, logN, logB, t_fast, t, j);
@@ -213,7 +217,7 @@ __device__ __forceinline__ void out_pos(int m, int logN, int logB, bool t_fast, 
     bfly_tj<4>(q, logN, logB, t_fast, t, j);
   else
     bfly_tj<2>(q, logN, logB, t_fast, t, j);
-  e = j + r * ((1 << logN) / R);
+  e = j + (r << (logN - LR));
 }
 
 // ---------------------------------------------------------------- launch geometry

@@ -88,3 +88,24 @@ def test_chunked_upload_checks_every_chunk(where):
         assert _add(sim, a).sid == 0  # neither failure added a species; the context stays usable
         sim.prepare()
         sim.step(1)
+
+
+def test_upload_scratch_grows_and_reads_page_locked_arrays():
+    """A small species, then a large one from page-locked host memory (the
+    context's upload scratch grows between them), then a small one again."""
+    import torch
+    from spectral_rs_b200 import Sim
+    cfg = _cfg(**CFG)
+    big = _shuffled_species(cfg.params, 66, 6)
+    pinned = {}
+    for k, v in big.items():
+        t = torch.empty(len(v), dtype=torch.int64 if v.dtype == np.uint64 else torch.float32, pin_memory=True)
+        t.numpy().view(v.dtype)[:] = v
+        pinned[k] = t.numpy().view(v.dtype)
+    small = {k: v[:1000].copy() for k, v in big.items()}
+    with Sim(cfg) as sim:
+        prs = [_add(sim, small), _add(sim, pinned), _add(sim, small)]
+        for pr, a in zip(prs, (small, big, small)):
+            g = pr.state()
+            for k in ("ix", "iy", "dx", "dy", "px", "py", "pz", "psa"):
+                assert np.array_equal(g[k], a[k].astype(g[k].dtype)), k
