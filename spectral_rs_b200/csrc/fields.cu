@@ -222,7 +222,7 @@ __device__ __forceinline__ void out_pos(int m, int logN, int logB, bool t_fast, 
 
 // ---------------------------------------------------------------- launch geometry
 // Row pass: B rows per CTA with blockDim = N*B/8 threads.
-__host__ __device__ inline int row_logB(int logN) {
+__host__ __device__ constexpr int row_logB(int logN) {
   int lb = 11 - logN;  // N*B = 2048 -> 256 threads for small rows
   return lb < 0 ? 0 : lb;
 }
@@ -273,10 +273,19 @@ __device__ __forceinline__ void store_ghosted(float* dst, const Grid& g, int row
 // transform of <= 4096 points) runs the SMALL instantiation, bounded to three
 // such CTAs per SM (40 registers); 8192-point transforms need 1024 threads.
 #define FFT_BOUNDS(SMALL) __launch_bounds__((SMALL) ? 512 : 1024, (SMALL) ? 3 : 1)
+// LOGN > 0: the transform length 2^LOGN as a compile-time constant (every index
+// of the passes folds); LOGN = 0 reads it from the grid.
+constexpr int FFT_LOGN_MIN = 6, FFT_LOGN_MAX = 13;
 
-template <int IN, int OUT, bool INV, bool SMALL>
-__global__ void FFT_BOUNDS(SMALL) k_rows(const __grid_constant__ RowArgs a, Grid g, const float2* __restrict__ tw) {
+template <int IN, int OUT, bool INV, bool SMALL, int LOGN>
+__global__ void FFT_BOUNDS(SMALL) k_rows(const __grid_constant__ RowArgs a, Grid g0, const float2* __restrict__ tw) {
   extern __shared__ float2 sm[];
+  Grid g = g0;
+  if (LOGN) {
+    g.log2nx = LOGN;
+    g.nx = 1 << LOGN;
+    g.W = g.nx + 2;
+  }
   const int f = blockIdx.y;
   const int logN = g.log2nx, N = g.nx;
   const int logB = row_logB(logN);
@@ -335,9 +344,14 @@ __global__ void FFT_BOUNDS(SMALL) k_rows(const __grid_constant__ RowArgs a, Grid
 struct ColArgs {
   float2* data[8];
 };
-template <bool INV, bool SMALL>
-__global__ void FFT_BOUNDS(SMALL) k_cols(const __grid_constant__ ColArgs a, Grid g, const float2* __restrict__ tw) {
+template <bool INV, bool SMALL, int LOGN>
+__global__ void FFT_BOUNDS(SMALL) k_cols(const __grid_constant__ ColArgs a, Grid g0, const float2* __restrict__ tw) {
   extern __shared__ float2 sm[];
+  Grid g = g0;
+  if (LOGN) {
+    g.log2ny = LOGN;
+    g.ny = 1 << LOGN;
+  }
   const int f = blockIdx.y;
   const int logN = g.log2ny, N = g.ny;
   const int logW = col_logW(g.log2ny, g.log2nx);
@@ -672,42 +686,99 @@ void launch_filter_pass(const Grid& g, float* const* src, float* const* dst, int
 // Dynamic shared memory above 48 KB must be opted into once per kernel (on
 // every device that runs it; done when a context is created, never while a
 // stream is being captured).
-template <bool SMALL>
+// Rows: the launch is SMALL when it has at most 512 threads, known at compile
+// time for a given length.
+constexpr bool rows_small(int logN) { return ((1 << logN) << row_logB(logN)) / 8 <= 512; }
+
+static void fft_attr(const void* f) {
+  SPX_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+}
+template <int LOGN>
 static void fft_set_kernel_attributes() {
-  for (const void* f : {(const void*)k_rows<0, 0, false, SMALL>, (const void*)k_rows<1, 0, false, SMALL>,
-                        (const void*)k_rows<1, 0, true, SMALL>, (const void*)k_rows<1, 1, true, SMALL>,
-                        (const void*)k_cols<false, SMALL>, (const void*)k_cols<true, SMALL>})
-    SPX_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+  if constexpr (LOGN == 0) {
+    fft_attr((const void*)k_rows<0, 0, false, true, 0>);
+    fft_attr((const void*)k_rows<1, 0, false, true, 0>);
+    fft_attr((const void*)k_rows<1, 0, true, true, 0>);
+    fft_attr((const void*)k_rows<1, 1, true, true, 0>);
+    fft_attr((const void*)k_rows<0, 0, false, false, 0>);
+    fft_attr((const void*)k_rows<1, 0, false, false, 0>);
+    fft_attr((const void*)k_rows<1, 0, true, false, 0>);
+    fft_attr((const void*)k_rows<1, 1, true, false, 0>);
+  } else {
+    constexpr bool S = rows_small(LOGN);
+    fft_attr((const void*)k_rows<0, 0, false, S, LOGN>);
+    fft_attr((const void*)k_rows<1, 0, false, S, LOGN>);
+    fft_attr((const void*)k_rows<1, 0, true, S, LOGN>);
+    fft_attr((const void*)k_rows<1, 1, true, S, LOGN>);
+  }
+  fft_attr((const void*)k_cols<false, true, LOGN>);
+  fft_attr((const void*)k_cols<true, true, LOGN>);
+  fft_attr((const void*)k_cols<false, false, LOGN>);
+  fft_attr((const void*)k_cols<true, false, LOGN>);
+  if constexpr (LOGN == 0)
+    fft_set_kernel_attributes<FFT_LOGN_MIN>();
+  else if constexpr (LOGN < FFT_LOGN_MAX)
+    fft_set_kernel_attributes<LOGN + 1>();
 }
 void fields_set_kernel_attributes() {
-  fft_set_kernel_attributes<false>();
-  fft_set_kernel_attributes<true>();
-  SPX_CUDA_TRY(cudaFuncSetAttribute((const void*)k_filter_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    96 * 1024));
+  fft_set_kernel_attributes<0>();
+  fft_attr((const void*)k_filter_fused);
 }
 
-template <int IN, int OUT, bool INV>
-static void launch_rows(const Grid& g, const RowArgs& a, int nf, const float2* tw, cudaStream_t st) {
+template <int IN, int OUT, bool INV, int LOGN>
+static void launch_rows_n(const Grid& g, const RowArgs& a, int nf, const float2* tw, cudaStream_t st) {
   const int logB = row_logB(g.log2nx);
   const int threads = std::max(1, (g.nx << logB) / 8);
   const size_t smem = sizeof(float2) * fft_smem_elems(g.log2nx, logB);
   const int blocks = (g.ny + (1 << logB) - 1) >> logB;
-  if (threads <= 512)
-    k_rows<IN, OUT, INV, true><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
-  else
-    k_rows<IN, OUT, INV, false><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
+  if constexpr (LOGN > 0) {
+    k_rows<IN, OUT, INV, rows_small(LOGN), LOGN><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
+  } else {
+    if (threads <= 512)
+      k_rows<IN, OUT, INV, true, 0><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
+    else
+      k_rows<IN, OUT, INV, false, 0><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
+  }
 }
 
-template <bool INV>
-static void launch_cols(const Grid& g, const ColArgs& a, int nf, const float2* tw, cudaStream_t st) {
+template <bool INV, int LOGN>
+static void launch_cols_n(const Grid& g, const ColArgs& a, int nf, const float2* tw, cudaStream_t st) {
   const int logW = col_logW(g.log2ny, g.log2nx);
   const int threads = std::max(1, (g.ny << logW) / 8);
   const size_t smem = sizeof(float2) * fft_smem_elems(g.log2ny, logW);
   const int blocks = g.nx >> logW;
   if (threads <= 512)
-    k_cols<INV, true><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
+    k_cols<INV, true, LOGN><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
   else
-    k_cols<INV, false><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
+    k_cols<INV, false, LOGN><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
+}
+
+// Dispatch on the transform length: 2^6 .. 2^13 compiled per length, shorter ones generic.
+#define FFT_DISPATCH(LOG, CALL) \
+  switch (LOG) {                \
+    case 6: CALL(6); break;     \
+    case 7: CALL(7); break;     \
+    case 8: CALL(8); break;     \
+    case 9: CALL(9); break;     \
+    case 10: CALL(10); break;   \
+    case 11: CALL(11); break;   \
+    case 12: CALL(12); break;   \
+    case 13: CALL(13); break;   \
+    default: CALL(0); break;    \
+  }
+
+template <int IN, int OUT, bool INV>
+static void launch_rows(const Grid& g, const RowArgs& a, int nf, const float2* tw, cudaStream_t st) {
+#define SPX_ROWS(L) launch_rows_n<IN, OUT, INV, L>(g, a, nf, tw, st)
+  FFT_DISPATCH(g.log2nx, SPX_ROWS)
+#undef SPX_ROWS
+}
+
+template <bool INV>
+static void launch_cols(const Grid& g, const ColArgs& a, int nf, const float2* tw, cudaStream_t st) {
+#define SPX_COLS(L) launch_cols_n<INV, L>(g, a, nf, tw, st)
+  FFT_DISPATCH(g.log2ny, SPX_COLS)
+#undef SPX_COLS
 }
 
 void FieldBuffers::allocate(const Grid& grid) {
