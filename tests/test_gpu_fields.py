@@ -60,8 +60,9 @@ def test_gpu_fused_filter_bit_exact(nx, ny):
                               orc.field_op(nx, ny, 2, x, n_pass=npass, dtype=np.float32)), npass
 
 
+# every compiled transform length (2^6 .. 2^13) as rows and as columns, and the generic shorter ones
 @pytest.mark.parametrize("nx,ny", [(8, 8), (16, 32), (64, 8), (512, 64), (128, 1024), (2048, 16), (8192, 8),
-                                   (16, 2048)])
+                                   (16, 2048), (256, 4096), (4096, 128), (1024, 512), (32, 8192), (64, 256)])
 def test_gpu_fft2d_vs_numpy(nx, ny):
     rng = np.random.default_rng(nx * 7 + ny)
     x = (rng.standard_normal((ny, nx)) + 1j * rng.standard_normal((ny, nx))).astype(np.complex64)
