@@ -32,8 +32,9 @@ struct UploadRing {
   uint64_t chunk = 0;       // particles per buffer
   uint32_t* cell = nullptr;  // packed cells (ix | iy << 16) of the species being added
   uint64_t cell_n = 0;
-  // room for a species of n particles
-  void reserve(uint64_t n) {
+  // room for a species of n particles in nbuf chunk buffers (cells: also the
+  // packed-cell buffer of n)
+  void reserve(uint64_t n, bool cells = true, int nbuf = 2) {
     if (!cs) {
       SPX_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
       for (int b = 0; b < 2; ++b) {
@@ -42,17 +43,17 @@ struct UploadRing {
       }
     }
     const uint64_t m = std::max<uint64_t>(1, std::min(n, UPLOAD_CHUNK));
-    if (m > chunk) {
+    if (m > chunk) {  // all buffers share one size
       SPX_CUDA_TRY(cudaStreamSynchronize(cs));
-      chunk = 0;
       for (int b = 0; b < 2; ++b) {
         if (buf[b]) SPX_CUDA_TRY(cudaFree(buf[b]));
         buf[b] = nullptr;
-        SPX_CUDA_TRY(cudaMalloc(&buf[b], UPLOAD_BYTES * m));
       }
       chunk = m;
     }
-    if (std::max<uint64_t>(n, 1) > cell_n) {
+    for (int b = 0; b < nbuf; ++b)
+      if (!buf[b]) SPX_CUDA_TRY(cudaMalloc(&buf[b], UPLOAD_BYTES * chunk));
+    if (cells && std::max<uint64_t>(n, 1) > cell_n) {
       if (cell) SPX_CUDA_TRY(cudaFree(cell));
       cell = nullptr;
       cell_n = 0;
@@ -342,23 +343,6 @@ static uint32_t max_count(spx_ctx* c) {
 
 static Capacity choose_capacity(spx_ctx* c, uint64_t n) { return capacity_for(c, n, max_count(c)); }
 
-static int finish_species(spx_ctx* c, Species& s, Staging& st, uint64_t n, const uint32_t* d_tag) {
-  if (c->plain) {
-    for (float** p : {&s.plain.x, &s.plain.y, &s.plain.px, &s.plain.py, &s.plain.pz})
-      SPX_CUDA_TRY(cudaMalloc(p, std::max<uint64_t>(n, 1) * 4));
-    if (n) k_plain_from_cells<<<148 * 8, 256, 0, c->st>>>(n, st.cell, st.dx, st.dy, s.plain.x, s.plain.y);
-    SPX_CUDA_TRY(cudaMemcpyAsync(s.plain.px, st.px, n * 4, cudaMemcpyDeviceToDevice, c->st));
-    SPX_CUDA_TRY(cudaMemcpyAsync(s.plain.py, st.py, n * 4, cudaMemcpyDeviceToDevice, c->st));
-    SPX_CUDA_TRY(cudaMemcpyAsync(s.plain.pz, st.pz, n * 4, cudaMemcpyDeviceToDevice, c->st));
-  } else {
-    slot_count(c->pg, n, st.cell, c->d_counts, c->st);
-    const Capacity cap = choose_capacity(c, n);
-    slot_allocate(s, c->pg, cap.KL, cap.H, n);
-    slot_scatter(s, c->pg, n, st.cell, st.dx, st.dy, st.px, st.py, st.pz, d_tag, c->d_counts, c->st);
-  }
-  SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
-  return SPX_OK;
-}
 
 __global__ void k_check_cells(uint64_t n, const uint32_t* cell, int nx, int ny, int* derr) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -518,8 +502,6 @@ extern "C" int spx_init_species(spx_ctx* c, float charge, float mass, float vth,
     s.beta = (charge / mass) * 0.5f * c->prm.dt;
     s.alpha = (charge / mass) * 0.5f * c->prm.dt / c->prm.c;
     s.n = n;
-    Staging st;
-    st.alloc(n);
     InitSpec is;
     is.charge = charge;
     is.mass = mass;
@@ -532,8 +514,37 @@ extern "C" int spx_init_species(spx_ctx* c, float charge, float mass, float vth,
     is.x1 = (int)x1;
     is.random_positions = random_positions;
     is.seed = seed;
-    init_particles(is, c->g, n, st.cell, st.dx, st.dy, st.px, st.py, st.pz, c->st);
-    finish_species(c, s, st, n, nullptr);
+    // generated chunk by chunk into the upload ring and placed at once: every
+    // cell of columns [x0, x1) holds exactly ppc particles, so the slot capacity
+    // is known before the first particle exists
+    UploadRing& up = c->up;
+    up.reserve(n, false, 1);
+    if (c->plain) {
+      for (float** p : {&s.plain.x, &s.plain.y, &s.plain.px, &s.plain.py, &s.plain.pz})
+        SPX_CUDA_TRY(cudaMalloc(p, std::max<uint64_t>(n, 1) * 4));
+    } else {
+      const Capacity cap = capacity_for(c, n, ppc);
+      slot_allocate(s, c->pg, cap.KL, cap.H, n);
+      slot_scatter_begin(s, c->pg, c->d_counts, c->st);
+    }
+    for (uint64_t off = 0; off < n; off += up.chunk) {  // one stream, one buffer: chunks in order
+      const uint64_t m = std::min(up.chunk, n - off);
+      uint32_t* cl = reinterpret_cast<uint32_t*>(up.buf[0]);
+      float* f = reinterpret_cast<float*>(up.buf[0]) + m;  // dx, dy, px, py, pz after the cells
+      init_particles(is, c->g, off, m, cl, f, f + m, f + 2 * m, f + 3 * m, f + 4 * m, c->st);
+      if (c->plain) {
+        k_plain_from_cells<<<148 * 4, 256, 0, c->st>>>(m, cl, f, f + m, s.plain.x + off, s.plain.y + off);
+        float* const mom[3] = {s.plain.px, s.plain.py, s.plain.pz};
+        for (int k = 0; k < 3; ++k)
+          SPX_CUDA_TRY(cudaMemcpyAsync(mom[k] + off, f + (2 + k) * m, m * 4, cudaMemcpyDeviceToDevice, c->st));
+      } else {
+        slot_scatter_chunk(s, c->pg, m, (uint32_t)off, cl, f, f + m, f + 2 * m, f + 3 * m, f + 4 * m, nullptr,
+                           c->d_counts, c->st);
+      }
+    }
+    if (!c->plain) slot_scatter_end(s, c->pg, c->d_counts, c->st);
+    SPX_CUDA_TRY(cudaGetLastError());
+    SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
     c->species.push_back(s);
     if (species_out) *species_out = (int32_t)c->species.size() - 1;
     invalidate_graphs(c);

@@ -1489,14 +1489,15 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 ctr, uint2 key) {
 __device__ __forceinline__ float u01_open0(uint32_t x) { return ((x >> 8) + 1u) * (1.0f / 16777216.0f); }  // (0,1]
 __device__ __forceinline__ float u01(uint32_t x) { return (x >> 8) * (1.0f / 16777216.0f); }               // [0,1)
 
-__global__ void k_init(InitSpec is, int ny, uint64_t n, uint32_t* cell, float* dxo, float* dyo, float* pxo,
-                       float* pyo, float* pzo) {
+__global__ void k_init(InitSpec is, int ny, uint64_t off, uint64_t n, uint32_t* cell, float* dxo, float* dyo,
+                       float* pxo, float* pyo, float* pzo) {
   const int ncols = is.x1 - is.x0;
   const float c = is.c;
   const float csqinv = 1.0f / (c * c);
   const float g = is.gamma_drift;
   const float beta_inj = g > 1.0f ? is.sign_x * sqrtf(1.0f - 1.0f / (g * g)) : 0.0f;  // src/prtls.rs:224
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+  for (uint64_t o = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; o < n; o += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t i = off + o;  // particle index in the species (its RNG counter)
     const uint32_t k = (uint32_t)(i % is.ppc);
     const uint64_t cidx = i / is.ppc;
     const int col = is.x0 + (int)(cidx % ncols), row = (int)(cidx / ncols);
@@ -1530,18 +1531,18 @@ __global__ void k_init(InitSpec is, int ny, uint64_t n, uint32_t* cell, float* d
       px *= c;
     }
     const int ix = col + 1, iy = row + 1;
-    cell[i] = (uint32_t)ix | ((uint32_t)iy << 16);
-    dxo[i] = dx;
-    dyo[i] = dy;
-    pxo[i] = px;
-    pyo[i] = py;
-    pzo[i] = pz;
+    cell[o] = (uint32_t)ix | ((uint32_t)iy << 16);
+    dxo[o] = dx;
+    dyo[o] = dy;
+    pxo[o] = px;
+    pyo[o] = py;
+    pzo[o] = pz;
   }
 }
 
-void init_particles(const InitSpec& is, const Grid& g, uint64_t n, uint32_t* cell, float* dx, float* dy, float* px,
-                    float* py, float* pz, cudaStream_t st) {
-  if (n) k_init<<<148 * 16, 256, 0, st>>>(is, g.ny, n, cell, dx, dy, px, py, pz);
+void init_particles(const InitSpec& is, const Grid& g, uint64_t off, uint64_t n, uint32_t* cell, float* dx,
+                    float* dy, float* px, float* py, float* pz, cudaStream_t st) {
+  if (n) k_init<<<148 * 16, 256, 0, st>>>(is, g.ny, off, n, cell, dx, dy, px, py, pz);
   SPX_CUDA_TRY(cudaGetLastError());
 }
 

@@ -166,9 +166,10 @@ struct InitSpec {
   int random_positions;
   uint64_t seed;
 };
-// Writes particles in the reference's particle order into device arrays
-// (cell packed, dx, dy, px, py, pz); tag = index.
-void init_particles(const InitSpec& is, const Grid& g, uint64_t n, uint32_t* cell, float* dx, float* dy, float* px,
-                    float* py, float* pz, cudaStream_t st);
+// Writes particles [off, off + n) of the species, in the reference's particle
+// order, into device arrays (cell packed, dx, dy, px, py, pz) indexed from 0;
+// particle i depends only on i and the seed, so any chunking gives the same species.
+void init_particles(const InitSpec& is, const Grid& g, uint64_t off, uint64_t n, uint32_t* cell, float* dx,
+                    float* dy, float* px, float* py, float* pz, cudaStream_t st);
 
 }  // namespace spx

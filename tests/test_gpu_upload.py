@@ -109,3 +109,52 @@ def test_upload_scratch_grows_and_reads_page_locked_arrays():
             g = pr.state()
             for k in ("ix", "iy", "dx", "dy", "px", "py", "pz", "psa"):
                 assert np.array_equal(g[k], a[k].astype(g[k].dtype)), k
+
+
+def test_device_init_in_chunks_matches_a_single_chunk():
+    """spx_init_species generates a species chunk by chunk (particle i depends only
+    on i and the seed): the first rows of a 3-chunk species equal the whole of a
+    one-chunk species on a grid of fewer rows, every cell holds ppc particles, and
+    the plain path holds the same particles."""
+    from spectral_rs_b200 import Sim
+    big_cfg = _cfg(**CFG)
+    small_cfg = _cfg(**dict(CFG, size_y=8))
+    args = (-1.0, 1.0, 0.1, 66, 0, 512)
+    kw = dict(gamma_drift=1.2, sign_x=1.0, random_positions=True, seed=9)
+    with Sim(big_cfg) as sim:
+        big = sim.init_species(*args, **kw).state()
+        sim.prepare()
+        sim.step(1)
+    assert 2 * CHUNK < len(big["ix"]) < 3 * CHUNK
+    with Sim(small_cfg) as sim:
+        small = sim.init_species(*args, **kw).state()
+    n = len(small["ix"])
+    for k in ("ix", "iy", "dx", "dy", "px", "py", "pz", "psa"):
+        assert np.array_equal(big[k][:n], small[k]), k
+    assert np.all(np.bincount((big["iy"] - 1) * 512 + (big["ix"] - 1)) == 66)
+    with Sim(big_cfg, path="plain") as sim:
+        plain = sim.init_species(*args, **kw).state()
+    for k in ("px", "py", "pz"):
+        assert np.array_equal(plain[k], big[k]), k
+    f = np.float32
+    for c, d in (("ix", "dx"), ("iy", "dy")):
+        x = (big[c].astype(f) + big[d]).astype(f)
+        cx = np.floor((x + f(0.5)).astype(f))
+        assert np.array_equal(plain[c], cx.astype(np.uint64)), c
+        assert np.array_equal(plain[d], (x - cx).astype(f)), d
+
+
+def test_device_init_partial_columns_against_a_wall():
+    """Columns [x0, x1) of a wall grid (with the mirrored left wall): the slot
+    capacity comes from ppc before any particle exists; the species runs a few
+    steps against the wall."""
+    from spectral_rs_b200 import Sim
+    cfg = _cfg(size_x=512, size_y=64, delta=8, c=3.0, dt=0.1, dens=16, periodic_x=False, left_wall=True)
+    with Sim(cfg) as sim:
+        pr = sim.init_species(-1.0, 1.0, 0.1, 16, 8, 504, gamma_drift=1.1, sign_x=1.0, seed=3)
+        st = pr.state()
+        counts = np.bincount((st["iy"] - 1) * 512 + (st["ix"] - 1), minlength=512 * 64).reshape(64, 512)
+        assert np.all(counts[:, 8:504] == 16) and counts[:, :8].sum() == 0 and counts[:, 504:].sum() == 0
+        sim.prepare()
+        sim.step(5)
+        assert len(pr.state()["ix"]) == 64 * 496 * 16
