@@ -1097,13 +1097,11 @@ extern "C" int spx_fft2d(uint64_t nx, uint64_t ny, int32_t inverse, float* data)
     float2* d = nullptr;
     float2 *tx = nullptr, *ty = nullptr;
     SPX_CUDA_TRY(cudaMalloc(&d, bytes));
-    SPX_CUDA_TRY(cudaMalloc(&tx, nx * 8));
-    SPX_CUDA_TRY(cudaMalloc(&ty, ny * 8));
-    std::vector<float2> t(std::max(nx, ny));
-    make_twiddles((int)nx, t.data());
-    SPX_CUDA_TRY(cudaMemcpy(tx, t.data(), nx * 8, cudaMemcpyHostToDevice));
-    make_twiddles((int)ny, t.data());
-    SPX_CUDA_TRY(cudaMemcpy(ty, t.data(), ny * 8, cudaMemcpyHostToDevice));
+    const std::vector<float2> twx = make_pass_twiddles((int)nx), twy = make_pass_twiddles((int)ny);
+    SPX_CUDA_TRY(cudaMalloc(&tx, twx.size() * 8));
+    SPX_CUDA_TRY(cudaMalloc(&ty, twy.size() * 8));
+    SPX_CUDA_TRY(cudaMemcpy(tx, twx.data(), twx.size() * 8, cudaMemcpyHostToDevice));
+    SPX_CUDA_TRY(cudaMemcpy(ty, twy.data(), twy.size() * 8, cudaMemcpyHostToDevice));
     SPX_CUDA_TRY(cudaMemcpy(d, data, bytes, cudaMemcpyHostToDevice));
     fields_set_kernel_attributes();
     fft2d_inplace(g, d, tx, ty, inverse != 0, 0);

@@ -47,6 +47,34 @@ void make_twiddles(int n, float2* out) {
   }
 }
 
+// Pass-major twiddle records.  Every pass after the first (Ns = 8^p earlier
+// outputs per group, radix R) has Ns records of R float2 (8 for radix 8):
+// record k holds w^(r k step), r = 1 .. R-1, step = n / (Ns R), then one unused
+// slot, so a butterfly reads its twiddles as R/2 aligned 16-byte loads.  The
+// values are entries of make_twiddles(n).
+static int host_passes(int logN) { return logN / 3 + (logN % 3 ? 1 : 0); }
+static int host_last_radix(int logN) { return logN % 3 == 0 ? 8 : (logN % 3 == 2 ? 4 : 2); }
+size_t pass_twiddle_count(int n) {
+  const int logN = ilog2(n), np = host_passes(logN);
+  size_t total = 0;
+  for (int i = 1, logNs = 3; i < np; ++i, logNs += 3) total += ((size_t)1 << logNs) * (i < np - 1 ? 8 : host_last_radix(logN));
+  return std::max<size_t>(total, 2);
+}
+std::vector<float2> make_pass_twiddles(int n) {
+  std::vector<float2> tw(n), out(pass_twiddle_count(n), make_float2(0.f, 0.f));
+  make_twiddles(n, tw.data());
+  const int logN = ilog2(n), np = host_passes(logN);
+  size_t base = 0;
+  for (int i = 1, logNs = 3; i < np; ++i, logNs += 3) {
+    const int R = i < np - 1 ? 8 : host_last_radix(logN);
+    const int Ns = 1 << logNs, step = n / (Ns * R);
+    for (int k = 0; k < Ns; ++k)
+      for (int r = 1; r < R; ++r) out[base + (size_t)k * R + (r - 1)] = tw[(size_t)r * k * step];
+    base += (size_t)Ns * R;
+  }
+  return out;
+}
+
 // ---------------------------------------------------------------- complex
 __device__ __forceinline__ float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -122,21 +150,28 @@ __device__ __forceinline__ void bfly_tj(int q, int logN, int logB, bool t_fast, 
 }
 
 // twiddles and DFTs of the thread's butterflies, slot q*R + r = input r of butterfly q;
-// Ns = 2^logNs (all index arithmetic is on powers of two: shifts and masks)
+// Ns = 2^logNs (all index arithmetic is on powers of two: shifts and masks);
+// twp: this pass's twiddle records (make_pass_twiddles)
 template <int R>
 __device__ __forceinline__ void pass_compute(float2 (&v)[8], int logN, int logB, bool t_fast, int logNs,
-                                             const float2* __restrict__ tw) {
+                                             const float2* __restrict__ twp) {
   constexpr int PER = 8 / R;
-  constexpr int LR = R == 8 ? 3 : R == 4 ? 2 : 1;
 #pragma unroll
   for (int q = 0; q < PER; ++q) {
     if (logNs > 0) {
       int t, j;
       bfly_tj<R>(q, logN, logB, t_fast, t, j);
       const int k = j & ((1 << logNs) - 1);
-      const int step = 1 << (logN - logNs - LR);
+      const float4* rec = reinterpret_cast<const float4*>(twp + (size_t)k * R);
+      float2 w[R];
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[q * R + r] = c_mul(v[q * R + r], __ldg(&tw[r * k * step]));
+      for (int l = 0; l < R / 2; ++l) {
+        const float4 p = __ldg(rec + l);
+        w[2 * l] = make_float2(p.x, p.y);
+        w[2 * l + 1] = make_float2(p.z, p.w);
+      }
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[q * R + r] = c_mul(v[q * R + r], w[r - 1]);
     }
     if constexpr (R == 8) {
       dft8(v);
@@ -185,20 +220,22 @@ __device__ __forceinline__ void block_fft_regs(float2 (&v)[8], float2* s, int lo
   const int np = num_passes(logN);
   pass_compute<8>(v, logN, logB, t_fast, 0, tw);
   int logNs = 0;
+  const float2* twp = tw;  // records of the current pass
   for (int i = 1; i < np; ++i) {
     pass_store<8>(v, s, logN, logB, ES, TS, t_fast, logNs);  // only the last pass can have radix < 8
     __syncthreads();
+    if (i > 1) twp += (size_t)8 << logNs;  // the previous pass had radix 8
     logNs += 3;
     const int R = (i < np - 1) ? 8 : last_radix(logN);
     if (R == 8) {
       pass_load<8>(v, s, logN, logB, ES, TS, t_fast);
-      pass_compute<8>(v, logN, logB, t_fast, logNs, tw);
+      pass_compute<8>(v, logN, logB, t_fast, logNs, twp);
     } else if (R == 4) {
       pass_load<4>(v, s, logN, logB, ES, TS, t_fast);
-      pass_compute<4>(v, logN, logB, t_fast, logNs, tw);
+      pass_compute<4>(v, logN, logB, t_fast, logNs, twp);
     } else {
       pass_load<2>(v, s, logN, logB, ES, TS, t_fast);
-      pass_compute<2>(v, logN, logB, t_fast, logNs, tw);
+      pass_compute<2>(v, logN, logB, t_fast, logNs, twp);
     }
     __syncthreads();  // every thread has read before the next pass overwrites
   }
@@ -797,13 +834,11 @@ void FieldBuffers::allocate(const Grid& grid) {
     SPX_CUDA_TRY(cudaMalloc(&spec[i], cs));
     SPX_CUDA_TRY(cudaMemset(spec[i], 0, cs));
   }
-  std::vector<float2> t(std::max(g.nx, g.ny));
-  SPX_CUDA_TRY(cudaMalloc(&tw_x, g.nx * sizeof(float2)));
-  SPX_CUDA_TRY(cudaMalloc(&tw_y, g.ny * sizeof(float2)));
-  make_twiddles(g.nx, t.data());
-  SPX_CUDA_TRY(cudaMemcpy(tw_x, t.data(), g.nx * sizeof(float2), cudaMemcpyHostToDevice));
-  make_twiddles(g.ny, t.data());
-  SPX_CUDA_TRY(cudaMemcpy(tw_y, t.data(), g.ny * sizeof(float2), cudaMemcpyHostToDevice));
+  for (auto [dst, n] : {std::pair<float2**, int>{&tw_x, g.nx}, {&tw_y, g.ny}}) {
+    const std::vector<float2> t = make_pass_twiddles(n);
+    SPX_CUDA_TRY(cudaMalloc(dst, t.size() * sizeof(float2)));
+    SPX_CUDA_TRY(cudaMemcpy(*dst, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice));
+  }
 }
 
 void FieldBuffers::release() {

@@ -1,5 +1,7 @@
 // Pseudo-spectral field solver of the B200 hot path (src/flds/* of the reference).
 #pragma once
+#include <vector>
+
 #include "common.cuh"
 
 namespace spx {
@@ -46,6 +48,9 @@ int fft2d_inplace(const Grid& g, float2* data, const float2* tw_x, const float2*
 void fields_set_kernel_attributes();
 // Host generation of the FP64 twiddle table exp(-2 pi i m / n), m in [0, n).
 void make_twiddles(int n, float2* host_out);
+// The table the transform kernels read: per pass, per butterfly group, its
+// twiddles side by side (entries of make_twiddles(n)).
+std::vector<float2> make_pass_twiddles(int n);
 bool is_pow2(uint64_t v);
 int ilog2(uint64_t v);
 
