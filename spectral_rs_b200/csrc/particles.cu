@@ -408,8 +408,11 @@ __device__ __forceinline__ void bc_of(const StepArgs& a, int nx, int ny, int& ix
 }
 
 // BC: see bc_of.  T16: tiles of 16 x 16 cells (compile-time index arithmetic; else from a).
+// Species [s0, s1) of the step (all of them, or one per CTA when a small grid
+// splits the species across CTAs).
 template <bool PUSH, bool MOVE, bool COMP = false, int BC = BC_ANY, bool T16 = false>
-__device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, float* smem) {
+__device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, float* smem, const int s0,
+                                          const int s1) {
   const int TXc = T16 ? 16 : a.TX, TYc = T16 ? 16 : a.TY, logTXc = T16 ? 4 : a.logTX;
   const int TC = TXc * TYc;
   const int tx = tile % a.NTX, ty = tile / a.NTX;
@@ -464,7 +467,7 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
   const float csqinv = a.p.csqinv;
   const unsigned lt_mask = (1u << lane) - 1u;
 
-  for (int s = 0; s < a.ns; ++s) {
+  for (int s = s0; s < s1; ++s) {
     const SpeciesArgs& S = a.sp[s];
     const int K = S.K;
     const size_t tb = (size_t)tile * K * TC;  // this tile's block of slots
@@ -721,19 +724,22 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
 template <bool PUSH, bool MOVE, int BC, bool T16>
 __global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS) k_slot(const __grid_constant__ StepArgs a) {
   extern __shared__ float smem[];
-  slot_tile<PUSH, MOVE, false, BC, T16>(a, blockIdx.x, smem);
+  // gridDim.y > 1: CTA (tile, s) handles species s of the tile only
+  const int s0 = gridDim.y > 1 ? (int)blockIdx.y : 0, s1 = gridDim.y > 1 ? s0 + 1 : a.ns;
+  slot_tile<PUSH, MOVE, false, BC, T16>(a, blockIdx.x, smem, s0, s1);
 }
 
 // Compensated current sums: the extra registers allow one 256-thread CTA per SM.
 template <bool PUSH, int BC>
 __global__ void __launch_bounds__(256, 1) k_slot_comp(const __grid_constant__ StepArgs a) {
   extern __shared__ float smem[];
-  slot_tile<PUSH, true, true, BC>(a, blockIdx.x, smem);
+  const int s0 = gridDim.y > 1 ? (int)blockIdx.y : 0, s1 = gridDim.y > 1 ? s0 + 1 : a.ns;
+  slot_tile<PUSH, true, true, BC>(a, blockIdx.x, smem, s0, s1);
 }
 
 // the instantiation for (push, move, compensated, boundaries, 16 x 16 tiles)
 template <int BC, bool T16>
-static void launch_slot(bool push, bool move, bool comp, int grid, int threads, size_t smem, cudaStream_t st,
+static void launch_slot(bool push, bool move, bool comp, dim3 grid, int threads, size_t smem, cudaStream_t st,
                         const StepArgs& a) {
   if (comp && push)
     k_slot_comp<true, BC><<<grid, threads, smem, st>>>(a);
@@ -762,7 +768,7 @@ __global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS)
     __syncthreads();
     if (it >= nitems) break;
     const int2 item = items[it];
-    slot_tile<PUSH, MOVE, false, BC, T16>(args[item.x], item.y, smem);
+    slot_tile<PUSH, MOVE, false, BC, T16>(args[item.x], item.y, smem, 0, args[item.x].ns);
     __syncthreads();  // the shared windows are reused by the next item
   }
 }
@@ -957,14 +963,19 @@ int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysPar
   const bool comp = pp.compensated && move;
   const size_t smem = slot_smem_floats(pg.TX, pg.TY, push, move, comp) * sizeof(float);
   const bool t16 = pg.TX == 16 && pg.TY == 16;
+  // a grid whose tiles fill less than one wave of CTAs (148 SMs x 512 threads)
+  // takes one CTA per (tile, species): the species' particles are independent and
+  // the CTAs' deposit windows are added into the fields with atomics anyway
+  const bool split = a.ns > 1 && (size_t)pg.ntiles() * TC < (size_t)148 * 512;
+  const dim3 grid(pg.ntiles(), split ? a.ns : 1);
   if (pp.periodic_x && t16)
-    launch_slot<BC_PERIODIC, true>(push, move, comp, pg.ntiles(), TC, smem, st, a);
+    launch_slot<BC_PERIODIC, true>(push, move, comp, grid, TC, smem, st, a);
   else if (pp.periodic_x)
-    launch_slot<BC_PERIODIC, false>(push, move, comp, pg.ntiles(), TC, smem, st, a);
+    launch_slot<BC_PERIODIC, false>(push, move, comp, grid, TC, smem, st, a);
   else if (t16)
-    launch_slot<BC_WALL, true>(push, move, comp, pg.ntiles(), TC, smem, st, a);
+    launch_slot<BC_WALL, true>(push, move, comp, grid, TC, smem, st, a);
   else
-    launch_slot<BC_WALL, false>(push, move, comp, pg.ntiles(), TC, smem, st, a);
+    launch_slot<BC_WALL, false>(push, move, comp, grid, TC, smem, st, a);
   ++launches;
   for (int s = 0; s < a.ns; ++s) {
     // the overflow fallback reads its count on the device; a small fixed grid covers it

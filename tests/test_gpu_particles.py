@@ -182,14 +182,17 @@ def test_compensated_currents_track_fp64():
     assert errs[True] < 0.5 * errs[False]
 
 
+@pytest.mark.parametrize("grid", [(64, 32), (512, 256)])
 @pytest.mark.parametrize("tile", TILES)
 @pytest.mark.parametrize("periodic", [True, False])
-def test_fused_step_equals_per_phase_sequence(periodic, tile):
+def test_fused_step_equals_per_phase_sequence(periodic, tile, grid):
     """spx_step (push of step t fused with move+deposit of t+1, CUDA graphs) must
-    equal the reference's sequence of per-phase calls on the same device."""
+    equal the reference's sequence of per-phase calls on the same device.  The
+    64x32 grid is small enough for the fused kernel to take one CTA per (tile,
+    species); the 512x256 grid runs both species in every CTA."""
     from spectral_rs_b200 import Sim
-    cfg = _cfg(size_x=64, size_y=32, delta=0 if periodic else 6, c=3.0, dt=0.1, dens=8, periodic_x=periodic,
-               left_wall=not periodic, n_pass=2, tile_x=tile[0], tile_y=tile[1])
+    cfg = _cfg(size_x=grid[0], size_y=grid[1], delta=0 if periodic else 6, c=3.0, dt=0.1, dens=8,
+               periodic_x=periodic, left_wall=not periodic, n_pass=2, tile_x=tile[0], tile_y=tile[1])
     p = cfg.params
     sp = [(1.0, 16.0, 0.1, _species(p, 8, 0.1, 1.0, 1.0, 31)), (-1.0, 1.0, 0.1, _species(p, 8, 0.1, 1.0, 1.0, 32))]
     fused = Sim(cfg)
