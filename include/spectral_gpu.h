@@ -198,7 +198,8 @@ SPX_API void* spx_get_stream(const spx_ctx* ctx);
  * check, [3] slot capacity K of species 0, [4] tiles, [5] cells per tile,
  * [6] kernel launches of the last spx_step call, [7] device bytes held. */
 SPX_API int spx_get_counters(const spx_ctx* ctx, uint64_t* out8);
-/* Number of kernel launches issued by the last spx_step call. */
+/* Number of kernel launches issued by the last spx_step call (the kernels of a
+ * step launched as a CUDA graph counted one by one). */
 SPX_API uint64_t spx_last_launch_count(const spx_ctx* ctx);
 
 /* ---- Batches of independent simulations ------------------------------------
@@ -224,6 +225,7 @@ SPX_API int spx_batch_step(spx_batch* batch, uint32_t n);
 SPX_API int spx_batch_set_timing(spx_batch* batch, int32_t enable);
 SPX_API int spx_batch_get_timing(spx_batch* batch, float* out2);
 SPX_API void* spx_batch_get_stream(const spx_batch* batch);
+/* Kernels launched by the last spx_batch_step call (inside its graphs, one by one). */
 SPX_API uint64_t spx_batch_last_launch_count(const spx_batch* batch);
 
 /* Allocation-free binomial filter, for callers that cannot call cudaMalloc:

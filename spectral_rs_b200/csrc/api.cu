@@ -907,14 +907,11 @@ extern "C" int spx_step(spx_ctx* c, uint32_t n) {
         }
         const uint32_t key = parity_key(c);
         auto it = c->graphs.find(key);
-        if (it == c->graphs.end()) {
-          it = capture_step(c, key);
-          launches += it->second.launches - 1;
-        }
+        if (it == c->graphs.end()) it = capture_step(c, key);
         SPX_CUDA_TRY(cudaGraphLaunch(it->second.exec, c->st));
         if (!c->plain)
           for (auto& sp : c->species) sp.slot.ocur ^= 1;  // what slot_step does to the host-side state
-        launches += 1;
+        launches += it->second.launches;  // the kernels the graph runs
       }
     }
     c->last_launches = launches;
@@ -1344,12 +1341,9 @@ extern "C" int spx_batch_step(spx_batch* b, uint32_t steps) {
       }
       const uint32_t key = batch_key(b);
       auto it = b->graphs.find(key);
-      if (it == b->graphs.end()) {
-        it = capture_batch_step(b, key);
-        launches += it->second.launches - 1;
-      }
+      if (it == b->graphs.end()) it = capture_batch_step(b, key);
       SPX_CUDA_TRY(cudaGraphLaunch(it->second.exec, b->st));
-      ++launches;
+      launches += it->second.launches;  // the kernels the graph runs
       // what the captured step does to the host-side state
       for (spx_ctx* c : b->sims) {
         for (auto& sp : c->species) sp.slot.ocur ^= 1;
