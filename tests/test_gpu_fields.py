@@ -99,7 +99,9 @@ def _field_state(nx, ny, seed):
     return st, bw
 
 
-@pytest.mark.parametrize("nx,ny,n_pass", [(64, 32, 4), (128, 64, 1), (512, 64, 4)])
+# includes the benchmark's row length (4096) and column length (1024) and the 8192-point rows
+@pytest.mark.parametrize("nx,ny,n_pass", [(64, 32, 4), (128, 64, 1), (512, 64, 4), (4096, 64, 4), (1024, 256, 2),
+                                          (8192, 16, 8)])
 def test_gpu_fields_update_vs_oracle(nx, ny, n_pass):
     """Flds::update on identical inputs: E, B, filtered J and B_wrk against the FP64 oracle."""
     from spectral_rs_b200 import Sim
