@@ -2,32 +2,45 @@
 """Benchmark of the spectral_rs per-timestep hot path on B200.
 
 Metric: particle-steps/s (particles x steps / device time of the timed steps)
-and the HBM roofline fraction of the fused push + move + deposit kernel.
+and the HBM roofline fraction of the fused push + move + deposit kernel, for
+the batched split-position FP32 path against the plain FP32 path.
 
-Workload (one GPU): the plain method at scale -- a 2-D periodic thermal
-electron-proton plasma on a 4096 x 1024 grid, mass ratio 64, 64 particles per
-cell per species (536,870,912 particles), Maxwellian momenta with thermal
-spread 0.05c drawn from a seed, FP32 fields and particles, 4 binomial filter
-passes per step, c = 3.0, dt = 0.1 (Courant number c dt = 0.3; the reference
-algorithm is numerically unstable for this plasma at c dt = 0.45).  Synthetic
+Default workload (one GPU): the batched uneven ensemble -- 64 independent
+shock simulations (reflecting wall, mirror wall on the left) advanced together:
+one persistent particle launch over a work queue of (simulation, tile) items
+and one CUDA graph per step.  Grids from {128x128, 256x128, 512x256, 1024x256},
+4-32 particles per cell per species, mass ratio in {1, 16, 64}, upstream drift
+uniform in [0.05c, 0.3c], thermal spread 0.1c, seed 4242 (265,764,864
+particles), c = 3.0, dt = 0.1 (Courant number 0.3; the reference algorithm is
+numerically unstable for these plasmas at 0.45), 4 filter passes.  Synthetic
 data from the build's own seeded generator; a "step" is one iteration of the
-reference's loop (zero sources, move + deposit both species, ghost fold,
-Flds::update, Boris push).  The particle arrays (13 GB) exceed the 126 MB L2,
-so no flush is needed between steps.
+reference's loop for every member (zero sources, move + deposit, ghost fold,
+Flds::update, Boris push).  The particle state (several GB) exceeds the 126 MB
+L2, so no flush is needed between steps.
 
-Besides `value` (device-resident, split path) the line carries:
-  plain_fp32   the plain single-simulation FP32 GPU path on the same workload
-  roofline     the fused particle kernel: algorithmic bytes / CUDA-event time
-  cpu_baseline the C++ restatement of the reference CPU path (oracle/) on a crop
-  e2e          the same metric through the public API from host buffers
+The line carries:
+  value        device-resident, production launch path (one graph per step)
+  roofline     the batch particle kernel: 48 B x particles + 44 B x member cells
+               per launch / its CUDA-event time (a separate event-timed run)
+  plain_fp32   the plain single-simulation FP32 GPU path on the same members
+  cpu_baseline the C++ restatement of the reference CPU path (oracle/) on a
+               sample of the members (all host threads)
+  e2e          the same metric through the public API from pinned host buffers
+  thermal_c2   the 4096 x 1024 thermal e-p plasma (536,870,912 particles)
+  weibel_c5    the 8192 x 2048 Weibel pair plasma (1,073,741,824 particles)
   clocks       SM clocks sampled during the timed region
 
+--workload thermal|shock|weibel runs one simulation instead (same keys).
 --impl reference times the reference's CPU path (the oracle restatement; the
 Rust crate cannot be built here) on all host cores, same metric and workload,
-each step a 512 x 256 crop of it.
+each step one step of a bounded sample of it.
 
-Multi-GPU (torchrun): the workload does not shard without exchange steps, so
-N > 1 runs N independent replicas (weak scaling); the time is the max over ranks.
+Multi-GPU (torchrun): members are independent units with no exchange step.
+N ranks run an ensemble of 64 N members, rank r the contiguous block of 64
+starting at 64 r (the N = 1 workload is rank 0's block): every member runs on
+exactly one rank, the work per GPU is fixed (weak scaling), no collective is on
+the data path; the time is the max over ranks.  Single-simulation workloads run
+independent replicas.
 """
 import argparse
 import json
@@ -43,15 +56,14 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+
 def _sp(q, m, vth, ppc, gamma=0.0, sign=1.0):
     return dict(q=q, m=m, vth=vth, ppc=ppc, gamma=gamma, sign=sign)
 
 
-# Workloads (species: ions first, as run() creates them, src/lib.rs:124-126).
-# c = 3.0, dt = 0.1 everywhere: Courant number c dt = 0.3 (the reference
-# algorithm is numerically unstable for these plasmas at c dt = 0.45).
+# Single-simulation workloads (species: ions first, as run() creates them, src/lib.rs:124-126).
 WORKLOADS = {
-    # the headline: the plain method at scale
+    # the plain method at scale
     "thermal": dict(name="thermal_ep_4096x1024_ppc64", size_x=4096, size_y=1024, delta=0, dt=0.1, c=3.0, dens=64,
                     n_pass=4, periodic_x=True, left_wall=False,
                     species=[_sp(1.0, 64.0, 0.05, 64), _sp(-1.0, 1.0, 0.05, 64)],
@@ -73,6 +85,10 @@ WORKLOAD = WORKLOADS["thermal"]
 FALLBACK_HBM_GBS = 6650.0
 B_PER_PARTICLE = 48.0  # {cell, dx, dy, px, py, pz} read and written once
 B_PER_CELL = 44.0      # E, B read (24 B); Jx, Jy, Jz, rho, dens written (20 B)
+ENSEMBLE_SEED = 4242
+ENSEMBLE_GRIDS = ((128, 128), (256, 128), (512, 256), (1024, 256))
+ENSEMBLE_PER_RANK = 64
+CPU_SAMPLE_PARTICLES = 16_000_000  # members sampled for the CPU legs, in list order
 
 
 def params(w, **over):
@@ -152,19 +168,98 @@ def measured_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def traffic_per_launch(particles, cells):
-    """dram bytes of the fused kernel from the committed ncu summary, scaled to this launch."""
+def traffic_per_launch(particles, cells, name="k_slot_traffic.json"):
+    """dram bytes of the particle kernel from a committed ncu summary, scaled to this launch."""
     try:
-        with open(os.path.join(ROOT, "profiles", "k_slot_traffic.json")) as f:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
             t = json.load(f)
         return t["dram_bytes_per_particle"] * particles + t.get("dram_bytes_per_cell", 0.0) * cells
     except (OSError, KeyError, ValueError):
         return None
 
 
+def roofline(particles, cells, kern_ms, kernel, traffic_file):
+    peak, peak_kind = measured_peak()
+    alg = B_PER_PARTICLE * particles + B_PER_CELL * cells
+    achieved = alg / (kern_ms / 1e3) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic_per_launch(particles, cells, traffic_file), "peak_kind": peak_kind,
+            "kernel": kernel, "kernel_ms": kern_ms, "alg_bytes_per_launch": alg,
+            "alg_bytes": f"{B_PER_PARTICLE:g} B x {particles} particles + {B_PER_CELL:g} B x {cells} cells"}
+
+
+def _events(stream):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    return e0, e1
+
+
+# ---------------------------------------------------------------- the ensemble's members
+def ensemble_members(n=64, seed=ENSEMBLE_SEED):
+    """The uneven shock ensemble, drawn from a fixed seed: shocks against the
+    reflecting wall, grids from ENSEMBLE_GRIDS, ppc in [4, 32], mass ratio in
+    {1, 16, 64}, upstream drift uniform in [0.05c, 0.3c], thermal spread 0.1c.
+    A longer list extends a shorter one (the first 64 members never change)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        nx, ny = ENSEMBLE_GRIDS[rng.integers(len(ENSEMBLE_GRIDS))]
+        beta = float(rng.uniform(0.05, 0.3))
+        out.append(dict(size_x=nx, size_y=ny, ppc=int(rng.integers(4, 33)),
+                        mass_ratio=float(rng.choice([1.0, 16.0, 64.0])), beta=beta,
+                        gamma=1.0 / np.sqrt(1.0 - beta * beta)))
+    return out
+
+
+def rank_members(per_rank, rank, world):
+    """Member indices of `rank`: the contiguous block [per_rank * rank, per_rank * (rank + 1))
+    of an ensemble of per_rank * world members (each member on exactly one rank)."""
+    return list(range(per_rank * rank, per_rank * (rank + 1)))
+
+
+def ensemble_config(m):
+    from spectral_rs_b200.config import Config, Params, Setup, Output
+    p = Params(size_x=m["size_x"], size_y=m["size_y"], delta=8, dt=0.1, c=3.0, dens=m["ppc"],
+               gamma_inj=m["gamma"], n_pass=4, mass_ratio=m["mass_ratio"], vth=0.1, periodic_x=False,
+               left_wall=True)
+    return Config(p, Setup(0), Output(False, False, 1, 1, 1, 1))
+
+
+def member_species(m):
+    """(charge, mass, vth, ppc, drift gamma) of a member's two species, ions first."""
+    return [(1.0, m["mass_ratio"], 0.1, m["ppc"], m["gamma"]), (-1.0, 1.0, 0.1, m["ppc"], m["gamma"])]
+
+
+def member_particles(m):
+    return 2 * m["ppc"] * (m["size_x"] - 16) * m["size_y"]
+
+
+def member_arrays(m, seed):
+    """Host arrays of a member's species (random positions in the cell, the build's seeded generator)."""
+    from spectral_rs_b200.config import SpeciesSpec
+    from spectral_rs_b200.init import species_arrays
+    p = ensemble_config(m).params
+    p.random_positions, p.seed = True, seed
+    return [(q, mass, vth, species_arrays(p, SpeciesSpec(q, mass, vth, ppc, g, 1.0, 8, m["size_x"] - 8),
+                                          seed_offset=k))
+            for k, (q, mass, vth, ppc, g) in enumerate(member_species(m))]
+
+
+def cpu_sample(members, target=CPU_SAMPLE_PARTICLES):
+    """Indices of the members the CPU legs time: the list's first members up to `target` particles."""
+    idx, acc = [], 0
+    for i, m in enumerate(members):
+        idx.append(i)
+        acc += member_particles(m)
+        if acc >= target:
+            break
+    return idx
+
+
 # ---------------------------------------------------------------- CPU (oracle) arms
 def oracle_crop_rate(w, seconds_target, steps=None, warmup=1):
-    """The reference CPU path (C++ restatement, all host threads) on a crop of the workload."""
+    """The reference CPU path (C++ restatement, all host threads) on a crop of a single-simulation workload."""
     from oracle import oracle as orc
     from spectral_rs_b200.config import SpeciesSpec
     from spectral_rs_b200.init import species_arrays
@@ -193,18 +288,60 @@ def oracle_crop_rate(w, seconds_target, steps=None, warmup=1):
     return n * steps / dt, orc.num_threads(), sample, dt
 
 
+def oracle_ensemble_rate(members, seconds_target, steps=None, warmup=1):
+    """The reference CPU path on a sample of the ensemble's members: one step is one
+    loop iteration of every sampled member, one member after another (the reference
+    runs one simulation per process, its push parallel over all host threads)."""
+    from oracle import oracle as orc
+    idx = cpu_sample(members)
+    sims, n = [], 0
+    for i in idx:
+        m = members[i]
+        o = orc.OracleSim.from_params(ensemble_config(m).params, dtype=np.float32)
+        for q, mass, vth, a in member_arrays(m, 7000 + i):
+            o.add_species(q, mass, vth, a["ix"], a["iy"], a["dx"], a["dy"], a["px"], a["py"], a["pz"], a["psa"])
+            n += len(a["ix"])
+        o.prepare()
+        sims.append(o)
+
+    def one_step():
+        for o in sims:
+            o.step(1)
+
+    for _ in range(warmup):
+        one_step()
+    if steps is None:
+        t0 = time.perf_counter()
+        one_step()
+        steps = max(1, int(seconds_target / max(time.perf_counter() - t0, 1e-3)))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one_step()
+    dt = time.perf_counter() - t0
+    for o in sims:
+        o.close()
+    sample = (f"members {idx[0]}-{idx[-1]} of the ensemble ({len(idx)} of {len(members)} shocks, full size), "
+              f"{n} particles, {steps} steps")
+    return n * steps / dt, orc.num_threads(), sample, dt
+
+
 def run_reference(args, w):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    # bounded sample: the crop is ~1/32 of the workload; each step is one loop iteration of it
-    rate, cores, sample, dt = oracle_crop_rate(w, 0, steps=args.steps, warmup=args.warmup)
+    if w is None:
+        members = ensemble_members(ENSEMBLE_PER_RANK)
+        rate, cores, sample, dt = oracle_ensemble_rate(members, 0, steps=args.steps, warmup=args.warmup)
+        cfg = {"workload": f"ensemble_{len(members)}_shocks", "seed": ENSEMBLE_SEED, "sample": sample}
+    else:
+        # bounded sample: the crop is ~1/32 of the workload; each step is one loop iteration of it
+        rate, cores, sample, dt = oracle_crop_rate(w, 0, steps=args.steps, warmup=args.warmup)
+        cfg = {"workload": w["name"], "grid": [w["size_x"], w["size_y"]],
+               "ppc_per_species": [sp["ppc"] for sp in w["species"]], "sample": sample}
     line = {"metric": "particle-steps/s", "value": rate, "unit": "particle-steps/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded)", "impl": "reference",
-            "config": {"workload": w["name"], "grid": [w["size_x"], w["size_y"]],
-                       "ppc_per_species": [sp["ppc"] for sp in w["species"]], "sample": sample},
+            "data": "synthetic (seeded)", "impl": "reference", "config": cfg,
             "cpu_baseline": {"value": rate, "unit": "particle-steps/s", "cores": cores, "kind": "port",
                              "sample": sample + " (C++ restatement of the reference CPU path)"},
             "e2e": {"value": rate, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -228,14 +365,74 @@ def max_over_ranks(ms, device="cpu"):
     return float(t.item())
 
 
-# ---------------------------------------------------------------- GPU arm
-def e2e_run(w, steps, seed):
-    """Same metric through the public API from pinned host buffers: upload both
+def _barrier(dist):
+    if dist:
+        dist.barrier()
+
+
+# ---------------------------------------------------------------- single-simulation measurement
+def measure_single(w, steps, warmup, seed, dist=None, sampler=None, timed_steps=3):
+    """value: `steps` graph-launched steps (the production path), device-resident;
+    then `timed_steps` event-timed steps for the phase split and the particle kernel's time."""
+    import torch
+    sim = make_sim(w, "split", seed)
+    n_particles = sum(len(p) for p in sim.prtls)
+    sim.prepare()
+    sim.step(warmup)
+    stream = torch.cuda.ExternalStream(sim.stream())
+    _barrier(dist)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.start()
+    e0, e1 = _events(stream)
+    sim.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    clocks = sampler.stop() if sampler else None
+    ms = e0.elapsed_time(e1)
+    launches = sim.last_launch_count()
+    sim.set_timing(True)  # per-step CUDA events around each phase, on the library's stream
+    sim.step(timed_steps)
+    phases = [float(x) / timed_steps for x in sim.timing()]  # particles, fold, field update, step
+    sim.set_timing(False)
+    counters = sim.counters()
+    diag = sim.diag()
+    sim.close()
+    cells = w["size_x"] * w["size_y"]
+    return {"particles": n_particles, "ms": ms, "launches": launches, "clocks": clocks, "counters": counters,
+            "value": n_particles * steps / (ms / 1e3), "ms_per_step": ms / steps,
+            "phase_ms_per_step": dict(zip(("particles", "fold", "fields", "step"), phases)),
+            "roofline": roofline(n_particles, cells, phases[0], "k_slot<push,move> (fused push + move + deposit)",
+                                 "k_slot_traffic.json"),
+            "diag": {"field_energy_E": diag[0], "field_energy_B": diag[1], "kinetic": diag[2]}}
+
+
+def plain_single(w, steps, seed):
+    import torch
+    ps = make_sim(w, "plain", seed)
+    n = sum(len(p) for p in ps.prtls)
+    ps.prepare()
+    ps.step(1)
+    stream = torch.cuda.ExternalStream(ps.stream())
+    torch.cuda.synchronize()
+    a0, a1 = _events(stream)
+    ps.step(steps)
+    a1.record(stream)
+    a1.synchronize()
+    pms = a0.elapsed_time(a1)
+    ps.close()
+    return {"value": n * steps / (pms / 1e3), "unit": "particle-steps/s", "ms_per_step": pms / steps, "steps": steps,
+            "path": "plain FP32 (global x = ix + dx, per-phase kernels, global atomics, no sort)"}
+
+
+def e2e_single(w, steps, seed):
+    """Same metric through the public API from pinned host buffers: upload every
     species, prepare, `steps` steps, read the saved fields (into pinned host
     buffers) and the diagnostics back."""
     import torch
     from spectral_rs_b200 import Sim
-    from spectral_rs_b200.config import Config, Setup, Output, SpeciesSpec
+    from spectral_rs_b200.config import Config, Setup, Output
     from spectral_rs_b200.init import positions, draws, velocities
     p = params(w, random_positions=True, seed=seed)
     host = []
@@ -261,16 +458,12 @@ def e2e_run(w, steps, seed):
     cfg = Config(p, Setup(steps), Output(False, False, 1, 1, 1, 1))
     sim = Sim(cfg)
     names = ("Jx", "Jy", "Jz", "Ex", "Ey", "Ez", "Bx", "By", "Bz", "Dens")
-    # page-locked result buffers, like the inputs
     outs = [torch.empty((p.size_y, p.size_x), dtype=torch.float32, pin_memory=True).numpy() for _ in names]
     h2d = sum(a["ix"].nbytes + a["iy"].nbytes + 6 * a["dx"].nbytes for (_, a) in host)
     t0 = time.perf_counter()
-    per_species = []
     for sp, a in host:
-        ts = time.perf_counter()
         sim.add_species(sp["q"], sp["m"], sp["vth"], a["ix"], a["iy"], a["dx"], a["dy"], a["px"], a["py"], a["pz"],
                         a["psa"])
-        per_species.append(time.perf_counter() - ts)
     t1 = time.perf_counter()
     sim.prepare()
     t2 = time.perf_counter()
@@ -284,13 +477,59 @@ def e2e_run(w, steps, seed):
     sim.close()
     return {"value": n * steps / dt, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d / steps,
             "d2h_bytes_per_step": d2h / steps, "wall_s": dt,
-            "split_s": {"upload": t1 - t0, "upload_per_species": per_species, "prepare": t2 - t1, "steps": t3 - t2,
-                        "readback": t0 + dt - t3},
-            "scope": "pinned host arrays -> spx_add_species x2 -> spx_prepare -> spx_step(K) -> 10 fields "
+            "split_s": {"upload": t1 - t0, "prepare": t2 - t1, "steps": t3 - t2, "readback": t0 + dt - t3},
+            "scope": "pinned host arrays -> spx_add_species per species -> spx_prepare -> spx_step(K) -> 10 fields "
                      "(into pinned host buffers) + diag to host"}
 
 
-def run_gpu(args, w):
+def run_single(args, w):
+    import torch
+    rank, world, local, dist = _init_ranks()
+    seed = rank_seed(args.seed, rank)
+    e2e = e2e_single(w, args.steps, seed) if rank == 0 and not args.no_e2e else None
+    if e2e is not None:
+        e2e["ranks_measured"] = 1
+    r = measure_single(w, args.steps, args.warmup, seed, dist, ClockSampler(local))
+    ms = max_over_ranks(r["ms"], device="cuda") if dist else r["ms"]
+    value = r["particles"] * args.steps * world / (ms / 1e3)
+    plain = plain_single(w, args.plain_steps, seed) if rank == 0 and not args.no_plain else None
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, cores, sample, _ = oracle_crop_rate(w, args.cpu_seconds)
+        cpu = {"value": rate, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+               "sample": sample + " (C++ restatement of the reference CPU path, OpenMP push/FFT, serial deposit)"}
+    if rank == 0:
+        line = _line(args, world, value, ms, w["name"], r["launches"], r["clocks"])
+        line["config"].update({"grid": [w["size_x"], w["size_y"]],
+                               "species": [{"charge": sp["q"], "mass": sp["m"], "vth": sp["vth"], "ppc": sp["ppc"],
+                                            "drift_gamma": sp["gamma"], "drift_sign": sp["sign"]}
+                                           for sp in w["species"]],
+                               "particles_per_gpu": r["particles"], "n_pass": w["n_pass"], "c": w["c"], "dt": w["dt"],
+                               "delta": w["delta"], "periodic_x": w["periodic_x"], "left_wall": w["left_wall"],
+                               "path": "split, one CUDA graph per step",
+                               "parallelism": "replicas" if world > 1 else "single",
+                               "l2": _l2_note(r["particles"])})
+        line.update({"roofline": r["roofline"], "phase_ms_per_step": r["phase_ms_per_step"], "plain_fp32": plain,
+                     "cpu_baseline": cpu, "e2e": e2e, "layout": r["counters"], "diag": r["diag"]})
+        if plain:
+            line["split_vs_plain"] = value / world / plain["value"]
+        print(json.dumps(line), flush=True)
+    _finish(dist)
+
+
+def _l2_note(particles):
+    return (f"inputs larger than L2 ({24 * particles / 1e9:.1f} GB particle state)" if 24 * particles > 126e6
+            else "inputs smaller than L2 (no flush)")
+
+
+def _line(args, world, value, ms, workload, launches, clocks):
+    return {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": workload}, "gpu_launches": launches, "clocks": clocks}
+
+
+def _init_ranks():
     import torch
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -301,223 +540,214 @@ def run_gpu(args, w):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    seed = rank_seed(args.seed, rank)
-
-    # end to end through the public API, first, on the clean device; rank 0 only (the pinned
-    # host copy of the workload is 21 GB per rank)
-    e2e = e2e_run(w, args.steps, seed) if rank == 0 and not args.no_e2e else None
-    if e2e is not None:
-        e2e["ranks_measured"] = 1
-
-    sim = make_sim(w, "split", seed)
-    n_particles = sum(len(p) for p in sim.prtls)
-    cells = w["size_x"] * w["size_y"]
-    sim.prepare()
-    sim.step(args.warmup)
-    stream = torch.cuda.ExternalStream(sim.stream())
-    sim.set_timing(True)  # per-step CUDA events around each phase, on the library's stream
-    sampler = ClockSampler(local)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    sampler.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    sim.step(args.steps)
-    e1.record(stream)
-    e1.synchronize()
-    torch.cuda.synchronize()
-    clocks = sampler.stop()
-    ms = e0.elapsed_time(e1)
-    phases = sim.timing()  # [particles, fold, field update, step] summed over the steps
-    launches = sim.last_launch_count()
-    counters = sim.counters()
-    sim.set_timing(False)
-    diag = sim.diag()
-    if dist:
-        ms = max_over_ranks(ms, device="cuda")
-        dist.barrier()
-    sim.close()
-    del sim
-    value = n_particles * args.steps * world / (ms / 1e3)
-
-    peak, peak_kind = measured_peak()
-    kern_ms = float(phases[0]) / args.steps
-    alg_bytes = B_PER_PARTICLE * n_particles + B_PER_CELL * cells
-    achieved = alg_bytes / (kern_ms / 1e3) / 1e9
-    traffic = traffic_per_launch(n_particles, cells)
+    return rank, world, local, dist
 
 
-    plain = None
-    if not args.no_plain and rank == 0:
-        ps = make_sim(w, "plain", seed)
-        ps.prepare()
-        ps.step(1)
-        stream_p = torch.cuda.ExternalStream(ps.stream())
-        torch.cuda.synchronize()
-        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a0.record(stream_p)
-        ps.step(args.plain_steps)
-        a1.record(stream_p)
-        a1.synchronize()
-        pms = a0.elapsed_time(a1)
-        ps.close()
-        plain = {"value": n_particles * args.plain_steps / (pms / 1e3), "unit": "particle-steps/s",
-                 "ms_per_step": pms / args.plain_steps, "steps": args.plain_steps,
-                 "path": "plain FP32 (global x = ix + dx, per-phase kernels, global atomics, no sort)"}
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        rate, cores, sample, _ = oracle_crop_rate(w, args.cpu_seconds)
-        cpu = {"value": rate, "unit": "particle-steps/s", "cores": cores, "kind": "port",
-               "sample": sample + " (C++ restatement of the reference CPU path, OpenMP push/FFT, serial deposit)"}
-
-    if rank == 0:
-        line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic (seeded device init)",
-                "config": {"workload": w["name"], "grid": [w["size_x"], w["size_y"]],
-                           "species": [{"charge": sp["q"], "mass": sp["m"], "vth": sp["vth"], "ppc": sp["ppc"],
-                                        "drift_gamma": sp["gamma"], "drift_sign": sp["sign"]}
-                                       for sp in w["species"]],
-                           "particles_per_gpu": n_particles, "n_pass": w["n_pass"], "c": w["c"], "dt": w["dt"],
-                           "delta": w["delta"], "periodic_x": w["periodic_x"], "left_wall": w["left_wall"],
-                           "path": "split", "parallelism": "replicas" if world > 1 else "single",
-                           "l2": f"inputs larger than L2 ({24 * n_particles / 1e9:.1f} GB particle state)"
-                           if 24 * n_particles > 126e6 else "inputs smaller than L2 (no flush)"},
-                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                             "kernel": "k_slot<push,move> (fused push + move + deposit)",
-                             "kernel_ms": kern_ms, "alg_bytes_per_launch": alg_bytes},
-                "phase_ms_per_step": {"particles": float(phases[0]) / args.steps,
-                                      "fold": float(phases[1]) / args.steps,
-                                      "fields": float(phases[2]) / args.steps,
-                                      "step": float(phases[3]) / args.steps},
-                "plain_fp32": plain, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-                "gpu_launches": launches, "layout": counters,
-                "diag": {"field_energy_E": diag[0], "field_energy_B": diag[1], "kinetic": diag[2]}}
-        if plain:
-            line["split_vs_plain"] = value / world / plain["value"]
-        print(json.dumps(line), flush=True)
+def _finish(dist):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
 
 
 # ---------------------------------------------------------------- batched uneven ensemble
-ENSEMBLE_SEED = 4242
-ENSEMBLE_GRIDS = ((128, 128), (256, 128), (512, 256), (1024, 256))
+def _build_batch(members, idx):
+    from spectral_rs_b200 import Batch
+    b = Batch([ensemble_config(members[i]) for i in idx])
+    for sim, i in zip(b.sims, idx):
+        m = members[i]
+        for k, (q, mass, vth, ppc, g) in enumerate(member_species(m)):
+            sim.init_species(q, mass, vth, ppc, 8, m["size_x"] - 8, g, 1.0, True, 2 * i + k + 1)
+    return b
 
 
-def ensemble_members(n=64, seed=ENSEMBLE_SEED):
-    """The uneven shock ensemble, drawn from a fixed seed: shocks against the
-    reflecting wall, grids from ENSEMBLE_GRIDS, ppc in [4, 32], mass ratio in
-    {1, 16, 64}, upstream drift uniform in [0.05c, 0.3c], thermal spread 0.1c."""
-    rng = np.random.default_rng(seed)
-    out = []
-    for _ in range(n):
-        nx, ny = ENSEMBLE_GRIDS[rng.integers(len(ENSEMBLE_GRIDS))]
-        beta = float(rng.uniform(0.05, 0.3))
-        out.append(dict(size_x=nx, size_y=ny, ppc=int(rng.integers(4, 33)),
-                        mass_ratio=float(rng.choice([1.0, 16.0, 64.0])), beta=beta,
-                        gamma=1.0 / np.sqrt(1.0 - beta * beta)))
-    return out
-
-
-def ensemble_config(m):
-    from spectral_rs_b200.config import Config, Params, Setup, Output
-    p = Params(size_x=m["size_x"], size_y=m["size_y"], delta=8, dt=0.1, c=3.0, dens=m["ppc"],
-               gamma_inj=m["gamma"], n_pass=4, mass_ratio=m["mass_ratio"], vth=0.1, periodic_x=False,
-               left_wall=True)
-    return Config(p, Setup(0), Output(False, False, 1, 1, 1, 1))
-
-
-def run_ensemble(args):
+def measure_ensemble(members, idx, steps, warmup, dist=None, sampler=None, timed_steps=3):
     import torch
-    from spectral_rs_b200 import Batch, Sim
-    members = ensemble_members(args.ensemble)
-    cfgs = [ensemble_config(m) for m in members]
-    b = Batch(cfgs)
-    for k, (sim, m) in enumerate(zip(b.sims, members)):
-        x0, x1 = 8, m["size_x"] - 8
-        sim.init_species(1.0, m["mass_ratio"], 0.1, m["ppc"], x0, x1, m["gamma"], 1.0, True, 2 * k + 1)
-        sim.init_species(-1.0, 1.0, 0.1, m["ppc"], x0, x1, m["gamma"], 1.0, True, 2 * k + 2)
+    b = _build_batch(members, idx)
     n_particles = sum(len(p) for s in b.sims for p in s.prtls)
+    cells = sum(members[i]["size_x"] * members[i]["size_y"] for i in idx)
     b.prepare()
-    b.step(args.warmup)
+    b.step(warmup)
     stream = torch.cuda.ExternalStream(b.stream())
+    _barrier(dist)
     torch.cuda.synchronize()
-    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
-    sampler.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    b.step(args.steps)
+    if sampler:
+        sampler.start()
+    e0, e1 = _events(stream)
+    b.step(steps)
     e1.record(stream)
     e1.synchronize()
-    clocks = sampler.stop()
+    clocks = sampler.stop() if sampler else None
     ms = e0.elapsed_time(e1)
     launches = b.last_launch_count()
     b.set_timing(True)
-    b.step(3)
-    part_ms, step_ms = (float(x) / 3 for x in b.timing())
+    b.step(timed_steps)
+    part_ms, step_ms = (float(x) / timed_steps for x in b.timing())
     b.close()
-    value = n_particles * args.steps / (ms / 1e3)
-    # the plain single-simulation FP32 path on the same members, one after the other
-    plain_ms = 0.0
-    if not args.no_plain:
-        for k, (cfg, m) in enumerate(zip(cfgs, members)):
-            s = Sim(cfg, path="plain")
-            x0, x1 = 8, m["size_x"] - 8
-            s.init_species(1.0, m["mass_ratio"], 0.1, m["ppc"], x0, x1, m["gamma"], 1.0, True, 2 * k + 1)
-            s.init_species(-1.0, 1.0, 0.1, m["ppc"], x0, x1, m["gamma"], 1.0, True, 2 * k + 2)
-            s.prepare()
-            s.step(1)
-            st = torch.cuda.ExternalStream(s.stream())
-            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a0.record(st)
-            s.step(args.plain_steps)
-            a1.record(st)
-            a1.synchronize()
-            plain_ms += a0.elapsed_time(a1) / args.plain_steps
-            s.close()
-    line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded device init)",
-            "config": {"workload": f"ensemble_{args.ensemble}_shocks", "seed": ENSEMBLE_SEED,
-                       "particles": n_particles, "grids": [[m["size_x"], m["size_y"]] for m in members],
-                       "path": "split, batched (persistent work-queue particle kernel, one graph per step)"},
-            "phase_ms_per_step": {"particles": part_ms, "step": step_ms}, "gpu_launches": launches,
-            "clocks": clocks}
-    if plain_ms:
-        line["plain_fp32"] = {"value": n_particles / (plain_ms / 1e3), "unit": "particle-steps/s",
-                              "ms_per_step": plain_ms, "path": "plain FP32, one simulation after another"}
-        line["split_vs_plain"] = value / line["plain_fp32"]["value"]
-    print(json.dumps(line), flush=True)
+    return {"particles": n_particles, "cells": cells, "ms": ms, "launches": launches, "clocks": clocks,
+            "phase_ms_per_step": {"particles": part_ms, "step": step_ms},
+            "roofline": roofline(n_particles, cells, part_ms,
+                                 "k_slot_batch<push,move> (persistent fused push + move + deposit over all members)",
+                                 "k_slot_batch_traffic.json")}
+
+
+def plain_ensemble(members, idx, steps):
+    """The plain single-simulation FP32 path on the same members, one after another."""
+    import torch
+    from spectral_rs_b200 import Sim
+    total_ms, n = 0.0, 0
+    for i in idx:
+        m = members[i]
+        s = Sim(ensemble_config(m), path="plain")
+        for k, (q, mass, vth, ppc, g) in enumerate(member_species(m)):
+            s.init_species(q, mass, vth, ppc, 8, m["size_x"] - 8, g, 1.0, True, 2 * i + k + 1)
+        n += sum(len(p) for p in s.prtls)
+        s.prepare()
+        s.step(1)
+        st = torch.cuda.ExternalStream(s.stream())
+        a0, a1 = _events(st)
+        s.step(steps)
+        a1.record(st)
+        a1.synchronize()
+        total_ms += a0.elapsed_time(a1) / steps
+        s.close()
+    return {"value": n / (total_ms / 1e3), "unit": "particle-steps/s", "ms_per_step": total_ms, "steps": steps,
+            "path": "plain FP32 (global x = ix + dx, per-phase kernels, global atomics), one simulation after another"}
+
+
+def e2e_ensemble(members, idx, steps):
+    """The same metric through the public API (spx_batch_*) from pinned host buffers:
+    upload both species of every member (spx_add_species), spx_batch_prepare, `steps`
+    batch steps, read 10 fields of every member (into pinned host buffers) and each
+    member's diagnostics back."""
+    import torch
+    from spectral_rs_b200 import Batch
+    arrays = [member_arrays(members[i], 9000 + i) for i in idx]
+    n = sum(len(a["ix"]) for sp in arrays for (_, _, _, a) in sp)
+    # page-locked host copies of every array (two large allocations, sliced per species)
+    pin_i = torch.empty(2 * n, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+    pin_f = torch.empty(6 * n, dtype=torch.float32, pin_memory=True).numpy()
+    host, oi, of = [], 0, 0
+    for sp in arrays:
+        hs = []
+        for q, mass, vth, a in sp:
+            k = len(a["ix"])
+            h = {}
+            for name in ("ix", "iy"):
+                h[name] = pin_i[oi:oi + k]
+                h[name][:] = a[name]
+                oi += k
+            for name in ("dx", "dy", "px", "py", "pz", "psa"):
+                h[name] = pin_f[of:of + k]
+                h[name][:] = a[name]
+                of += k
+            hs.append((q, mass, vth, h))
+        host.append(hs)
+    del arrays
+    names = ("Jx", "Jy", "Jz", "Ex", "Ey", "Ez", "Bx", "By", "Bz", "Dens")
+    cells = sum(members[i]["size_x"] * members[i]["size_y"] for i in idx)
+    pin_o = torch.empty(len(names) * cells, dtype=torch.float32, pin_memory=True).numpy()
+    b = Batch([ensemble_config(members[i]) for i in idx])
+    t0 = time.perf_counter()
+    for sim, hs in zip(b.sims, host):
+        for q, mass, vth, h in hs:
+            sim.add_species(q, mass, vth, h["ix"], h["iy"], h["dx"], h["dy"], h["px"], h["py"], h["pz"], h["psa"])
+    t1 = time.perf_counter()
+    b.prepare()
+    t2 = time.perf_counter()
+    b.step(steps)
+    t3 = time.perf_counter()
+    off, diags = 0, []
+    for sim in b.sims:
+        c = sim.size_x * sim.size_y
+        for name in names:
+            sim.flds.spatial(name, with_ghosts=False, out=pin_o[off:off + c].reshape(sim.size_y, sim.size_x))
+            off += c
+        diags.append(sim.diag())
+    dt = time.perf_counter() - t0
+    b.close()
+    h2d = 40 * n  # ix, iy (8 B each), dx, dy, px, py, pz, psa (4 B each) per particle
+    d2h = 4 * off + sum(d.nbytes for d in diags)
+    return {"value": n * steps / dt, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d / steps,
+            "d2h_bytes_per_step": d2h / steps, "wall_s": dt,
+            "split_s": {"upload": t1 - t0, "prepare": t2 - t1, "steps": t3 - t2, "readback": t0 + dt - t3},
+            "scope": "pinned host arrays -> spx_add_species (2 per member) -> spx_batch_prepare -> "
+                     "spx_batch_step(K) -> 10 fields per member (into pinned host buffers) + spx_diag per member"}
+
+
+def run_ensemble(args):
+    rank, world, local, dist = _init_ranks()
+    per = args.ensemble
+    members = ensemble_members(per * world)
+    idx = rank_members(per, rank, world)
+    e2e = e2e_ensemble(members, idx, args.steps) if rank == 0 and not args.no_e2e else None
+    if e2e is not None:
+        e2e["ranks_measured"] = 1
+    r = measure_ensemble(members, idx, args.steps, args.warmup, dist, ClockSampler(local))
+    ms = max_over_ranks(r["ms"], device="cuda") if dist else r["ms"]
+    value = r["particles"] * args.steps * world / (ms / 1e3)  # every rank holds the same number of members
+    plain = plain_ensemble(members, idx, args.plain_steps) if rank == 0 and not args.no_plain else None
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, cores, sample, _ = oracle_ensemble_rate(members[:per], args.cpu_seconds)
+        cpu = {"value": rate, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+               "sample": sample + " (C++ restatement of the reference CPU path, OpenMP push/FFT, serial deposit)"}
+    extras = {}
+    if rank == 0 and not args.no_extras:
+        for key, wname in (("thermal_c2", "thermal"), ("weibel_c5", "weibel")):
+            w = WORKLOADS[wname]
+            x = measure_single(w, args.extra_steps, 3, args.seed)
+            extras[key] = {"workload": w["name"], "particles": x["particles"], "value": x["value"],
+                           "unit": "particle-steps/s", "steps": args.extra_steps, "ms_per_step": x["ms_per_step"],
+                           "phase_ms_per_step": x["phase_ms_per_step"], "roofline": x["roofline"],
+                           "gpu_launches": x["launches"]}
+    if rank == 0:
+        line = _line(args, world, value, ms, f"ensemble_{per}_shocks", r["launches"], r["clocks"])
+        line["config"].update({"seed": ENSEMBLE_SEED, "members_per_gpu": per, "particles_per_gpu": r["particles"],
+                               "cells_per_gpu": r["cells"],
+                               "grids": [[members[i]["size_x"], members[i]["size_y"]] for i in idx],
+                               "ppc": [members[i]["ppc"] for i in idx],
+                               "mass_ratio": [members[i]["mass_ratio"] for i in idx],
+                               "drift_beta": [round(members[i]["beta"], 4) for i in idx],
+                               "vth": 0.1, "c": 3.0, "dt": 0.1, "n_pass": 4, "delta": 8, "walls": "right + left",
+                               "path": "split, batched (persistent work-queue particle kernel, one graph per step)",
+                               "parallelism": f"member list partitioned over {world} ranks" if world > 1 else "single",
+                               "l2": _l2_note(r["particles"])})
+        line.update({"roofline": r["roofline"], "phase_ms_per_step": r["phase_ms_per_step"], "plain_fp32": plain,
+                     "cpu_baseline": cpu, "e2e": e2e})
+        if plain:
+            line["split_vs_plain"] = value / world / plain["value"]
+        line.update(extras)
+        print(json.dumps(line), flush=True)
+    _finish(dist)
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--extra-steps", type=int, default=10, help="timed steps of the C2 / C5 extra keys")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--small", action="store_true", help="1/16 of the workload (quick checks)")
-    ap.add_argument("--workload", default="thermal", choices=sorted(WORKLOADS) + ["ensemble"])
+    ap.add_argument("--no-extras", action="store_true", help="ensemble: skip the C2 / C5 keys")
+    ap.add_argument("--small", action="store_true", help="single workloads: 1/16 of the grid (quick checks)")
+    ap.add_argument("--workload", default="ensemble", choices=sorted(WORKLOADS) + ["ensemble"])
     ap.add_argument("--tile", default=None, help="split-path tile shape TXxTY (default: the library's choice)")
     ap.add_argument("--compensated", action="store_true", help="Kahan-compensated current sums (split path)")
     ap.add_argument("--ppc", type=int, default=None,
                     help="particles per cell of every species (field-phase profiling on the full grid)")
-    ap.add_argument("--ensemble", type=int, default=64, help="members of the batched ensemble")
+    ap.add_argument("--ensemble", type=int, default=ENSEMBLE_PER_RANK, help="members of the ensemble per GPU")
     args = ap.parse_args()
     if args.workload == "ensemble":
-        run_ensemble(args)
+        if args.impl == "reference":
+            run_reference(args, None)
+        else:
+            run_ensemble(args)
         return
     w = dict(WORKLOADS[args.workload])
     if args.small:
@@ -534,7 +764,7 @@ def main():
     if args.impl == "reference":
         run_reference(args, w)
     else:
-        run_gpu(args, w)
+        run_single(args, w)
 
 
 if __name__ == "__main__":

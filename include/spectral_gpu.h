@@ -234,16 +234,21 @@ SPX_API uint64_t spx_batch_last_launch_count(const spx_batch* batch);
  * forbids allocation once the run has started.  It has no counterpart in the
  * reference; it computes what spx_field_op(op = 2) computes (n_pass passes of
  * Field::binomial_filter_2_d) on device buffers the caller owns.
- *   d_in, d_out: device pointers to (size_y+2)*(size_x+2) floats (d_in == d_out
- *   is allowed); stream: a cudaStream_t (NULL = default stream).
+ *   d_in, d_out: device pointers to (size_y+2)*(size_x+2) floats.  They must be
+ *   the same buffer (in place) or not overlap at all: the passes read a 3x3
+ *   neighbourhood while writing, so partly overlapping buffers are rejected
+ *   with SPX_ERR_ARG.  stream: a cudaStream_t (NULL = default stream).
  * The ping-pong scratch is a fixed device array of SPX_NOALLOC_MAX_CELLS floats
  * (16 MiB) that every GPU loading the library holds until exit; grids with
- * (size_x+2)*(size_y+2) above that are rejected with SPX_ERR_ARG.  The first
- * call on a device looks the array's address up (cudaGetSymbolAddress), so make
- * it before any stream capture.  All calls share the one array: calls that
- * overlap on the GPU race, so order them on one stream.  The scratch is fully
- * overwritten by every pass; nothing in it needs clearing.  The message of a
- * failed call is returned by spx_noalloc_last_error(). */
+ * (size_x+2)*(size_y+2) above that, or either side above SPX_NOALLOC_MAX_CELLS,
+ * are rejected with SPX_ERR_ARG before any CUDA call.  The first call on a
+ * device looks the array's address up (cudaGetSymbolAddress), so make it before
+ * any stream capture.  All calls share the one array: calls that overlap on the
+ * GPU race, so order them on one stream.  The scratch is fully overwritten by
+ * every pass; nothing in it needs clearing.  Each launch's own status is
+ * checked; an earlier, unrelated error of the caller's is neither reported nor
+ * cleared.  spx_noalloc_last_error() returns the message of the calling host
+ * thread's last failed call (one message per thread). */
 #define SPX_NOALLOC_MAX_CELLS (4u * 1024u * 1024u)
 SPX_API int spx_filter_noalloc(uint64_t size_x, uint64_t size_y, uint32_t n_pass, const float* d_in, float* d_out,
                                void* stream);

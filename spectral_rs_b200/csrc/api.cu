@@ -123,7 +123,8 @@ struct spx_ctx {
   float last_timing[4] = {0, 0, 0, 0};
   uint64_t last_launches = 0;
   uint64_t repacks = 0, last_overflow = 0, last_max_occ = 0;
-  UploadRing up;  // spx_add_species scratch
+  UploadRing own_up;         // spx_add_species scratch of a standalone context
+  UploadRing* up = &own_up;  // the ring in use: a batch lends its one ring to every member
 };
 
 static std::string g_create_err;
@@ -258,7 +259,7 @@ extern "C" int spx_destroy(spx_ctx* c) {
       if (p) cudaFree(p);
   }
   c->fb.release();
-  c->up.release();
+  c->own_up.release();
   for (void* p : {(void*)c->d_err, (void*)c->d_diag, (void*)c->d_u32, (void*)c->d_counts})
     if (p) cudaFree(p);
   for (auto e : c->ev) cudaEventDestroy(e);
@@ -395,7 +396,7 @@ extern "C" int spx_add_species(spx_ctx* c, float charge, float mass, float vth, 
     s.beta = (charge / mass) * 0.5f * c->prm.dt;
     s.alpha = (charge / mass) * 0.5f * c->prm.dt / c->prm.c;
     s.n = n;
-    UploadRing& up = c->up;
+    UploadRing& up = *c->up;
     up.reserve(n);
     uint32_t* const cell = up.cell;
     // pass 1: cell indices checked and packed on the device, occupancy per cell
@@ -517,7 +518,7 @@ extern "C" int spx_init_species(spx_ctx* c, float charge, float mass, float vth,
     // generated chunk by chunk into the upload ring and placed at once: every
     // cell of columns [x0, x1) holds exactly ppc particles, so the slot capacity
     // is known before the first particle exists
-    UploadRing& up = c->up;
+    UploadRing& up = *c->up;
     up.reserve(n, false, 1);
     if (c->plain) {
       for (float** p : {&s.plain.x, &s.plain.y, &s.plain.px, &s.plain.py, &s.plain.pz})
@@ -1124,6 +1125,7 @@ struct spx_batch {
   cudaEvent_t ev_fork = nullptr;
   std::vector<cudaEvent_t> ev_join;
   SlotBatch sb;
+  UploadRing up;  // one upload ring lent to every member (they add species one after another)
   bool built = false;
   std::map<uint32_t, StepGraph> graphs;
   std::string err;
@@ -1168,6 +1170,7 @@ extern "C" int spx_batch_create(int32_t n, const spx_params* params, spx_batch**
       int rc = spx_create(&p, &c);
       if (rc) throw spx::Error(rc, std::string("simulation ") + std::to_string(i) + ": " + g_create_err);
       c->use_graphs = false;  // members advance through the batch's own graphs
+      c->up = &b->up;
       b->sims.push_back(c);
       if (c->pg.TX != b->sims[0]->pg.TX || c->pg.TY != b->sims[0]->pg.TY)
         throw spx::Error(SPX_ERR_ARG, "all simulations of a batch need the same tile shape");
@@ -1193,6 +1196,7 @@ extern "C" int spx_batch_destroy(spx_batch* b) {
   for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second.exec);
   b->sb.release();
   for (spx_ctx* c : b->sims) spx_destroy(c);
+  b->up.release();
   if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   for (auto e : b->ev_join) cudaEventDestroy(e);
   for (auto e : {b->t0, b->t1, b->t2})
@@ -1217,8 +1221,8 @@ extern "C" int spx_batch_prepare(spx_batch* b) {
     spx_ctx* c = b->sims[i];
     if (c->species.empty()) return bfail(b, SPX_ERR_STATE, "simulation " + std::to_string(i) + " has no species");
     if (int rc = spx_prepare(c)) return bfail(b, rc, "simulation " + std::to_string(i) + ": " + c->err);
-    c->up.release();  // a batch holds many contexts: no upload scratch kept per member
   }
+  b->up.release();  // the members' shared upload scratch is not kept once they are set up
   try {
     b->sb.release();
     slot_batch_build(b->sb, batch_sims(b));

@@ -720,6 +720,18 @@ void launch_filter_pass(const Grid& g, float* const* src, float* const* dst, int
   k_filter<<<grd, blk, 0, st>>>(S, D, g);
 }
 
+cudaError_t launch_filter_pass_status(const Grid& g, const float* src, float* dst, cudaStream_t st) {
+  ConstFieldList S{};
+  FieldList D{};
+  S.f[0] = src;
+  D.f[0] = dst;
+  Grid gg = g;
+  void* args[] = {&S, &D, &gg};
+  const dim3 blk(64, 4);
+  const dim3 grd((g.nx + 2 + 63) / 64, (g.ny + 2 + 3) / 4, 1);
+  return cudaLaunchKernel((const void*)k_filter, grd, blk, args, 0, st);
+}
+
 // Dynamic shared memory above 48 KB must be opted into once per kernel (on
 // every device that runs it; done when a context is created, never while a
 // stream is being captured).

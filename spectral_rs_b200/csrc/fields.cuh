@@ -35,6 +35,9 @@ void launch_fold(const Grid& g, float* const* fields, int nf, cudaStream_t st);
 void launch_update_ghosts(const Grid& g, float* const* fields, int nf, cudaStream_t st);
 // One binomial_filter_2_d pass (src/flds/field.rs:376-426) from src[f] into dst[f].
 void launch_filter_pass(const Grid& g, float* const* src, float* const* dst, int nf, cudaStream_t st);
+// The same for one field through cudaLaunchKernel: returns that launch's own
+// status and leaves any earlier error of the caller's untouched.
+cudaError_t launch_filter_pass_status(const Grid& g, const float* src, float* dst, cudaStream_t st);
 // n_pass binomial_filter_2_d passes in one kernel, from src[f] into the
 // interior of dst[f] (ghosts untouched); usable when filter_fused_fits(n_pass).
 bool filter_fused_fits(uint32_t npass);

@@ -99,6 +99,36 @@ __device__ __forceinline__ void tsc_weights_x2(float dx, float dy, float (&w)[9]
   w[8] = r2.y;
 }
 
+// TSC weights are quadratics of the offset d (src/lib.rs:339-347):
+//   W0 = 0.5 (0.5 - d)^2 = 1/8 - d/2 + d^2/2,  W1 = 3/4 - d^2,  W2 = 1/8 + d/2 + d^2/2,
+// so the stencil a cell's particles deposit, S[a][b] = sum_p v_p W_a(dy_p) W_b(dx_p),
+// is fixed by the nine moments M[i][j] = sum_p v_p dy_p^i dx_p^j (i, j = 0..2):
+// S[a][b] = sum_ij P[a][i] P[b][j] M[i][j].  A particle then adds to nine
+// moments instead of evaluating nine weights, and the stencil is formed once per
+// cell.  (Deposit sums are not in the reference's order anyway, so only their
+// rounding changes: a few ulps of the cell's total.)
+__device__ __forceinline__ float tsc_poly(int a, int i) {
+  // rows: W0, W1, W2; columns: coefficient of d^0, d^1, d^2
+  return a == 1 ? (i == 0 ? 0.75f : i == 1 ? 0.f : -1.f) : (i == 0 ? 0.125f : i == 2 ? 0.5f : (a == 0 ? -0.5f : 0.5f));
+}
+// m[i*3 + j] (dy power i, dx power j) -> s[a*3 + b] (stencil row a = y offset, column b = x offset)
+__device__ __forceinline__ void moments_to_stencil(const float (&m)[9], float (&s)[9]) {
+  // the zero coefficient of W1 is skipped (indices are compile-time after unrolling)
+  auto dot3 = [](int row, float x0, float x1, float x2) {
+    float r = tsc_poly(row, 0) * x0 + tsc_poly(row, 2) * x2;
+    return row == 1 ? r : r + tsc_poly(row, 1) * x1;
+  };
+  float n[9];  // n[i*3 + b] = sum_j P[b][j] m[i*3 + j]
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) n[i * 3 + b] = dot3(b, m[i * 3], m[i * 3 + 1], m[i * 3 + 2]);
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) s[a * 3 + b] = dot3(a, n[b], n[3 + b], n[6 + b]);
+}
+
 // Boris push of src/prtls.rs:412-440 given the gathered fields g[0..5] = E, B.
 // Every operation is the reference's, in its order (Rust evaluates a + b * c - d * e
 // as (a + (b*c)) - (d*e)); independent multiplications run in pairs as packed
@@ -484,9 +514,11 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
     const int KL = S.KL, rin = S.rin;
     int kept = 0;  // particles kept so far (moving steps): the next low-range slot
     const float q = S.charge, beta = S.beta, alpha = S.alpha;
-    float accD[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) accD[k] = 0.f;
+    // density moments of the particles that stay (the count is `kept`):
+    // rm1 = (sum dx, sum dy), rm2 = (sum dx^2, sum dy^2), rm11 = sum dx dy,
+    // rm12 = (sum dy dx^2, sum dx dy^2), rm22 = sum dx^2 dy^2
+    float2 rm1 = make_float2(0.f, 0.f), rm2 = make_float2(0.f, 0.f), rm12 = make_float2(0.f, 0.f);
+    float rm11 = 0.f, rm22 = 0.f;
     int nq_j = 0, nq_m = 0;  // warp-uniform queue sizes
 
     auto slot_of = [&](int r, bool& act) -> int {
@@ -586,14 +618,39 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
           }
           vz = q * pz * inv;
           jcross = ix != ox || iy != oy;
-          if (!jcross) {
+          if (!jcross && !COMP) {
+            // moments sum v dy^i dx^j, i, j = 0..2 (see moments_to_stencil); fused
+            // multiply-adds: the deposit sums are not the reference's order anyway
+            const float2 vxy = make_float2(vx, vy);
+            const float2 a1 = mul2(vxy, bc2(dx));  // v dx
+            const float2 a2 = mul2(a1, bc2(dx));   // v dx^2
+            const float z1 = vz * dx, z2 = z1 * dx;
+            const float dy2 = dy * dy;
+            accJxy[0] = add2(accJxy[0], vxy);
+            accJxy[1] = add2(accJxy[1], a1);
+            accJxy[2] = add2(accJxy[2], a2);
+            accJxy[3] = fma2(bc2(dy), vxy, accJxy[3]);
+            accJxy[4] = fma2(bc2(dy), a1, accJxy[4]);
+            accJxy[5] = fma2(bc2(dy), a2, accJxy[5]);
+            accJxy[6] = fma2(bc2(dy2), vxy, accJxy[6]);
+            accJxy[7] = fma2(bc2(dy2), a1, accJxy[7]);
+            accJxy[8] = fma2(bc2(dy2), a2, accJxy[8]);
+            accJz[0] += vz;
+            accJz[1] += z1;
+            accJz[2] += z2;
+            accJz[3] = __fmaf_rn(dy, vz, accJz[3]);
+            accJz[4] = __fmaf_rn(dy, z1, accJz[4]);
+            accJz[5] = __fmaf_rn(dy, z2, accJz[5]);
+            accJz[6] = __fmaf_rn(dy2, vz, accJz[6]);
+            accJz[7] = __fmaf_rn(dy2, z1, accJz[7]);
+            accJz[8] = __fmaf_rn(dy2, z2, accJz[8]);
+          } else if (!jcross) {
             float w[9];
             tsc_weights_x2(dx, dy, w);
-            // summation order of deposits is not the reference's anyway: fused multiply-add here
             const float2 vxy = make_float2(vx, vy);
 #pragma unroll
             for (int k = 0; k < 9; ++k) {
-              if (COMP) {  // Kahan summation: y = w v - comp; t = acc + y; comp = (t - acc) - y
+              {  // Kahan summation: y = w v - comp; t = acc + y; comp = (t - acc) - y
                 const float2 y = fma2(bc2(w[k]), vxy, make_float2(-cmpJxy[k].x, -cmpJxy[k].y));
                 const float2 t = add2(accJxy[k], y);
                 cmpJxy[k] = sub2(sub2(t, accJxy[k]), y);
@@ -602,9 +659,6 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
                 const float tz = __fadd_rn(accJz[k], yz);
                 cmpJz[k] = __fsub_rn(__fsub_rn(tz, accJz[k]), yz);
                 accJz[k] = tz;
-              } else {
-                accJxy[k] = fma2(bc2(w[k]), vxy, accJxy[k]);
-                accJz[k] = __fmaf_rn(w[k], vz, accJz[k]);
               }
             }
           } else {
@@ -620,10 +674,14 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
           // cell's arrivals like a mover
           mover = ix != ox || iy != oy || kept >= KL;
           if (!mover) {
-            float w[9];
-            tsc_weights_x2(dx, dy, w);
-#pragma unroll
-            for (int k = 0; k < 9; ++k) accD[k] += w[k];
+            // density moments (the count is `kept`): sum dx, dy, dx^2, dy^2, dx dy, dy dx^2, dx dy^2, dx^2 dy^2
+            const float2 dd = make_float2(dx, dy);
+            const float2 sq = mul2(dd, dd);
+            rm1 = add2(rm1, dd);
+            rm2 = add2(rm2, sq);
+            rm11 = __fmaf_rn(dx, dy, rm11);
+            rm12 = fma2(make_float2(dy, dx), sq, rm12);
+            rm22 = __fmaf_rn(sq.x, sq.y, rm22);
             const int o = kept * TC + c;
             sdx[o] = dx;
             sdy[o] = dy;
@@ -675,20 +733,39 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
       S.nlow[gc] = (uint32_t)kept;
       S.ain[gc] = 0u;
       // this species' density stencil of the owner cell -> window
-      const int bl = (oy - 1 - wy0) * WX + (ox - 1 - wx0);
+      if (kept > 0) {
+        const float m[9] = {(float)kept, rm1.x, rm2.x, rm1.y, rm11, rm12.x, rm2.y, rm12.y, rm22};
+        float d[9];
+        moments_to_stencil(m, d);
+        const int bl = (oy - 1 - wy0) * WX + (ox - 1 - wx0);
 #pragma unroll
-      for (int r = 0; r < 3; ++r)
+        for (int r = 0; r < 3; ++r)
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          const float d = accD[r * 3 + k];
-          if (d != 0.f) {
-            atomicAdd(wrho + bl + r * WX + k, d * q);
-            atomicAdd(wdens + bl + r * WX + k, d);
+          for (int k = 0; k < 3; ++k) {
+            atomicAdd(wrho + bl + r * WX + k, d[r * 3 + k] * q);
+            atomicAdd(wdens + bl + r * WX + k, d[r * 3 + k]);
           }
-        }
+      }
     }
   }
   if (!MOVE) return;
+  if (!COMP) {  // the current moments -> stencils (accumulated in place)
+    float mx[9], my[9], mz[9], sx[9], sy[9], sz[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      mx[k] = accJxy[k].x;
+      my[k] = accJxy[k].y;
+      mz[k] = accJz[k];
+    }
+    moments_to_stencil(mx, sx);
+    moments_to_stencil(my, sy);
+    moments_to_stencil(mz, sz);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      accJxy[k] = make_float2(sx[k], sy[k]);
+      accJz[k] = sz[k];
+    }
+  }
   {
     const int bl = (oy - 1 - wy0) * WX + (ox - 1 - wx0);
 #pragma unroll

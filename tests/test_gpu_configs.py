@@ -1,0 +1,270 @@
+"""Full-loop parity at the benchmark configurations (src/lib.rs:130-200 of the reference).
+
+Each test runs the production path (spx_prepare + graph-launched spx_step) from
+seeded host arrays that the CPU oracle also receives, and compares with the
+oracle's FP32 path (the reference's default build) and FP64 path (its dprec
+build):
+
+  C2 crop   thermal electron-proton plasma, 1024 x 256, mass ratio 64, 64 per
+            cell per species (33,554,432 particles), 50 steps, live oracles.
+  C1        the unmagnetized shock at its own size (512 x 64, wall, 1000 steps)
+            against the committed oracle energy histories, then one more
+            move_and_deposit from the run's final state, bit-exact with the
+            oracle (the reflecting wall on a compressed shock).
+  C5        the Weibel configuration on its 1024 x 256 sub-run: magnetic-energy
+            growth rate and saturation against the committed FP64 history.
+  C4        two members of the 64-member shock ensemble (one 1024 x 256, one
+            128 x 128) stepped inside the batch, against live oracles.
+
+Tolerances (fields are compared against FP64, scaled by the field's max |value|):
+  - GPU field error <= 10x the FP32 oracle's own error (floor 1e-5);
+  - cell-index mismatch against the FP32 oracle <= 1e-4 of the particles;
+  - momenta within 1e-3 of max |p| of the FP32 oracle;
+  - energy histories: see each test.
+The oracles run in threads while the GPU steps (ctypes releases the GIL).
+"""
+import json
+import os
+import sys
+import threading
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+
+FIELDS = ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Jx", "Jy", "Jz", "Dens")
+HIST = os.path.join(ROOT, "tests", "golden", "config_histories.json")
+
+
+def _cfg(p, steps=0):
+    from spectral_rs_b200.config import Config, Setup, Output
+    return Config(p, Setup(steps), Output(False, False, 1, 1, 1, 1))
+
+
+class OracleRun(threading.Thread):
+    """An oracle run of `steps` loop iterations in a background thread."""
+
+    def __init__(self, p, species, dtype, steps):
+        super().__init__(daemon=True)
+        self.p, self.species, self.dtype, self.steps = p, species, dtype, steps
+        self.o, self.err = None, None
+
+    def run(self):
+        try:
+            o = orc.OracleSim.from_params(self.p, dtype=self.dtype)
+            for q, m, vth, a in self.species:
+                o.add_species(q, m, vth, a["ix"], a["iy"], a["dx"], a["dy"], a["px"], a["py"], a["pz"], a["psa"])
+            o.prepare()
+            o.step(self.steps)
+            self.o = o
+        except Exception as e:  # surfaced by result()
+            self.err = e
+
+    def result(self):
+        self.join()
+        if self.err:
+            raise self.err
+        return self.o
+
+
+def _add(sim, species):
+    for q, m, vth, a in species:
+        sim.add_species(q, m, vth, a["ix"], a["iy"], a["dx"], a["dy"], a["px"], a["py"], a["pz"], a["psa"])
+
+
+def _compare(tag, get_gpu, o32, o64, prtls=None):
+    """Fields against FP64 (within 10x the FP32 oracle's error), particles against FP32."""
+    report = {}
+    for name in FIELDS:
+        g, r = get_gpu(name).astype(np.float64), o64.spatial(name)
+        r32 = o32.spatial(name).astype(np.float64)
+        scale = max(np.max(np.abs(r)), 1e-30)
+        err_gpu, err_ref = np.max(np.abs(g - r)) / scale, np.max(np.abs(r32 - r)) / scale
+        report[name] = (err_gpu, err_ref)
+    print(f"\n[{tag}] field error vs fp64 (gpu, oracle fp32): " +
+          ", ".join(f"{k} {a:.1e}/{b:.1e}" for k, (a, b) in report.items()))
+    for name, (err_gpu, err_ref) in report.items():
+        assert err_gpu <= max(10 * err_ref, 1e-5), (tag, name, err_gpu, err_ref)
+    for s, pr in enumerate(prtls or []):
+        g, r = pr.state(), o32.state(s)
+        mism = np.mean((g["ix"] != r["ix"]) | (g["iy"] != r["iy"]))
+        pmax = max(float(np.max(np.abs(r[k]))) for k in ("px", "py", "pz"))
+        perr = max(float(np.max(np.abs(g[k] - r[k]))) for k in ("px", "py", "pz")) / pmax
+        print(f"[{tag}] species {s}: cell mismatch {mism:.2e}, momentum error {perr:.2e} of max |p|")
+        assert mism <= 1e-4, (tag, s, mism)
+        assert perr < 1e-3, (tag, s, perr)
+
+
+# ---------------------------------------------------------------- C2 crop
+def test_c2_thermal_crop_vs_fp32_fp64():
+    """1024 x 256 crop of the thermal plasma (the benchmark's particle load per cell), 50 steps."""
+    from spectral_rs_b200 import Sim
+    from spectral_rs_b200.config import Params, SpeciesSpec
+    from spectral_rs_b200.init import species_arrays
+    steps = 50
+    p = Params(size_x=1024, size_y=256, delta=0, dt=0.1, c=3.0, dens=64, gamma_inj=1.000001, n_pass=4,
+               mass_ratio=64.0, vth=0.05, periodic_x=True, random_positions=True, seed=2024)
+    species = []
+    for k, (q, m) in enumerate(((1.0, 64.0), (-1.0, 1.0))):  # ions first, as run() creates them
+        a = species_arrays(p, SpeciesSpec(q, m, 0.05, 64, 0.0), seed_offset=k)
+        species.append((q, m, 0.05, a))
+    runs = [OracleRun(p, species, dt, steps) for dt in (np.float32, np.float64)]
+    for r in runs:
+        r.start()
+    with Sim(_cfg(p, steps)) as sim:
+        _add(sim, species)
+        sim.prepare()
+        sim.step(steps)
+        o32, o64 = (r.result() for r in runs)
+        _compare("C2 crop", sim.flds.spatial, o32, o64, sim.prtls)
+
+
+# ---------------------------------------------------------------- C1 shock
+@pytest.fixture(scope="module")
+def histories():
+    with open(HIST) as f:
+        return json.load(f)
+
+
+def _energies(sim):
+    d = sim.diag()
+    return float(d[0]), float(d[1])
+
+
+def test_c1_shock_1000_steps(histories):
+    """The shock at its own size for 1000 steps: field-energy history against the oracle,
+    then the wall (src/prtls.rs:124-190) on the compressed final state, bit-exact."""
+    import make_config_histories as mch
+    from spectral_rs_b200 import Sim
+    h = histories["shock"]
+    cfg = h["config"]
+    p = mch.params_of(cfg)
+    species = mch.species_of(cfg)
+    hist = []
+    with Sim(_cfg(p, cfg["steps"])) as sim:
+        _add(sim, species)
+        sim.prepare()
+        for _ in range(0, cfg["steps"], cfg["every"]):
+            sim.step(cfg["every"])  # raises SpxError on a wall assertion (SPX_ERR_WALL)
+            hist.append(_energies(sim))
+        e_gpu, b_gpu = np.array([x[0] for x in hist]), np.array([x[1] for x in hist])
+        e64, e32 = np.array(h["fp64"]["E"]), np.array(h["fp32"]["E"])
+        b64, b32 = np.array(h["fp64"]["B"]), np.array(h["fp32"]["B"])
+        rel = np.abs(e_gpu - e64) / e64
+        rel32 = np.abs(e32 - e64) / e64
+        print(f"\n[C1] field energy vs fp64: median {np.median(rel):.2e} (oracle fp32 {np.median(rel32):.2e}), "
+              f"first 100 steps max {np.max(rel[:10]):.2e} (oracle fp32 {np.max(rel32[:10]):.2e}), "
+              f"step 1000 {rel[-1]:.2e} (oracle fp32 {rel32[-1]:.2e})")
+        # early steps track FP64 as closely as the reference's FP32 path does
+        assert np.max(rel[:10]) <= max(10 * np.max(rel32[:10]), 1e-5)
+        assert np.median(rel) <= max(10 * np.median(rel32), 1e-3)
+        # over the run (the shock's particle noise decorrelates FP32 runs): energies agree statistically
+        assert abs(np.mean(e_gpu) - np.mean(e64)) < 0.05 * np.mean(e64)
+        assert abs(np.mean(b_gpu) - np.mean(b64)) < 0.1 * np.mean(b64) + 1e-12
+        # the wall on the final state: one move_and_deposit on both sides from the same particles
+        states = [pr.state() for pr in sim.prtls]
+        o = orc.OracleSim.from_params(p, dtype=np.float32)
+        for (q, m, vth, _), st in zip(species, states):
+            o.add_species(q, m, vth, st["ix"], st["iy"], st["dx"], st["dy"], st["px"], st["py"], st["pz"], st["psa"])
+        wall = p.size_x + 1 - p.delta
+        for s, pr in enumerate(sim.prtls):
+            near = np.mean(states[s]["ix"] >= wall - 1)
+            sim.move_and_deposit(pr)
+            o.move_and_deposit(s)
+            g, r = pr.state(), o.state(s)
+            for k in ("ix", "iy", "dx", "dy", "px", "py", "pz", "psa"):
+                assert np.array_equal(g[k], r[k].astype(g[k].dtype)), (s, k)
+            # the move changes no |p| component: reflections flip px only
+            for k in ("px", "py", "pz"):
+                assert np.array_equal(np.abs(g[k]), np.abs(states[s][k])), (s, k)
+            flipped = np.mean(np.sign(g["px"]) != np.sign(states[s]["px"]))
+            print(f"[C1] species {s}: {near:.2%} at the wall cells, {flipped:.3%} reflected in the extra move")
+            assert near > 0 and flipped > 0
+
+
+# ---------------------------------------------------------------- C5 Weibel sub-run
+def _growth_window(b):
+    """Exponential phase of a magnetic-energy history: from 100x its first value to 1/4 of its peak."""
+    peak = int(np.argmax(b))
+    lo = int(np.flatnonzero(b[:peak + 1] > 100 * b[0])[0])
+    hi = int(np.flatnonzero(b[:peak + 1] > 0.25 * b[peak])[0])
+    return np.arange(lo, hi + 1)
+
+
+def test_c5_weibel_growth_vs_fp64(histories):
+    """Magnetic-energy growth of the Weibel filamentation (1024 x 256 sub-run) against FP64."""
+    import make_config_histories as mch
+    from spectral_rs_b200 import Sim
+    h = histories["weibel"]
+    cfg = h["config"]
+    p = mch.params_of(cfg)
+    hist = []
+    with Sim(_cfg(p, cfg["steps"])) as sim:
+        _add(sim, mch.species_of(cfg))
+        sim.prepare()
+        for _ in range(0, cfg["steps"], cfg["every"]):
+            sim.step(cfg["every"])
+            hist.append(_energies(sim))
+    b_gpu = np.array([x[1] for x in hist])
+    b64, b32 = np.array(h["fp64"]["B"]), np.array(h["fp32"]["B"])
+    t = (np.arange(len(b64)) + 1) * cfg["every"] * cfg["dt"]
+    win = _growth_window(b64)
+    assert len(win) >= 5, "no exponential phase in the FP64 history"
+    rate = {k: np.polyfit(t[win], np.log(v[win]), 1)[0] / 2 for k, v in (("fp64", b64), ("fp32", b32),
+                                                                          ("gpu", b_gpu))}
+    sat = {k: float(np.max(v)) for k, v in (("fp64", b64), ("fp32", b32), ("gpu", b_gpu))}
+    rel = np.abs(b_gpu - b64) / b64
+    rel32 = np.abs(b32 - b64) / b64
+    print(f"\n[C5] growth rate of |B| (1/omega_pe): fp64 {rate['fp64']:.4f}, gpu {rate['gpu']:.4f}, "
+          f"oracle fp32 {rate['fp32']:.4f}; saturation max B energy: fp64 {sat['fp64']:.4e}, gpu {sat['gpu']:.4e}, "
+          f"oracle fp32 {sat['fp32']:.4e}; rel. error over the growth window max {np.max(rel[win]):.2e} "
+          f"(oracle fp32 {np.max(rel32[win]):.2e})")
+    assert abs(rate["gpu"] - rate["fp64"]) < 0.01 * abs(rate["fp64"])
+    assert abs(sat["gpu"] - sat["fp64"]) < 0.05 * sat["fp64"]
+    assert np.max(rel[win]) < max(10 * np.max(rel32[win]), 1e-3)
+
+
+# ---------------------------------------------------------------- C4 members inside the batch
+def test_c4_members_in_batch_vs_oracle():
+    """Members 6 (1024 x 256) and 1 (128 x 128) of the 64-member shock ensemble, stepped
+    inside the batch (one persistent particle launch over all members), against the oracle."""
+    import bench
+    from spectral_rs_b200 import Batch
+    from spectral_rs_b200.config import SpeciesSpec
+    from spectral_rs_b200.init import species_arrays
+    steps = 20
+    members = bench.ensemble_members(64)
+    cfgs = [bench.ensemble_config(m) for m in members]
+    checked = {6: None, 1: None}
+    assert (members[6]["size_x"], members[6]["size_y"]) == (1024, 256)
+    assert (members[1]["size_x"], members[1]["size_y"]) == (128, 128)
+    runs = {}
+    for i in checked:
+        m, p = members[i], cfgs[i].params
+        p.random_positions, p.seed = True, 500 + i
+        sp = []
+        for k, (q, mass) in enumerate(((1.0, m["mass_ratio"]), (-1.0, 1.0))):
+            spec = SpeciesSpec(q, mass, 0.1, m["ppc"], m["gamma"], 1.0, 8, m["size_x"] - 8)
+            sp.append((q, mass, 0.1, species_arrays(p, spec, seed_offset=k)))
+        checked[i] = sp
+        runs[i] = [OracleRun(p, sp, dt, steps) for dt in (np.float32, np.float64)]
+        for r in runs[i]:
+            r.start()
+    with Batch(cfgs) as b:
+        for k, (sim, m) in enumerate(zip(b.sims, members)):
+            if k in checked:
+                _add(sim, checked[k])
+            else:
+                x0, x1 = 8, m["size_x"] - 8
+                sim.init_species(1.0, m["mass_ratio"], 0.1, m["ppc"], x0, x1, m["gamma"], 1.0, True, 2 * k + 1)
+                sim.init_species(-1.0, 1.0, 0.1, m["ppc"], x0, x1, m["gamma"], 1.0, True, 2 * k + 2)
+        b.prepare()
+        b.step(steps)
+        for i in checked:
+            o32, o64 = (r.result() for r in runs[i])
+            _compare(f"C4 member {i}", b.sims[i].flds.spatial, o32, o64, b.sims[i].prtls)

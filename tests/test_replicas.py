@@ -1,9 +1,11 @@
 """Multi-GPU semantics of bench.py on CPU: world_size 2 gloo ranks.
 
-The workload does not shard without exchange steps, so N GPUs run N independent
-replicas (weak scaling).  What must hold across ranks: each rank gets its own
-seed, every rank takes the same collective steps, and the reported time is the
-maximum over ranks.  No GPU is touched here.
+The batched ensemble shards by member (independent simulations, no exchange):
+N ranks run 64 N members, each on exactly one rank (weak scaling).  A single
+simulation does not shard without exchange steps, so N GPUs run N independent
+replicas of it.  What must hold across ranks: each member or replica on one
+rank with its own seed, every rank takes the same collective steps, and the
+reported time is the maximum over ranks.  No GPU is touched here.
 """
 import os
 import socket
@@ -52,3 +54,45 @@ def test_reference_arm_only_rank0_prints(capsys, monkeypatch):
         steps, warmup, gpus = 1, 0, 2
     bench.run_reference(A, dict(bench.WORKLOAD))
     assert capsys.readouterr().out == ""
+
+
+def _partition_main(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import bench
+    mine = bench.rank_members(bench.ENSEMBLE_PER_RANK, rank, world)
+    everyone = [None] * world
+    dist.all_gather_object(everyone, mine)
+    ms = bench.max_over_ranks(20.0 - rank)
+    out[rank] = (everyone, ms)
+    dist.destroy_process_group()
+
+
+def test_ensemble_members_partitioned_over_ranks():
+    """The batched ensemble shards by member: with N ranks the list has 64 N members and
+    every member runs on exactly one rank; rank 0's block is the one-GPU workload."""
+    import bench
+    world = 2
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.start_processes(_partition_main, args=(world, _free_port(), out), nprocs=world, start_method="spawn")
+    assert out[0][0] == out[1][0]
+    blocks = out[0][0]
+    flat = [i for b in blocks for i in b]
+    assert sorted(flat) == list(range(bench.ENSEMBLE_PER_RANK * world))  # each member exactly once
+    assert blocks[0] == list(range(bench.ENSEMBLE_PER_RANK))
+    assert out[0][1] == out[1][1] == 20.0
+    # a longer member list extends the one-GPU list unchanged
+    short, long = bench.ensemble_members(64), bench.ensemble_members(64 * world)
+    assert all(a["size_x"] == b["size_x"] and a["ppc"] == b["ppc"] and a["beta"] == b["beta"]
+               for a, b in zip(short, long[:64]))
+
+
+def test_ensemble_cpu_sample_is_bounded():
+    import bench
+    members = bench.ensemble_members(64)
+    idx = bench.cpu_sample(members)
+    n = sum(bench.member_particles(members[i]) for i in idx)
+    assert idx == list(range(len(idx))) and n >= bench.CPU_SAMPLE_PARTICLES
+    assert n - bench.member_particles(members[idx[-1]]) < bench.CPU_SAMPLE_PARTICLES
+    assert sum(bench.member_particles(m) for m in members) == 265_764_864
