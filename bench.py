@@ -721,6 +721,66 @@ def run_ensemble(args):
     _finish(dist)
 
 
+# ---------------------------------------------------------------- precision study (two-stream)
+def two_stream_study(args):
+    """Symmetric two-stream electron beams (+-0.2c along x, thermal spread 0.01c, 32 per cell
+    per beam, immobile neutralizing ions left out: their uniform background only touches
+    k = 0, which the solver ignores) on the full 2048 x 2048 grid for 2000 steps, split,
+    compensated and plain paths.  Compared with the FP64 oracle history of the 128 x 128
+    crop (tests/golden/two_stream_energy.json): growth rate of the field energy, its
+    saturated level per cell, and the error at the end of the linear phase."""
+    import torch
+    from spectral_rs_b200 import Sim
+    from spectral_rs_b200.config import Config, Params, Setup, Output
+    with open(os.path.join(ROOT, "tests", "golden", "two_stream_energy.json")) as f:
+        ref = json.load(f)
+    st = ref["study"]
+    n = args.study_size
+    steps, every, dt = args.study_steps, st["every"], st["dt"]
+    e64 = np.array(ref["fp64"]["E"]) / (st["size_x"] * st["size_y"])  # energy per cell
+    t64 = (np.arange(len(e64)) + 1) * every * dt
+    peak = int(np.argmax(e64))
+    start = int(np.argmin(e64[:peak + 1]))
+    end = start + int(np.flatnonzero(e64[start:] > 0.5 * e64[peak])[0])
+    win = np.arange(start + (end - start) // 4, end + 1)
+    g64 = np.polyfit(t64[win], np.log(e64[win]), 1)[0] / 2
+    late64 = float(np.mean(e64[len(e64) * 3 // 4:]))
+    out = {"study": "two-stream precision", "grid": [n, n], "steps": steps, "particles": 2 * st["ppc"] * n * n,
+           "fp64_crop": {"grid": [st["size_x"], st["size_y"]], "growth_rate": g64, "late_energy_per_cell": late64,
+                         "peak_energy_per_cell": float(e64[peak])}}
+    for mode in args.study_modes.split(","):
+        p = Params(size_x=n, size_y=n, delta=0, dt=dt, c=st["c"], dens=st["dens"], gamma_inj=st["gamma_inj"],
+                   n_pass=st["n_pass"], periodic_x=True, compensated=mode == "compensated")
+        sim = Sim(Config(p, Setup(steps), Output(False, False, 1, 1, 1, 1)), path="plain" if mode == "plain" else "split")
+        for k, sign in enumerate((1.0, -1.0)):
+            sim.init_species(-1.0, 1.0, st["vth"], st["ppc"], 0, n, st["gamma_inj"], sign, True, 77 + k)
+        sim.prepare()
+        hist = []
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(0, steps, every):
+            sim.step(every)
+            hist.append(float(sim.diag()[0]) / (n * n))
+        wall = time.perf_counter() - t0
+        sim.close()
+        e = np.array(hist)
+        t = (np.arange(len(e)) + 1) * every * dt
+        pk = int(np.argmax(e))
+        s0 = int(np.argmin(e[:pk + 1]))
+        s1 = s0 + int(np.flatnonzero(e[s0:] > 0.5 * e[pk])[0])
+        w = np.arange(s0 + (s1 - s0) // 4, s1 + 1)
+        g = float(np.polyfit(t[w], np.log(e[w]), 1)[0] / 2) if len(w) >= 3 else None
+        late = float(np.mean(e[len(e) * 3 // 4:]))
+        out[mode] = {"growth_rate": g, "growth_rate_rel_err_vs_fp64": None if g is None else abs(g - g64) / g64,
+                     "late_energy_per_cell": late, "late_rel_diff_vs_fp64": abs(late - late64) / late64,
+                     "peak_energy_per_cell": float(e[pk]), "peak_step": (pk + 1) * every,
+                     "fp64_peak_step": (peak + 1) * every, "wall_s": wall,
+                     "history_every": every, "energy_per_cell": [round(x, 8) for x in e.tolist()]}
+        print(json.dumps({mode: {k: v for k, v in out[mode].items() if k != "energy_per_cell"}}), flush=True)
+    with open(args.study_out, "w") as f:
+        json.dump(out, f)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -736,13 +796,20 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="ensemble: skip the C2 / C5 keys")
     ap.add_argument("--small", action="store_true", help="single workloads: 1/16 of the grid (quick checks)")
-    ap.add_argument("--workload", default="ensemble", choices=sorted(WORKLOADS) + ["ensemble"])
+    ap.add_argument("--workload", default="ensemble", choices=sorted(WORKLOADS) + ["ensemble", "two_stream"])
     ap.add_argument("--tile", default=None, help="split-path tile shape TXxTY (default: the library's choice)")
     ap.add_argument("--compensated", action="store_true", help="Kahan-compensated current sums (split path)")
     ap.add_argument("--ppc", type=int, default=None,
                     help="particles per cell of every species (field-phase profiling on the full grid)")
     ap.add_argument("--ensemble", type=int, default=ENSEMBLE_PER_RANK, help="members of the ensemble per GPU")
+    ap.add_argument("--study-size", type=int, default=2048, help="two_stream: grid side")
+    ap.add_argument("--study-steps", type=int, default=2000, help="two_stream: steps")
+    ap.add_argument("--study-modes", default="split,compensated,plain", help="two_stream: paths")
+    ap.add_argument("--study-out", default="two_stream_study.json", help="two_stream: result file")
     args = ap.parse_args()
+    if args.workload == "two_stream":
+        two_stream_study(args)
+        return
     if args.workload == "ensemble":
         if args.impl == "reference":
             run_reference(args, None)

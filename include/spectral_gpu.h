@@ -88,6 +88,10 @@ typedef struct spx_params {
   int32_t device;      /* CUDA device ordinal                                              */
   int32_t compensated; /* 1: current sums of the split path Kahan-compensated in registers and
                           carried through the tile flush (one CTA per SM, slower); 0: plain FP32 */
+  float slot_headroom; /* sort bins (split path): low-range slots per cell = headroom x the fullest
+                          cell's count (at least mean + 8 sqrt(mean)), + 8; 0: 1.25 on a periodic
+                          grid, 4 with a reflecting wall (a shock compresses the plasma)       */
+  int32_t arrival_slots; /* slots per cell of each of the two arrival regions; 0: max(16, low/4) */
 } spx_params;
 
 typedef struct spx_ctx spx_ctx;
@@ -132,6 +136,24 @@ SPX_API int32_t spx_num_species(const spx_ctx* ctx);
  * as save_output does (src/save/mod.rs:36-72). */
 SPX_API int spx_get_species(spx_ctx* ctx, int32_t species, uint64_t stride, uint64_t* ix, uint64_t* iy, float* dx,
                     float* dy, float* px, float* py, float* pz, float* psa);
+
+/* Prtl::tag and Prtl::track (src/prtls.rs:21-22) of one species, n entries each
+ * in the reference's particle order (either pointer may be NULL to leave that
+ * table as it is; track: 0 or 1 per particle).  Particles keep their reference
+ * index for life, so the tables travel with them through every step at no
+ * device cost.  Until set, the reference's defaults hold: tag[i] = i
+ * (src/prtls.rs:213) and only particle 40 tracked (src/prtls.rs:79). */
+SPX_API int spx_set_tags(spx_ctx* ctx, int32_t species, const uint64_t* tag, const uint8_t* track);
+/* The same tables back, every stride-th particle (as spx_get_species). */
+SPX_API int spx_get_tags(spx_ctx* ctx, int32_t species, uint64_t stride, uint64_t* tag, uint8_t* track);
+/* The particle-tracking output of save_output (src/save/mod.rs:82-97) for the
+ * tracked particles, in reference order, gathered on the device:
+ * x = (ix + dx) / c, y = (iy + dy) / c, gamma.  *count receives the number of
+ * tracked particles; with all three outputs NULL the call only counts, else
+ * SPX_ERR_ARG if the count exceeds `capacity` (nothing copied).  Any output
+ * pointer may be NULL. */
+SPX_API int spx_get_tracked(spx_ctx* ctx, int32_t species, uint64_t capacity, float* x, float* y, float* gamma,
+                            uint64_t* count);
 
 /* Zero j_x, j_y, j_z, dsty, dens, ghosts included (src/lib.rs:157-167). */
 SPX_API int spx_zero_sources(spx_ctx* ctx);

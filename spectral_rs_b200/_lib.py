@@ -25,6 +25,7 @@ PATH_SPLIT, PATH_PLAIN = 0, 1
 EXPORTS = [
     "spx_create", "spx_destroy", "spx_last_error", "spx_version", "spx_add_species",
     "spx_init_species", "spx_species_count", "spx_num_species", "spx_get_species",
+    "spx_set_tags", "spx_get_tags", "spx_get_tracked",
     "spx_zero_sources", "spx_move_and_deposit", "spx_deposit_ghosts", "spx_fields_update",
     "spx_boris_push", "spx_prepare", "spx_step", "spx_flush", "spx_synchronize",
     "spx_get_field", "spx_set_field", "spx_get_bwrk", "spx_set_bwrk", "spx_diag",
@@ -45,6 +46,7 @@ class SpxParams(ctypes.Structure):
         ("left_wall", ctypes.c_int32),
         ("path", ctypes.c_int32), ("tile_x", ctypes.c_int32), ("tile_y", ctypes.c_int32),
         ("slot_capacity", ctypes.c_int32), ("device", ctypes.c_int32), ("compensated", ctypes.c_int32),
+        ("slot_headroom", ctypes.c_float), ("arrival_slots", ctypes.c_int32),
     ]
 
 
@@ -83,6 +85,10 @@ def load():
         "spx_species_count": (ctypes.c_uint64, [P, ctypes.c_int32]),
         "spx_num_species": (ctypes.c_int32, [P]),
         "spx_get_species": (ctypes.c_int, [P, ctypes.c_int32, ctypes.c_uint64, P, P, P, P, P, P, P, P]),
+        "spx_set_tags": (ctypes.c_int, [P, ctypes.c_int32, P, P]),
+        "spx_get_tags": (ctypes.c_int, [P, ctypes.c_int32, ctypes.c_uint64, P, P]),
+        "spx_get_tracked": (ctypes.c_int, [P, ctypes.c_int32, ctypes.c_uint64, P, P, P,
+                                            ctypes.POINTER(ctypes.c_uint64)]),
         "spx_zero_sources": (ctypes.c_int, [P]),
         "spx_move_and_deposit": (ctypes.c_int, [P, ctypes.c_int32]),
         "spx_deposit_ghosts": (ctypes.c_int, [P, ctypes.c_int32]),

@@ -13,6 +13,7 @@ reference's behaviour:
   left_wall = false       reflect at ix = delta+1 too (the reference asserts no particle gets there)
   path = "split"          "split" (integer cell + FP32 offset) or "plain" (global FP32 x)
   tile_x, tile_y, slot_capacity   GPU layout knobs (0 = automatic)
+  slot_headroom, arrival_slots    sort-bin sizes of the split path (0 = automatic; tune.py picks them)
   compensated = false     Kahan-compensated current sums in the split-path kernel
 
 [[species]]               optional list replacing the default ion/electron pair
@@ -49,6 +50,8 @@ class Params:
     tile_y: int = 0
     slot_capacity: int = 0
     compensated: bool = False
+    slot_headroom: float = 0.0
+    arrival_slots: int = 0
 
 
 @dataclasses.dataclass

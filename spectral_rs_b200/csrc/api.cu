@@ -123,6 +123,14 @@ struct spx_ctx {
   float last_timing[4] = {0, 0, 0, 0};
   uint64_t last_launches = 0;
   uint64_t repacks = 0, last_overflow = 0, last_max_occ = 0;
+  // Prtl::tag and Prtl::track (src/prtls.rs:21-22) per species.  Particles
+  // never change their reference index, so these are fixed tables over it; an
+  // empty table means the reference's defaults: tag[i] = i (src/prtls.rs:213),
+  // only particle 40 tracked (src/prtls.rs:79).
+  std::vector<std::vector<uint64_t>> tags;
+  std::vector<std::vector<uint8_t>> track;
+  std::vector<int32_t*> d_track_rank;  // output position of each tracked particle, -1 otherwise (lazy)
+  std::vector<uint64_t> n_tracked;
   UploadRing own_up;         // spx_add_species scratch of a standalone context
   UploadRing* up = &own_up;  // the ring in use: a batch lends its one ring to every member
 };
@@ -185,6 +193,8 @@ extern "C" int spx_create(const spx_params* p, spx_ctx** out) {
   if (!p->periodic_x && p->delta * 2 >= p->size_x)
     return fail(nullptr, SPX_ERR_ARG, "Delta must be less than 1/2 the size of size_x (src/lib.rs:88)");
   if (p->dens == 0 || !(p->c > 0) || !(p->dt > 0)) return fail(nullptr, SPX_ERR_ARG, "dens, c and dt must be positive");
+  if (p->slot_headroom < 0 || p->slot_headroom > 64 || p->arrival_slots < 0 || p->arrival_slots > 4096)
+    return fail(nullptr, SPX_ERR_ARG, "slot_headroom must be in [0, 64] and arrival_slots in [0, 4096]");
   spx_ctx* c = new spx_ctx();
   c->prm = *p;
   try {
@@ -258,6 +268,8 @@ extern "C" int spx_destroy(spx_ctx* c) {
     for (float* p : {s.plain.x, s.plain.y, s.plain.px, s.plain.py, s.plain.pz})
       if (p) cudaFree(p);
   }
+  for (int32_t* p : c->d_track_rank)
+    if (p) cudaFree(p);
   c->fb.release();
   c->own_up.release();
   for (void* p : {(void*)c->d_err, (void*)c->d_diag, (void*)c->d_u32, (void*)c->d_counts})
@@ -319,14 +331,16 @@ static Capacity capacity_for(const spx_ctx* c, uint64_t n, uint32_t mx) {
   const double mean = (double)n / (double)c->pg.ncells();
   // room for Poisson-like fluctuations of the occupancy; the overflow list and
   // repack handle anything beyond
-  int KL = (int)std::ceil(std::max(1.25 * mx, mean + 8.0 * std::sqrt(mean))) + 8;
+  const double f = c->prm.slot_headroom > 0 ? (double)c->prm.slot_headroom : 1.25;
+  int KL = (int)std::ceil(std::max(f * mx, mean + 8.0 * std::sqrt(mean))) + 8;
   // a reflecting wall piles incoming and reflected particles up (a shock
-  // compresses the plasma about fourfold): leave room for that from the start
-  if (!c->prm.periodic_x) KL = std::max(KL, (int)std::ceil(4.0 * mx + 8.0 * std::sqrt(4.0 * mx)) + 8);
+  // compresses the plasma about fourfold): by default leave room for that from the start
+  if (!c->prm.periodic_x && !(c->prm.slot_headroom > 0))
+    KL = std::max(KL, (int)std::ceil(4.0 * mx + 8.0 * std::sqrt(4.0 * mx)) + 8);
   if (c->prm.slot_capacity > 0) KL = std::max(KL, c->prm.slot_capacity);
   // arrivals of one step: a few per cent of the occupancy in a thermal plasma,
   // a few tens in a fast flow
-  const int H = std::max(16, (KL + 3) / 4);
+  const int H = c->prm.arrival_slots > 0 ? c->prm.arrival_slots : std::max(16, (KL + 3) / 4);
   return {KL, H};
 }
 
@@ -376,6 +390,14 @@ __global__ void k_pack_check(uint64_t n, uint64_t off, const uint64_t* ix, const
       cell[i] = (uint32_t)x | ((uint32_t)y << 16);
     }
   }
+}
+
+static void add_species_tables(spx_ctx* c, const Species& s) {
+  c->species.push_back(s);
+  c->tags.emplace_back();
+  c->track.emplace_back();
+  c->d_track_rank.push_back(nullptr);
+  c->n_tracked.push_back(0);
 }
 
 extern "C" int spx_add_species(spx_ctx* c, float charge, float mass, float vth, uint64_t n, const uint64_t* ix,
@@ -478,7 +500,7 @@ extern "C" int spx_add_species(spx_ctx* c, float charge, float mass, float vth, 
       release();
       return fail(c, SPX_ERR_GAMMA, "psa differs from sqrt(1 + |p|^2/c^2); the GPU derives gamma from p");
     }
-    c->species.push_back(s);
+    add_species_tables(c, s);
     if (species_out) *species_out = (int32_t)c->species.size() - 1;
     invalidate_graphs(c);
   });
@@ -546,7 +568,7 @@ extern "C" int spx_init_species(spx_ctx* c, float charge, float mass, float vth,
     if (!c->plain) slot_scatter_end(s, c->pg, c->d_counts, c->st);
     SPX_CUDA_TRY(cudaGetLastError());
     SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
-    c->species.push_back(s);
+    add_species_tables(c, s);
     if (species_out) *species_out = (int32_t)c->species.size() - 1;
     invalidate_graphs(c);
   });
@@ -637,6 +659,68 @@ extern "C" int spx_get_species(spx_ctx* c, int32_t sidx, uint64_t stride, uint64
     for (void* p : {(void*)d_ix, (void*)d_iy, (void*)d_dx, (void*)d_dy, (void*)d_px, (void*)d_py, (void*)d_pz,
                     (void*)d_g, (void*)d_u64, (void*)d_f})
       SPX_CUDA_TRY(cudaFreeAsync(p, c->st));
+    SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+  });
+  return SPX_OK;
+}
+
+// ---------------------------------------------------------------- tags and tracked particles
+extern "C" int spx_set_tags(spx_ctx* c, int32_t sidx, const uint64_t* tag, const uint8_t* track) {
+  if (!c) return fail(nullptr, SPX_ERR_ARG, "null context");
+  if (sidx < 0 || sidx >= (int)c->species.size()) return fail(c, SPX_ERR_ARG, "no such species");
+  const uint64_t n = c->species[sidx].n;
+  if (tag) c->tags[sidx].assign(tag, tag + n);
+  if (track) {
+    c->track[sidx].assign(track, track + n);
+    if (c->d_track_rank[sidx]) cudaFree(c->d_track_rank[sidx]);
+    c->d_track_rank[sidx] = nullptr;  // rebuilt by the next spx_get_tracked
+  }
+  return SPX_OK;
+}
+
+extern "C" int spx_get_tags(spx_ctx* c, int32_t sidx, uint64_t stride, uint64_t* tag, uint8_t* track) {
+  if (!c) return fail(nullptr, SPX_ERR_ARG, "null context");
+  if (sidx < 0 || sidx >= (int)c->species.size()) return fail(c, SPX_ERR_ARG, "no such species");
+  if (stride == 0) stride = 1;
+  const uint64_t n = c->species[sidx].n;
+  const std::vector<uint64_t>& tg = c->tags[sidx];
+  const std::vector<uint8_t>& tr = c->track[sidx];
+  for (uint64_t i = 0, k = 0; i < n; i += stride, ++k) {
+    if (tag) tag[k] = tg.empty() ? i : tg[i];
+    if (track) track[k] = tr.empty() ? (uint8_t)(i == 40) : tr[i];
+  }
+  return SPX_OK;
+}
+
+extern "C" int spx_get_tracked(spx_ctx* c, int32_t sidx, uint64_t capacity, float* x, float* y, float* gamma,
+                               uint64_t* count) {
+  if (!c || !count) return fail(c, SPX_ERR_ARG, "null argument");
+  if (sidx < 0 || sidx >= (int)c->species.size()) return fail(c, SPX_ERR_ARG, "no such species");
+  SPX_GUARD(c, {
+    if (int e = spx_flush(c)) return e;
+    const Species& s = c->species[sidx];
+    if (!c->d_track_rank[sidx]) {  // output position of every tracked particle, reference order
+      std::vector<int32_t> rank(std::max<uint64_t>(s.n, 1), -1);
+      const std::vector<uint8_t>& tr = c->track[sidx];
+      uint64_t k = 0;
+      for (uint64_t i = 0; i < s.n; ++i)
+        if (tr.empty() ? i == 40 : tr[i] != 0) rank[i] = (int32_t)k++;
+      SPX_CUDA_TRY(cudaMalloc(&c->d_track_rank[sidx], rank.size() * sizeof(int32_t)));
+      SPX_CUDA_TRY(cudaMemcpy(c->d_track_rank[sidx], rank.data(), rank.size() * sizeof(int32_t),
+                              cudaMemcpyHostToDevice));
+      c->n_tracked[sidx] = k;
+    }
+    const uint64_t k = c->n_tracked[sidx];
+    *count = k;
+    if (k == 0 || (!x && !y && !gamma)) return SPX_OK;  // nothing tracked, or a count query
+    if (k > capacity) return fail(c, SPX_ERR_ARG, "output capacity below the number of tracked particles");
+    float* d_out;
+    SPX_CUDA_TRY(cudaMallocAsync(&d_out, 3 * k * sizeof(float), c->st));
+    gather_tracked(s, c->pg, c->plain, c->d_track_rank[sidx], c->prm.c, d_out, d_out + k, d_out + 2 * k, c->st);
+    float* const dst[3] = {x, y, gamma};
+    for (int f = 0; f < 3; ++f)
+      if (dst[f]) SPX_CUDA_TRY(cudaMemcpyAsync(dst[f], d_out + f * k, k * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+    SPX_CUDA_TRY(cudaFreeAsync(d_out, c->st));
     SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
   });
   return SPX_OK;

@@ -1493,6 +1493,68 @@ int plain_push(Species& s, uint64_t n, const ParticleGeom& pg, const PhysParams&
   return 1;
 }
 
+// ---------------------------------------------------------------- tracked particles
+// save/mod.rs:94-96 in FP32: (ix as Float + dx) / c, (iy as Float + dy) / c, psa
+__device__ __forceinline__ void put_tracked(int32_t r, uint32_t cx, uint32_t cy, float dx, float dy, float px,
+                                            float py, float pz, float c, float csqinv, float* x, float* y, float* g) {
+  x[r] = ((float)cx + dx) / c;
+  y[r] = ((float)cy + dy) / c;
+  g[r] = gamma_of(px, py, pz, csqinv);
+}
+
+__global__ void k_tracked_slot(SpeciesArgs S, int TX, int TY, int logTX, int NTX, size_t ncells, const int32_t* rank,
+                               float c, float csqinv, float* x, float* y, float* g) {
+  const int TC = TX * TY;
+  for (size_t gc = blockIdx.x * (size_t)blockDim.x + threadIdx.x; gc < ncells; gc += (size_t)gridDim.x * blockDim.x) {
+    const size_t tile = gc / TC;
+    const int cc = (int)(gc - tile * TC);
+    const uint32_t cx = (uint32_t)((tile % NTX) * TX + (cc & (TX - 1)) + 1);
+    const uint32_t cy = (uint32_t)((tile / NTX) * TY + (cc >> logTX) + 1);
+    const int nlow = (int)S.nlow[gc], nin = (int)S.ain[gc];
+    const size_t base = tile * (size_t)S.K * TC + cc;
+    for (int n = 0; n < nlow + nin; ++n) {
+      const size_t i = base + (size_t)(n < nlow ? n : S.rin + (n - nlow)) * TC;
+      const int32_t r = rank[S.tag[i]];
+      if (r >= 0) put_tracked(r, cx, cy, S.dx[i], S.dy[i], S.px[i], S.py[i], S.pz[i], c, csqinv, x, y, g);
+    }
+  }
+}
+
+__global__ void k_tracked_overflow(SpeciesArgs S, const int32_t* rank, float c, float csqinv, float* x, float* y,
+                                   float* g) {
+  const uint32_t n = min(*S.rocount, S.ocap);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int32_t r = rank[S.rotag[i]];
+    if (r >= 0)
+      put_tracked(r, S.rocell[i] & 0xFFFFu, S.rocell[i] >> 16, S.rodx[i], S.rody[i], S.ropx[i], S.ropy[i], S.ropz[i],
+                  c, csqinv, x, y, g);
+  }
+}
+
+__global__ void k_tracked_plain(PlainSpecies P, uint64_t n, const int32_t* rank, float c, float csqinv, float* x,
+                                float* y, float* g) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const int32_t r = rank[i];
+    if (r < 0) continue;
+    const int cx = (int)floorf(P.x[i] + 0.5f), cy = (int)floorf(P.y[i] + 0.5f);
+    put_tracked(r, (uint32_t)cx, (uint32_t)cy, P.x[i] - (float)cx, P.y[i] - (float)cy, P.px[i], P.py[i], P.pz[i], c,
+                csqinv, x, y, g);
+  }
+}
+
+void gather_tracked(const Species& s, const ParticleGeom& pg, bool plain, const int32_t* rank, float c, float* x,
+                    float* y, float* g, cudaStream_t st) {
+  const float csqinv = 1.0f / (c * c);
+  if (plain) {
+    if (s.n) k_tracked_plain<<<148 * 4, 256, 0, st>>>(s.plain, s.n, rank, c, csqinv, x, y, g);
+  } else {
+    SpeciesArgs A = species_args(const_cast<Species&>(s));
+    k_tracked_slot<<<148 * 4, 256, 0, st>>>(A, pg.TX, pg.TY, pg.logTX, pg.NTX, pg.ncells(), rank, c, csqinv, x, y, g);
+    k_tracked_overflow<<<16, 256, 0, st>>>(A, rank, c, csqinv, x, y, g);
+  }
+  SPX_CUDA_TRY(cudaGetLastError());
+}
+
 // ---------------------------------------------------------------- diagnostics
 __device__ __forceinline__ void block_add_double(double v, double* out) {
   for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

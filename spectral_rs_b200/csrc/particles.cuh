@@ -154,6 +154,12 @@ int plain_move_deposit(Species& s, uint64_t n, const ParticleGeom& pg, const Phy
 int plain_push(Species& s, uint64_t n, const ParticleGeom& pg, const PhysParams& pp, const FieldPtrs& fp,
                int* derr, cudaStream_t st);
 
+// The tracking output of src/save/mod.rs:85-97 for the particles with
+// rank[reference index] >= 0: x = (ix + dx) / c, y = (iy + dy) / c, gamma, each
+// written at that rank.
+void gather_tracked(const Species& s, const ParticleGeom& pg, bool plain, const int32_t* rank, float c, float* x,
+                    float* y, float* g, cudaStream_t st);
+
 // --- diagnostics ----------------------------------------------------------------
 // Adds sum m (gamma-1) c^2 and the particle count into d_acc[0], d_acc[1] (double).
 void kinetic_energy(const Species& s, const ParticleGeom& pg, bool plain, float c, double* d_acc, cudaStream_t st);

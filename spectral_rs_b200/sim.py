@@ -23,16 +23,18 @@ from .config import Config
 from .init import species_arrays
 
 
-def _tile_choice(cfg, tile):
-    """(tile_x, tile_y) for spx_params: explicit, autotuned, or from the config (0 = library rule)."""
+def _layout_choice(cfg, tile):
+    """(tile_x, tile_y, slot_headroom, arrival_slots) for spx_params: an explicit tile shape,
+    "auto" (tile shape and sort bins from spectral_rs_b200.tune), or the config's (0 = library rule)."""
     p = cfg.params
     if tile is None:
-        return p.tile_x, p.tile_y
+        return p.tile_x, p.tile_y, p.slot_headroom, p.arrival_slots
     if tile == "auto":
-        from .tune import autotune_tiles
+        from .tune import autotune_layout
         crop = (min(p.size_x, 1024), min(p.size_y, 256)) if p.periodic_x else None
-        return autotune_tiles(p, cfg.species_list(), crop=crop)[0]
-    return int(tile[0]), int(tile[1])
+        c = autotune_layout(p, cfg.species_list(), crop=crop)[0]
+        return c["tile"][0], c["tile"][1], c["slot_headroom"], c["arrival_slots"]
+    return int(tile[0]), int(tile[1]), p.slot_headroom, p.arrival_slots
 
 
 class Sim:
@@ -44,7 +46,7 @@ class Sim:
         self.lib = _lib.load()
         self.config = cfg
         p = cfg.params
-        tx, ty = _tile_choice(cfg, tile)
+        tx, ty, headroom, arrival = _layout_choice(cfg, tile)
         self.t = 0
         self.t_final = cfg.setup.t_final
         self.size_x, self.size_y, self.delta = p.size_x, p.size_y, p.delta
@@ -57,7 +59,8 @@ class Sim:
             left_wall=1 if p.left_wall else 0,
             path=_lib.PATH_PLAIN if (path or p.path) == "plain" else _lib.PATH_SPLIT,
             tile_x=tx, tile_y=ty, slot_capacity=p.slot_capacity, device=0,
-            compensated=1 if p.compensated else 0)
+            compensated=1 if p.compensated else 0, slot_headroom=headroom, arrival_slots=arrival)
+        self.layout = {"tile": (tx, ty), "slot_headroom": headroom, "arrival_slots": arrival}
         self._ctx = ctypes.c_void_p()
         _lib.check(self.lib.spx_create(ctypes.byref(prm), ctypes.byref(self._ctx)))
         self.flds = Flds(self)
@@ -238,6 +241,35 @@ class Prtl:
                                                                  ("ix", "iy", "dx", "dy", "px", "py", "pz", "psa")]))
         return out
 
+    def set_tags(self, tag=None, track=None):
+        """Prtl::tag / Prtl::track (src/prtls.rs:21-22) in the reference's order (None keeps a table)."""
+        s = self.sim
+        t = None if tag is None else np.ascontiguousarray(tag, dtype=np.uint64)
+        k = None if track is None else np.ascontiguousarray(track, dtype=np.uint8)
+        for a in (t, k):
+            if a is not None and len(a) != len(self):
+                raise ValueError("one entry per particle")
+        s._chk(s.lib.spx_set_tags(s._ctx, self.sid, _lib.ptr(t), _lib.ptr(k)))
+
+    def tags(self, stride=1):
+        """(tag uint64, track bool) every stride-th particle in the reference's order."""
+        s = self.sim
+        m = (len(self) + stride - 1) // stride
+        t, k = np.empty(m, dtype=np.uint64), np.empty(m, dtype=np.uint8)
+        s._chk(s.lib.spx_get_tags(s._ctx, self.sid, stride, _lib.ptr(t), _lib.ptr(k)))
+        return t, k.astype(bool)
+
+    def tracked(self):
+        """The tracking output of save_output (src/save/mod.rs:82-97): x, y (in units of c) and
+        gamma of the tracked particles, reference order, gathered on the device."""
+        s = self.sim
+        cnt = ctypes.c_uint64(0)
+        s._chk(s.lib.spx_get_tracked(s._ctx, self.sid, 0, None, None, None, ctypes.byref(cnt)))  # count only
+        k = int(cnt.value)
+        x, y, g = (np.empty(k, dtype=np.float32) for _ in range(3))
+        s._chk(s.lib.spx_get_tracked(s._ctx, self.sid, k, _lib.ptr(x), _lib.ptr(y), _lib.ptr(g), ctypes.byref(cnt)))
+        return x, y, g
+
     def boris_push(self, sim=None, flds=None):
         self.sim._chk(self.sim.lib.spx_boris_push(self.sim._ctx, self.sid))
 
@@ -298,17 +330,17 @@ class Batch:
         self.lib = _lib.load()
         prms = (_lib.SpxParams * len(cfgs))()
         shape = None
-        if tile is not None:
+        if tile is not None:  # tuned on the member with the most particles, used by all
             big = max(cfgs, key=lambda c: sum(s.ppc for s in c.species_list()) * c.params.size_x * c.params.size_y)
-            shape = _tile_choice(big, tile)
+            shape = _layout_choice(big, tile)
         for i, cfg in enumerate(cfgs):
             p = cfg.params
-            tx, ty = shape if shape else (p.tile_x, p.tile_y)
+            tx, ty, headroom, arrival = shape if shape else (p.tile_x, p.tile_y, p.slot_headroom, p.arrival_slots)
             prms[i] = _lib.SpxParams(
                 size_x=p.size_x, size_y=p.size_y, delta=p.delta, dt=p.dt, c=p.c, dens=p.dens,
                 gamma_inj=p.gamma_inj, n_pass=p.n_pass, periodic_x=1 if p.periodic_x else 0,
                 left_wall=1 if p.left_wall else 0, path=_lib.PATH_SPLIT, tile_x=tx, tile_y=ty,
-                slot_capacity=p.slot_capacity, device=0)
+                slot_capacity=p.slot_capacity, device=0, slot_headroom=headroom, arrival_slots=arrival)
         self._b = ctypes.c_void_p()
         code = self.lib.spx_batch_create(len(cfgs), prms, ctypes.byref(self._b))
         if code:

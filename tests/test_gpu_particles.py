@@ -371,3 +371,44 @@ def test_run_writes_the_reference_output_layout(tmp_path):
         assert np.max(np.abs(f - ref)) <= DEP_RTOL * max(float(np.max(np.abs(ref))), 1e-30) + 1e-30, name
     for d in ("dat_00001", "dat_00002"):
         assert len(np.load(os.path.join(out, d, "gam.npy"))) == len(x)
+
+
+@pytest.mark.parametrize("path", ["split", "plain"])
+def test_tags_round_trip_through_fused_steps(path):
+    """Prtl::tag / Prtl::track (src/prtls.rs:21-22) survive fused steps (particles change
+    cells and slots), and spx_get_tracked gathers the tracking output of save_output
+    (src/save/mod.rs:94-96) for exactly the tracked particles, in the reference's order."""
+    cfg = _cfg(size_x=64, size_y=32, delta=6, c=3.0, dt=0.1, dens=8, periodic_x=False, left_wall=True, n_pass=4)
+    p = cfg.params
+    specs = [(1.0, 16.0, 0.1, _species(p, 8, 0.1, 1.0050378, 1.0, 71)),
+             (-1.0, 1.0, 0.1, _species(p, 8, 0.1, 1.0050378, 1.0, 72))]
+    sim, _ = _pair(cfg, specs, path=path)
+    pr = sim.prtls[1]
+    n = len(pr)
+    # defaults: tag = index (src/prtls.rs:213), particle 40 tracked (src/prtls.rs:79)
+    t0, k0 = pr.tags()
+    assert np.array_equal(t0, np.arange(n, dtype=np.uint64)) and np.flatnonzero(k0).tolist() == [40]
+    rng = np.random.default_rng(5)
+    tags = rng.integers(0, 2 ** 63, n, dtype=np.uint64)
+    track = rng.random(n) < 0.01
+    pr.set_tags(tags, track)
+    sim.prepare()
+    sim.step(7)
+    t, k = pr.tags()
+    assert np.array_equal(t, tags) and np.array_equal(k, track)
+    ts, ks = pr.tags(stride=5)
+    assert np.array_equal(ts, tags[::5]) and np.array_equal(ks, track[::5])
+    x, y, g = pr.tracked()
+    st = pr.state()
+    f = np.float32
+    c = f(p.c)
+    sel = np.flatnonzero(track)
+    assert len(x) == len(sel)
+    assert np.array_equal(x, ((st["ix"][sel].astype(f) + st["dx"][sel]) / c).astype(f))
+    assert np.array_equal(y, ((st["iy"][sel].astype(f) + st["dy"][sel]) / c).astype(f))
+    assert np.array_equal(g, st["psa"][sel])
+    # the first species keeps its defaults
+    x0, _, _ = sim.prtls[0].tracked()
+    st0 = sim.prtls[0].state()
+    assert len(x0) == 1 and x0[0] == ((f(st0["ix"][40]) + st0["dx"][40]) / c).astype(f)
+    sim.close()

@@ -58,3 +58,33 @@ def test_no_candidate_fits():
     with pytest.raises(ValueError):
         tune.autotune_tiles(_p(size_x=8, size_y=8), SPECIES, candidates=((16, 16),), cache=None,
                             measure=lambda *a: 1.0)
+
+
+def test_autotune_layout_two_stages_and_cache(tmp_path):
+    """Tile shape first (default bins), then (headroom, arrival slots) with that tile; the
+    smallest room within 1 % of the fastest wins; the triple is cached per configuration."""
+    calls = []
+
+    def fake(p, species, shape, steps, headroom, arrival):
+        calls.append((shape, headroom, arrival))
+        if headroom is None:  # stage 1
+            return {(16, 8): 1.0}.get(shape, 2.0)
+        return {1.25: 1.3, 2.0: 1.0, 4.0: 1.005}[headroom] + (0.0 if arrival >= 8 else 9.0)
+
+    cache, tcache = str(tmp_path / "layout.json"), str(tmp_path / "tiles.json")
+    best, times = tune.autotune_layout(_p(), SPECIES, cache=cache, tile_cache=tcache, measure=fake)
+    assert best["tile"] == (16, 8)
+    assert best["slot_headroom"] == 2.0  # 4.0 is within 1 % but needs more room
+    assert best["arrival_slots"] == min(h for (f, h) in times if f == 2.0)
+    assert all(shape == (16, 8) for shape, f, h in calls if f is not None)
+    assert {f for (f, h) in times} == set(tune.HEADROOMS)
+    calls.clear()
+    again, t2 = tune.autotune_layout(_p(), SPECIES, cache=cache, tile_cache=tcache, measure=fake)
+    assert again == best and t2 == {} and calls == []
+
+
+def test_arrival_slots_follow_the_low_range():
+    # 16 per cell: KL = max(f*16, 16 + 32) + 8
+    assert tune.arrival_slots_for(_p(), SPECIES, 1.25, 0.25) == 14   # ceil(0.25 * 56)
+    assert tune.arrival_slots_for(_p(), SPECIES, 4.0, 0.5) == 36     # 0.5 * (64 + 8)
+    assert tune.arrival_slots_for(_p(), SPECIES, 1.25, 0.125) == 8   # floor of 8
