@@ -99,9 +99,12 @@ def _field_state(nx, ny, seed):
     return st, bw
 
 
-# includes the benchmark's row length (4096) and column length (1024) and the 8192-point rows
+# includes the benchmark's row length (4096) and column lengths (1024, 2048), the 8192-point
+# rows, every column length of the fused column pass (16 .. 4096: strips of 2048 points, one
+# 4096-point column) and the 8192-point columns of the three-kernel column path
 @pytest.mark.parametrize("nx,ny,n_pass", [(64, 32, 4), (128, 64, 1), (512, 64, 4), (4096, 64, 4), (1024, 256, 2),
-                                          (8192, 16, 8)])
+                                          (8192, 16, 8), (64, 1024, 4), (32, 2048, 8), (16, 4096, 4),
+                                          (16, 8192, 4), (8, 128, 4), (256, 512, 4)])
 def test_gpu_fields_update_vs_oracle(nx, ny, n_pass):
     """Flds::update on identical inputs: E, B, filtered J and B_wrk against the FP64 oracle."""
     from spectral_rs_b200 import Sim
