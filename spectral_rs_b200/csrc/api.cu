@@ -596,9 +596,12 @@ __global__ void k_plain_to_cells(uint64_t n, const float* x, const float* y, uin
     dy[i] = y[i] - (float)cy;
   }
 }
+// psa = sqrt(1 + |p|^2 / c^2) in the reference's rounding (src/prtls.rs:440): no contraction
 __global__ void k_gamma_arr(uint64_t n, const float* px, const float* py, const float* pz, float csqinv, float* g) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-    g[i] = sqrtf(1.0f + (px[i] * px[i] + py[i] * py[i] + pz[i] * pz[i]) * csqinv);
+    g[i] = __fsqrt_rn(__fadd_rn(1.0f, __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(px[i], px[i]), __fmul_rn(py[i], py[i])),
+                                                          __fmul_rn(pz[i], pz[i])),
+                                                csqinv)));
 }
 
 extern "C" int spx_get_species(spx_ctx* c, int32_t sidx, uint64_t stride, uint64_t* ix, uint64_t* iy, float* dx,

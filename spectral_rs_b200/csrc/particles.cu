@@ -408,6 +408,9 @@ __device__ __noinline__ void drain_m_fn(const StepArgs& a, const SpeciesArgs& S,
 #ifndef SPX_SKEW
 #define SPX_SKEW 0  // fused rounds pipelined across particles (see slot_tile)
 #endif
+#ifndef SPX_INNER_SKIP
+#define SPX_INNER_SKIP 0  // skip apply_bc on tiles no particle can leave the grid from (see slot_tile)
+#endif
 #ifndef SPX_SLOT_MIN_BLOCKS
 #define SPX_SLOT_MIN_BLOCKS 2  // resident 256-thread CTAs per SM the register budget is sized for
 #endif
@@ -642,7 +645,7 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
         const float c1 = half_dt * inv;
         int ix = ox, iy = oy;
         move_half(c1, px, py, ix, iy, dx, dy);
-        if (!INNER) bc_of<BC>(a, nx, ny, ix, iy, dx, px, act);
+        if (!INNER && !(SPX_SKEW == 2 && inner_tile)) bc_of<BC>(a, nx, ny, ix, iy, dx, px, act);
         const float2 vxy = mul2(mul2(bc2(q), make_float2(px, py)), bc2(inv));
         const float vz = q * pz * inv;
         const bool jcross = act && (ix != ox || iy != oy);
@@ -676,7 +679,7 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
         const int jxc = ix, jyc = iy;
         const float jdx = dx, jdy = dy;
         move_half(c1, px, py, ix, iy, dx, dy);
-        if (!INNER) bc_of<BC>(a, nx, ny, ix, iy, dx, px, act);
+        if (!INNER && !(SPX_SKEW == 2 && inner_tile)) bc_of<BC>(a, nx, ny, ix, iy, dx, px, act);
         const bool mover = act && (ix != ox || iy != oy || kept >= KL);
         const bool stay = act && !mover;
         {  // density moments (the count is `kept`); masked lanes add 0
@@ -730,25 +733,32 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
           if (nq_m >= 32) drain_m();
         }
       };
+      // particle r+1 is loaded while particle r is pushed and particle r-1 moved (a load of a
+      // round past the lane's count touches no memory)
       auto run_rounds = [&](auto inner) {
         load(0);
         push_loaded();
+        load(1);
         for (int r = 1; r < rounds; ++r) {
           const float mdx = qdx, mdy = qdy, mpx = qpx, mpy = qpy, mpz = qpz, minv = qinv;
           const uint32_t mtg = qtg;
           const int midx = qidx;
           const bool mact = qact;
-          load(r);
           push_loaded();
+          load(r + 1);
           move_pushed(inner, mdx, mdy, mpx, mpy, mpz, minv, mtg, midx, mact);
         }
         move_pushed(inner, qdx, qdy, qpx, qpy, qpz, qinv, qtg, qidx, qact);
       };
       if (rounds > 0) {
+#if SPX_SKEW == 2
+        run_rounds(std::false_type{});  // one instantiation; the boundary test is a uniform branch
+#else
         if (inner_tile)
           run_rounds(std::true_type{});
         else
           run_rounds(std::false_type{});
+#endif
       }
     } else {
       // software pipeline: the state of round r+1 is loaded during round r (with
@@ -825,7 +835,7 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
             const float c1 = half_dt * inv;
             // first half: position, boundaries, current (src/lib.rs:480-484)
             move_half(c1, px, py, ix, iy, dx, dy);
-            bc_of<BC>(a, nx, ny, ix, iy, dx, px);
+            if (!(SPX_INNER_SKIP && inner_tile)) bc_of<BC>(a, nx, ny, ix, iy, dx, px);
             {
               const float2 vxy = mul2(mul2(bc2(q), make_float2(px, py)), bc2(inv));
               vx = vxy.x;
@@ -884,7 +894,7 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
             }
             // second half: position, boundaries, density (src/lib.rs:486-488)
             move_half(c1, px, py, ix, iy, dx, dy);
-            bc_of<BC>(a, nx, ny, ix, iy, dx, px);
+            if (!(SPX_INNER_SKIP && inner_tile)) bc_of<BC>(a, nx, ny, ix, iy, dx, px);
             // a particle that stays but finds the low range full joins its own
             // cell's arrivals like a mover
             mover = ix != ox || iy != oy || kept >= KL;
