@@ -550,9 +550,9 @@ def _finish(dist):
 
 
 # ---------------------------------------------------------------- batched uneven ensemble
-def _build_batch(members, idx):
+def _build_batch(members, idx, tile=None):
     from spectral_rs_b200 import Batch
-    b = Batch([ensemble_config(members[i]) for i in idx])
+    b = Batch([ensemble_config(members[i]) for i in idx], tile=tile)
     for sim, i in zip(b.sims, idx):
         m = members[i]
         for k, (q, mass, vth, ppc, g) in enumerate(member_species(m)):
@@ -560,9 +560,9 @@ def _build_batch(members, idx):
     return b
 
 
-def measure_ensemble(members, idx, steps, warmup, dist=None, sampler=None, timed_steps=3):
+def measure_ensemble(members, idx, steps, warmup, dist=None, sampler=None, timed_steps=3, tile=None):
     import torch
-    b = _build_batch(members, idx)
+    b = _build_batch(members, idx, tile)
     n_particles = sum(len(p) for s in b.sims for p in s.prtls)
     cells = sum(members[i]["size_x"] * members[i]["size_y"] for i in idx)
     b.prepare()
@@ -682,7 +682,8 @@ def run_ensemble(args):
     e2e = e2e_ensemble(members, idx, args.steps) if rank == 0 and not args.no_e2e else None
     if e2e is not None:
         e2e["ranks_measured"] = 1
-    r = measure_ensemble(members, idx, args.steps, args.warmup, dist, ClockSampler(local))
+    tile = tuple(int(v) for v in args.tile.lower().split("x")) if args.tile else None
+    r = measure_ensemble(members, idx, args.steps, args.warmup, dist, ClockSampler(local), tile=tile)
     ms = max_over_ranks(r["ms"], device="cuda") if dist else r["ms"]
     value = r["particles"] * args.steps * world / (ms / 1e3)  # every rank holds the same number of members
     plain = plain_ensemble(members, idx, args.plain_steps) if rank == 0 and not args.no_plain else None
@@ -710,6 +711,7 @@ def run_ensemble(args):
                                "drift_beta": [round(members[i]["beta"], 4) for i in idx],
                                "vth": 0.1, "c": 3.0, "dt": 0.1, "n_pass": 4, "delta": 8, "walls": "right + left",
                                "path": "split, batched (persistent work-queue particle kernel, one graph per step)",
+                               "tile": list(tile) if tile else [16, 16],
                                "parallelism": f"member list partitioned over {world} ranks" if world > 1 else "single",
                                "l2": _l2_note(r["particles"])})
         line.update({"roofline": r["roofline"], "phase_ms_per_step": r["phase_ms_per_step"], "plain_fp32": plain,

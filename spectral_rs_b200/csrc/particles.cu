@@ -1579,39 +1579,44 @@ void slot_allocate(Species& s, const ParticleGeom& pg, int KL, int H, uint64_t n
   S.KL = KL;
   S.H = H;
   S.ncells = pg.ncells();
-  SPX_CUDA_TRY(cudaMalloc(&S.dx, cap * sizeof(float)));
-  SPX_CUDA_TRY(cudaMalloc(&S.dy, cap * sizeof(float)));
-  SPX_CUDA_TRY(cudaMalloc(&S.px, cap * sizeof(float)));
-  SPX_CUDA_TRY(cudaMalloc(&S.py, cap * sizeof(float)));
-  SPX_CUDA_TRY(cudaMalloc(&S.pz, cap * sizeof(float)));
-  SPX_CUDA_TRY(cudaMalloc(&S.tag, cap * sizeof(uint32_t)));
-  // nlow, narr and ocount are set by slot_scatter_end, on the stream of the scatter
-  SPX_CUDA_TRY(cudaMalloc(&S.nlow, pg.ncells() * sizeof(uint32_t)));
-  SPX_CUDA_TRY(cudaMalloc(&S.narr, 2 * pg.ncells() * sizeof(uint32_t)));
   S.ocap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(1u << 16, n / 32), 1u << 28);
+  // one allocation carved into the slot arrays, the counters and both overflow lists
+  // (one cudaMalloc per species instead of 23: a batch of many small simulations sets up
+  // hundreds of species)
+  const auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t slots = up(cap * 4), cells = up(pg.ncells() * 4), ovf = up((size_t)S.ocap * 4);
+  const size_t total = 6 * slots + 3 * cells + 14 * ovf + 256;
+  SPX_CUDA_TRY(cudaMalloc(&S.block, total));
+  char* p = static_cast<char*>(S.block);
+  auto take = [&](size_t b) {
+    char* q = p;
+    p += b;
+    return q;
+  };
+  S.dx = reinterpret_cast<float*>(take(slots));
+  S.dy = reinterpret_cast<float*>(take(slots));
+  S.px = reinterpret_cast<float*>(take(slots));
+  S.py = reinterpret_cast<float*>(take(slots));
+  S.pz = reinterpret_cast<float*>(take(slots));
+  S.tag = reinterpret_cast<uint32_t*>(take(slots));
+  // nlow, narr and ocount are set by slot_scatter_end, on the stream of the scatter
+  S.nlow = reinterpret_cast<uint32_t*>(take(cells));
+  S.narr = reinterpret_cast<uint32_t*>(take(2 * cells));
   for (int b = 0; b < 2; ++b) {
-    SPX_CUDA_TRY(cudaMalloc(&S.ocell[b], S.ocap * sizeof(uint32_t)));
-    SPX_CUDA_TRY(cudaMalloc(&S.odx[b], S.ocap * sizeof(float)));
-    SPX_CUDA_TRY(cudaMalloc(&S.ody[b], S.ocap * sizeof(float)));
-    SPX_CUDA_TRY(cudaMalloc(&S.opx[b], S.ocap * sizeof(float)));
-    SPX_CUDA_TRY(cudaMalloc(&S.opy[b], S.ocap * sizeof(float)));
-    SPX_CUDA_TRY(cudaMalloc(&S.opz[b], S.ocap * sizeof(float)));
-    SPX_CUDA_TRY(cudaMalloc(&S.otag[b], S.ocap * sizeof(uint32_t)));
+    S.ocell[b] = reinterpret_cast<uint32_t*>(take(ovf));
+    S.odx[b] = reinterpret_cast<float*>(take(ovf));
+    S.ody[b] = reinterpret_cast<float*>(take(ovf));
+    S.opx[b] = reinterpret_cast<float*>(take(ovf));
+    S.opy[b] = reinterpret_cast<float*>(take(ovf));
+    S.opz[b] = reinterpret_cast<float*>(take(ovf));
+    S.otag[b] = reinterpret_cast<uint32_t*>(take(ovf));
   }
-  SPX_CUDA_TRY(cudaMalloc(&S.ocount, 2 * sizeof(uint32_t)));
+  S.ocount = reinterpret_cast<uint32_t*>(take(256));
 }
 
 void slot_release(Species& s) {
   SlotSpecies& S = s.slot;
-  for (void* p : {(void*)S.dx, (void*)S.dy, (void*)S.px, (void*)S.py, (void*)S.pz, (void*)S.tag, (void*)S.nlow,
-                  (void*)S.narr})
-    if (p) cudaFree(p);
-  for (int b = 0; b < 2; ++b) {
-    for (void* p : {(void*)S.ocell[b], (void*)S.odx[b], (void*)S.ody[b], (void*)S.opx[b], (void*)S.opy[b],
-                    (void*)S.opz[b], (void*)S.otag[b]})
-      if (p) cudaFree(p);
-  }
-  if (S.ocount) cudaFree(S.ocount);
+  if (S.block) cudaFree(S.block);
   S = SlotSpecies();
 }
 

@@ -50,6 +50,7 @@ struct SlotSpecies {
   uint32_t ocap = 0;
   int K = 0, KL = 0, H = 0;
   size_t ncells = 0;
+  void* block = nullptr;  // the one device allocation every array above is carved from
   int ocur = 0;  // arrival region and overflow list read by the next step
 };
 
