@@ -875,10 +875,26 @@ static void maybe_repack(spx_ctx* c) {
     SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
     c->last_overflow += h[1];
     c->last_max_occ = std::max<uint64_t>(c->last_max_occ, h[0]);
-    if (h[1] == 0) continue;  // the overflow list is in use: grow the capacity
+    // The overflow list keeps every particle exact, but its fallback kernel is slower per
+    // particle: the slots grow once it holds more than 1/256 of the species.  The capacity
+    // is one number for all cells, so a few dense cells (a bunching beam, a shock) must not
+    // grow every cell's slots after each overflow until the device is full: a repack whose
+    // slots would not fit leaves the particles in the overflow list (its capacity, n/32,
+    // is checked every step: SPX_ERR_STATE when exceeded).
+    const uint64_t n = s.n;
+    if ((uint64_t)h[1] <= std::max<uint64_t>(n / 256, 64)) continue;
+    Capacity want = capacity_for(c, n, h[0]);
+    want.KL = std::max(want.KL, S.KL + std::max(S.KL / 2, 4));
+    want.H = std::max(want.H, S.H + std::max(S.H / 2, 4));
+    {
+      size_t free_b = 0, total_b = 0;
+      SPX_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+      const double old_b = 24.0 * (double)S.ncells * S.K, new_b = 24.0 * (double)S.ncells * (want.KL + 2 * want.H);
+      const double staging = 32.0 * (double)n, margin = 512.0 * 1024 * 1024;
+      if (new_b + staging + margin > (double)free_b + old_b) continue;
+    }
     ++c->repacks;
     // unpack (reference order) and pack again with a larger capacity
-    const uint64_t n = s.n;
     Staging st;
     st.alloc(n);
     uint32_t *d_ix, *d_iy;
@@ -888,8 +904,8 @@ static void maybe_repack(spx_ctx* c) {
     pack_cells(n, d_ix, d_iy, st.cell, c->st);  // cell = ix | iy << 16
     slot_count(c->pg, n, st.cell, c->d_counts, c->st);
     Capacity cap = choose_capacity(c, n);
-    cap.KL = std::max(cap.KL, S.KL + std::max(S.KL / 2, 4));
-    cap.H = std::max(cap.H, S.H + std::max(S.H / 2, 4));
+    cap.KL = std::max(cap.KL, want.KL);
+    cap.H = std::max(cap.H, want.H);
     slot_release(s);
     slot_allocate(s, c->pg, cap.KL, cap.H, n);
     slot_scatter(s, c->pg, n, st.cell, st.dx, st.dy, st.px, st.py, st.pz, nullptr, c->d_counts, c->st);

@@ -9,7 +9,6 @@
 // the particle state (cell indices, offsets, momenta) is then bit-identical to
 // the reference's FP32 arithmetic.
 #include <algorithm>
-#include <type_traits>
 
 #include "particles.cuh"
 #include "exact_math.cuh"
@@ -215,10 +214,9 @@ __device__ __forceinline__ void move_half(float c1, float px, float py, int& ix,
 // max(ix) <= wall_loc + 1 and min(ix) > delta over the species before the wall
 // pass; here each particle checks itself and raises the device error word.
 // the x part of apply_bc without the periodic feature: the reflecting wall
-__device__ __forceinline__ void wall_x(const PhysParams& p, int& ix, float& dx, float& px, int* derr,
-                                       bool live = true) {
+__device__ __forceinline__ void wall_x(const PhysParams& p, int& ix, float& dx, float& px, int* derr) {
   {
-    if (live && (ix > p.wall_loc + 1 || ix < p.delta + (p.left_wall ? 0 : 1))) atomicOr(derr, DERR_WALL);
+    if (ix > p.wall_loc + 1 || ix < p.delta + (p.left_wall ? 0 : 1)) atomicOr(derr, DERR_WALL);
     if (p.left_wall && ix <= p.delta + 1) {  // optional mirror image of the right wall
       if (ix == p.delta + 1) {
         const float sgn = isnan(dx) ? dx : copysignf(1.0f, dx);
@@ -424,12 +422,6 @@ __device__ __noinline__ void drain_m_fn(const StepArgs& a, const SpeciesArgs& S,
 // the loads of a round are coalesced; the particles that stay are written back
 // densely from slot 0 (a round's stores cover a few neighbouring slot rows and
 // merge in L2).
-#ifndef SPX_SKEW
-#define SPX_SKEW 0  // fused rounds pipelined across particles (see slot_tile)
-#endif
-#ifndef SPX_INNER_SKIP
-#define SPX_INNER_SKIP 0  // skip apply_bc on tiles no particle can leave the grid from (see slot_tile)
-#endif
 #ifndef SPX_SLOT_MIN_BLOCKS
 #define SPX_SLOT_MIN_BLOCKS 2  // resident 256-thread CTAs per SM the register budget is sized for
 #endif
@@ -449,10 +441,8 @@ __device__ __forceinline__ void periodic_bc(int nx, int ny, int& ix, int& iy) {
 // Boundary handling known at compile time: BC_ANY reads a.p, BC_PERIODIC is the
 // reference's `periodic` feature, BC_WALL the reflecting wall.
 enum : int { BC_ANY = 0, BC_PERIODIC = 1, BC_WALL = 2 };
-// live = false: a lane's resting dummy particle (the wall assertion is not raised for it)
 template <int BC>
-__device__ __forceinline__ void bc_of(const StepArgs& a, int nx, int ny, int& ix, int& iy, float& dx, float& px,
-                                      bool live = true) {
+__device__ __forceinline__ void bc_of(const StepArgs& a, int nx, int ny, int& ix, int& iy, float& dx, float& px) {
   if (BC == BC_PERIODIC) {
     periodic_bc(nx, ny, ix, iy);
   } else if (BC == BC_WALL) {
@@ -460,7 +450,7 @@ __device__ __forceinline__ void bc_of(const StepArgs& a, int nx, int ny, int& ix
       iy += ny;
     else if (iy > ny)
       iy -= ny;
-    wall_x(a.p, ix, dx, px, a.derr, live);
+    wall_x(a.p, ix, dx, px, a.derr);
   } else {
     if (iy < 1)
       iy += ny;
@@ -472,7 +462,7 @@ __device__ __forceinline__ void bc_of(const StepArgs& a, int nx, int ny, int& ix
       else if (ix > nx)
         ix -= nx;
     } else {
-      wall_x(a.p, ix, dx, px, a.derr, live);
+      wall_x(a.p, ix, dx, px, a.derr);
     }
   }
 }
@@ -587,139 +577,164 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
       nq_m = 0;
     };
 
-#if SPX_SKEW
-    constexpr bool SKEWED = PUSH && MOVE && !COMP;
-#else
-    constexpr bool SKEWED = false;
-#endif
-    if constexpr (SKEWED) {
-      // Fused push + move, pipelined across a lane's particles: iteration i moves
-      // particle i-1 (positions, boundaries, deposits, write-back) and pushes
-      // particle i (gather, Boris).  The two are independent and run as one
-      // straight-line block for every lane; a lane past its count works on a
-      // resting dummy particle whose effects (deposits, stores, queues, the wall
-      // assertion) are masked, so the scheduler can interleave the two chains.
-      // Writes stay at or below the slot of the particle written (kept <= its
-      // round), loads are of later slots: no particle is overwritten before read.
-      float ldx = 0.f, ldy = 0.f, lpx = 0.f, lpy = 0.f, lpz = 0.f;  // loaded, to be pushed
-      uint32_t ltg = 0u;
-      int lidx = c;
-      bool lact = false;
-      auto load = [&](int r) {
-        const int sl = slot_of(r, lact);
-        lidx = sl * TC + c;
-        if (lact) {
-          ldx = sdx[lidx];
-          ldy = sdy[lidx];
-          lpx = spx[lidx];
-          lpy = spy[lidx];
-          lpz = spz[lidx];
-          ltg = stg[lidx];
-        } else {
-          ldx = ldy = lpx = lpy = lpz = 0.f;
+    // software pipeline: the state of round r+1 is loaded during round r (with
+    // the tag on moving steps: a particle that moves or shifts down takes it along)
+    float ndx = 0.f, ndy = 0.f, npx = 0.f, npy = 0.f, npz = 0.f;
+    uint32_t ntg = 0u;
+    bool nact = false;
+    int nidx = c;
+    if (rounds > 0) {
+      const int sl = slot_of(0, nact);
+      nidx = sl * TC + c;
+      if (nact) {
+        ndx = sdx[nidx];
+        ndy = sdy[nidx];
+        npx = spx[nidx];
+        npy = spy[nidx];
+        npz = spz[nidx];
+        if (MOVE) ntg = stg[nidx];
+      }
+    }
+    for (int r = 0; r < rounds; ++r) {
+      const int idx = nidx;
+      const bool act = nact;
+      float dx = ndx, dy = ndy, px = npx, py = npy, pz = npz;
+      const uint32_t tg = ntg;
+      if (r + 1 < rounds) {
+        const int sl = slot_of(r + 1, nact);
+        nidx = sl * TC + c;
+        if (nact) {
+          ndx = sdx[nidx];
+          ndy = sdy[nidx];
+          npx = spx[nidx];
+          npy = spy[nidx];
+          npz = spz[nidx];
+          if (MOVE) ntg = stg[nidx];
         }
-      };
-      float qdx = 0.f, qdy = 0.f, qpx = 0.f, qpy = 0.f, qpz = 0.f, qinv = 1.f;  // pushed, to be moved
-      uint32_t qtg = 0u;
-      int qidx = c;
-      bool qact = false;
-      // push of the loaded particle into the pushed slot (src/prtls.rs:262-443)
-      auto push_loaded = [&]() {
-        float w[9];
-        tsc_weights_x2(ldx, ldy, w);
-        float2 g01, g23, g45;
+      }
+      bool jcross = false, mover = false;
+      int ix = ox, iy = oy, jxc = ox, jyc = oy;
+      float jdx = 0.f, jdy = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
+      if (act) {
+        float psa;
+        if (PUSH) {
+          float w[9];
+          tsc_weights_x2(dx, dy, w);
+          // six running sums, neighbour cells in the reference's order w00 .. w22
+          float gth[6];
+          float2 g01, g23, g45;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) {
-          const int o = ebo + (k / 3) * EX + (k % 3);
-          const float4 e4 = eb4[o];
-          const float2 e2 = eb2[o];
-          const float2 p01 = make_float2(w[k] * e4.x, w[k] * e4.y);
-          const float2 p23 = make_float2(w[k] * e4.z, w[k] * e4.w);
-          const float2 p45 = make_float2(w[k] * e2.x, w[k] * e2.y);
-          if (k == 0) {
-            g01 = p01; g23 = p23; g45 = p45;
+          for (int k = 0; k < 9; ++k) {
+            const int o = ebo + (k / 3) * EX + (k % 3);
+            const float4 e4 = eb4[o];
+            const float2 e2 = eb2[o];
+            const float2 p01 = make_float2(w[k] * e4.x, w[k] * e4.y);
+            const float2 p23 = make_float2(w[k] * e4.z, w[k] * e4.w);
+            const float2 p45 = make_float2(w[k] * e2.x, w[k] * e2.y);
+            if (k == 0) {
+              g01 = p01; g23 = p23; g45 = p45;
+            } else {
+              g01 = add2(g01, p01); g23 = add2(g23, p23); g45 = add2(g45, p45);
+            }
+          }
+          gth[0] = g01.x; gth[1] = g01.y; gth[2] = g23.x; gth[3] = g23.y; gth[4] = g45.x; gth[5] = g45.y;
+          boris(gth, beta, alpha, csqinv, px, py, pz, psa);
+        } else {
+          psa = gamma_of(px, py, pz, csqinv);
+        }
+        if (!MOVE) {
+          spx[idx] = px;
+          spy[idx] = py;
+          spz[idx] = pz;
+        } else {
+          const float inv = p_rcp(psa);
+          const float c1 = half_dt * inv;
+          // first half: position, boundaries, current (src/lib.rs:480-484)
+          move_half(c1, px, py, ix, iy, dx, dy);
+          if (!inner_tile) bc_of<BC>(a, nx, ny, ix, iy, dx, px);
+          {
+            const float2 vxy = mul2(mul2(bc2(q), make_float2(px, py)), bc2(inv));
+            vx = vxy.x;
+            vy = vxy.y;
+          }
+          vz = q * pz * inv;
+          jcross = ix != ox || iy != oy;
+          if (!jcross && !COMP) {
+            // moments sum v dy^i dx^j, i, j = 0..2 (see moments_to_stencil); fused
+            // multiply-adds: the deposit sums are not the reference's order anyway
+            const float2 vxy = make_float2(vx, vy);
+            const float2 a1 = mul2(vxy, bc2(dx));  // v dx
+            const float2 a2 = mul2(a1, bc2(dx));   // v dx^2
+            const float z1 = vz * dx, z2 = z1 * dx;
+            const float dy2 = dy * dy;
+            accJxy[0] = add2(accJxy[0], vxy);
+            accJxy[1] = add2(accJxy[1], a1);
+            accJxy[2] = add2(accJxy[2], a2);
+            accJxy[3] = fma2(bc2(dy), vxy, accJxy[3]);
+            accJxy[4] = fma2(bc2(dy), a1, accJxy[4]);
+            accJxy[5] = fma2(bc2(dy), a2, accJxy[5]);
+            accJxy[6] = fma2(bc2(dy2), vxy, accJxy[6]);
+            accJxy[7] = fma2(bc2(dy2), a1, accJxy[7]);
+            accJxy[8] = fma2(bc2(dy2), a2, accJxy[8]);
+            accJz[0] += vz;
+            accJz[1] += z1;
+            accJz[2] += z2;
+            accJz[3] = __fmaf_rn(dy, vz, accJz[3]);
+            accJz[4] = __fmaf_rn(dy, z1, accJz[4]);
+            accJz[5] = __fmaf_rn(dy, z2, accJz[5]);
+            accJz[6] = __fmaf_rn(dy2, vz, accJz[6]);
+            accJz[7] = __fmaf_rn(dy2, z1, accJz[7]);
+            accJz[8] = __fmaf_rn(dy2, z2, accJz[8]);
+          } else if (!jcross) {
+            float w[9];
+            tsc_weights_x2(dx, dy, w);
+            const float2 vxy = make_float2(vx, vy);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+              {  // Kahan summation: y = w v - comp; t = acc + y; comp = (t - acc) - y
+                const float2 y = fma2(bc2(w[k]), vxy, make_float2(-cmpJxy[k].x, -cmpJxy[k].y));
+                const float2 t = add2(accJxy[k], y);
+                cmpJxy[k] = sub2(sub2(t, accJxy[k]), y);
+                accJxy[k] = t;
+                const float yz = __fmaf_rn(w[k], vz, -cmpJz[k]);
+                const float tz = __fadd_rn(accJz[k], yz);
+                cmpJz[k] = __fsub_rn(__fsub_rn(tz, accJz[k]), yz);
+                accJz[k] = tz;
+              }
+            }
           } else {
-            g01 = add2(g01, p01); g23 = add2(g23, p23); g45 = add2(g45, p45);
+            jxc = ix;
+            jyc = iy;
+            jdx = dx;
+            jdy = dy;
+          }
+          // second half: position, boundaries, density (src/lib.rs:486-488)
+          move_half(c1, px, py, ix, iy, dx, dy);
+          if (!inner_tile) bc_of<BC>(a, nx, ny, ix, iy, dx, px);
+          // a particle that stays but finds the low range full joins its own
+          // cell's arrivals like a mover
+          mover = ix != ox || iy != oy || kept >= KL;
+          if (!mover) {
+            // density moments (the count is `kept`): sum dx, dy, dx^2, dy^2, dx dy, dy dx^2, dx dy^2, dx^2 dy^2
+            const float2 dd = make_float2(dx, dy);
+            const float2 sq = mul2(dd, dd);
+            rm1 = add2(rm1, dd);
+            rm2 = add2(rm2, sq);
+            rm11 = __fmaf_rn(dx, dy, rm11);
+            rm12 = fma2(make_float2(dy, dx), sq, rm12);
+            rm22 = __fmaf_rn(sq.x, sq.y, rm22);
+            const int o = kept * TC + c;
+            sdx[o] = dx;
+            sdy[o] = dy;
+            spx[o] = px;
+            spy[o] = py;
+            spz[o] = pz;
+            if (o != idx) stg[o] = tg;
+            ++kept;
           }
         }
-        const float gth[6] = {g01.x, g01.y, g23.x, g23.y, g45.x, g45.y};
-        float px = lpx, py = lpy, pz = lpz, psa;
-        boris(gth, beta, alpha, csqinv, px, py, pz, psa);
-        qdx = ldx;
-        qdy = ldy;
-        qpx = px;
-        qpy = py;
-        qpz = pz;
-        qinv = p_rcp(psa);
-        qtg = ltg;
-        qidx = lidx;
-        qact = lact;
-      };
-      // move_and_deposit (src/lib.rs:478-489) of the pushed particle, then its queues.
-      // INNER: the tile's particles cannot reach a grid edge or a wall this step (apply_bc is
-      // the identity for them), known per tile
-      auto move_pushed = [&](auto inner, float dx, float dy, float px, float py, float pz, float inv, uint32_t tg,
-                             int idx, bool act) {
-        constexpr bool INNER = decltype(inner)::value;
-        const float c1 = half_dt * inv;
-        int ix = ox, iy = oy;
-        move_half(c1, px, py, ix, iy, dx, dy);
-        if (!INNER && !(SPX_SKEW == 2 && inner_tile)) bc_of<BC>(a, nx, ny, ix, iy, dx, px, act);
-        const float2 vxy = mul2(mul2(bc2(q), make_float2(px, py)), bc2(inv));
-        const float vz = q * pz * inv;
-        const bool jcross = act && (ix != ox || iy != oy);
-        const bool jdep = act && !jcross;
-        {  // current moments of the owner cell (see moments_to_stencil); masked lanes add 0
-          const float2 v = jdep ? vxy : make_float2(0.f, 0.f);
-          const float w = jdep ? vz : 0.f;
-          const float2 a1 = mul2(v, bc2(dx));
-          const float2 a2 = mul2(a1, bc2(dx));
-          const float z1 = w * dx, z2 = z1 * dx;
-          const float dy2 = dy * dy;
-          accJxy[0] = add2(accJxy[0], v);
-          accJxy[1] = add2(accJxy[1], a1);
-          accJxy[2] = add2(accJxy[2], a2);
-          accJxy[3] = fma2(bc2(dy), v, accJxy[3]);
-          accJxy[4] = fma2(bc2(dy), a1, accJxy[4]);
-          accJxy[5] = fma2(bc2(dy), a2, accJxy[5]);
-          accJxy[6] = fma2(bc2(dy2), v, accJxy[6]);
-          accJxy[7] = fma2(bc2(dy2), a1, accJxy[7]);
-          accJxy[8] = fma2(bc2(dy2), a2, accJxy[8]);
-          accJz[0] += w;
-          accJz[1] += z1;
-          accJz[2] += z2;
-          accJz[3] = __fmaf_rn(dy, w, accJz[3]);
-          accJz[4] = __fmaf_rn(dy, z1, accJz[4]);
-          accJz[5] = __fmaf_rn(dy, z2, accJz[5]);
-          accJz[6] = __fmaf_rn(dy2, w, accJz[6]);
-          accJz[7] = __fmaf_rn(dy2, z1, accJz[7]);
-          accJz[8] = __fmaf_rn(dy2, z2, accJz[8]);
-        }
-        const int jxc = ix, jyc = iy;
-        const float jdx = dx, jdy = dy;
-        move_half(c1, px, py, ix, iy, dx, dy);
-        if (!INNER && !(SPX_SKEW == 2 && inner_tile)) bc_of<BC>(a, nx, ny, ix, iy, dx, px, act);
-        const bool mover = act && (ix != ox || iy != oy || kept >= KL);
-        const bool stay = act && !mover;
-        {  // density moments (the count is `kept`); masked lanes add 0
-          const float2 dd = stay ? make_float2(dx, dy) : make_float2(0.f, 0.f);
-          const float2 sq = mul2(dd, dd);
-          rm1 = add2(rm1, dd);
-          rm2 = add2(rm2, sq);
-          rm11 = __fmaf_rn(dd.x, dd.y, rm11);
-          rm12 = fma2(make_float2(dd.y, dd.x), sq, rm12);
-          rm22 = __fmaf_rn(sq.x, sq.y, rm22);
-        }
-        if (stay) {
-          const int o = kept * TC + c;
-          sdx[o] = dx;
-          sdy[o] = dy;
-          spx[o] = px;
-          spy[o] = py;
-          spz[o] = pz;
-          if (o != idx) stg[o] = tg;
-          ++kept;
-        }
+      }
+      if (MOVE) {
         const unsigned mj = __ballot_sync(0xffffffffu, jcross);
         if (mj) {
           if (jcross) {
@@ -727,8 +742,8 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
             qj[0 * QCAP + e] = __uint_as_float((uint32_t)jxc | ((uint32_t)jyc << 16));
             qj[1 * QCAP + e] = jdx;
             qj[2 * QCAP + e] = jdy;
-            qj[3 * QCAP + e] = vxy.x;
-            qj[4 * QCAP + e] = vxy.y;
+            qj[3 * QCAP + e] = vx;
+            qj[4 * QCAP + e] = vy;
             qj[5 * QCAP + e] = vz;
           }
           nq_j += __popc(mj);
@@ -750,225 +765,6 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
           nq_m += __popc(mm);
           __syncwarp();
           if (nq_m >= 32) drain_m();
-        }
-      };
-      // particle r+1 is loaded while particle r is pushed and particle r-1 moved (a load of a
-      // round past the lane's count touches no memory)
-      auto run_rounds = [&](auto inner) {
-        load(0);
-        push_loaded();
-        load(1);
-        for (int r = 1; r < rounds; ++r) {
-          const float mdx = qdx, mdy = qdy, mpx = qpx, mpy = qpy, mpz = qpz, minv = qinv;
-          const uint32_t mtg = qtg;
-          const int midx = qidx;
-          const bool mact = qact;
-          push_loaded();
-          load(r + 1);
-          move_pushed(inner, mdx, mdy, mpx, mpy, mpz, minv, mtg, midx, mact);
-        }
-        move_pushed(inner, qdx, qdy, qpx, qpy, qpz, qinv, qtg, qidx, qact);
-      };
-      if (rounds > 0) {
-#if SPX_SKEW == 2
-        run_rounds(std::false_type{});  // one instantiation; the boundary test is a uniform branch
-#else
-        if (inner_tile)
-          run_rounds(std::true_type{});
-        else
-          run_rounds(std::false_type{});
-#endif
-      }
-    } else {
-      // software pipeline: the state of round r+1 is loaded during round r (with
-      // the tag on moving steps: a particle that moves or shifts down takes it along)
-      float ndx = 0.f, ndy = 0.f, npx = 0.f, npy = 0.f, npz = 0.f;
-      uint32_t ntg = 0u;
-      bool nact = false;
-      int nidx = c;
-      if (rounds > 0) {
-        const int sl = slot_of(0, nact);
-        nidx = sl * TC + c;
-        if (nact) {
-          ndx = sdx[nidx];
-          ndy = sdy[nidx];
-          npx = spx[nidx];
-          npy = spy[nidx];
-          npz = spz[nidx];
-          if (MOVE) ntg = stg[nidx];
-        }
-      }
-      for (int r = 0; r < rounds; ++r) {
-        const int idx = nidx;
-        const bool act = nact;
-        float dx = ndx, dy = ndy, px = npx, py = npy, pz = npz;
-        const uint32_t tg = ntg;
-        if (r + 1 < rounds) {
-          const int sl = slot_of(r + 1, nact);
-          nidx = sl * TC + c;
-          if (nact) {
-            ndx = sdx[nidx];
-            ndy = sdy[nidx];
-            npx = spx[nidx];
-            npy = spy[nidx];
-            npz = spz[nidx];
-            if (MOVE) ntg = stg[nidx];
-          }
-        }
-        bool jcross = false, mover = false;
-        int ix = ox, iy = oy, jxc = ox, jyc = oy;
-        float jdx = 0.f, jdy = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
-        if (act) {
-          float psa;
-          if (PUSH) {
-            float w[9];
-            tsc_weights_x2(dx, dy, w);
-            // six running sums, neighbour cells in the reference's order w00 .. w22
-            float gth[6];
-            float2 g01, g23, g45;
-  #pragma unroll
-            for (int k = 0; k < 9; ++k) {
-              const int o = ebo + (k / 3) * EX + (k % 3);
-              const float4 e4 = eb4[o];
-              const float2 e2 = eb2[o];
-              const float2 p01 = make_float2(w[k] * e4.x, w[k] * e4.y);
-              const float2 p23 = make_float2(w[k] * e4.z, w[k] * e4.w);
-              const float2 p45 = make_float2(w[k] * e2.x, w[k] * e2.y);
-              if (k == 0) {
-                g01 = p01; g23 = p23; g45 = p45;
-              } else {
-                g01 = add2(g01, p01); g23 = add2(g23, p23); g45 = add2(g45, p45);
-              }
-            }
-            gth[0] = g01.x; gth[1] = g01.y; gth[2] = g23.x; gth[3] = g23.y; gth[4] = g45.x; gth[5] = g45.y;
-            boris(gth, beta, alpha, csqinv, px, py, pz, psa);
-          } else {
-            psa = gamma_of(px, py, pz, csqinv);
-          }
-          if (!MOVE) {
-            spx[idx] = px;
-            spy[idx] = py;
-            spz[idx] = pz;
-          } else {
-            const float inv = p_rcp(psa);
-            const float c1 = half_dt * inv;
-            // first half: position, boundaries, current (src/lib.rs:480-484)
-            move_half(c1, px, py, ix, iy, dx, dy);
-            if (!(SPX_INNER_SKIP && inner_tile)) bc_of<BC>(a, nx, ny, ix, iy, dx, px);
-            {
-              const float2 vxy = mul2(mul2(bc2(q), make_float2(px, py)), bc2(inv));
-              vx = vxy.x;
-              vy = vxy.y;
-            }
-            vz = q * pz * inv;
-            jcross = ix != ox || iy != oy;
-            if (!jcross && !COMP) {
-              // moments sum v dy^i dx^j, i, j = 0..2 (see moments_to_stencil); fused
-              // multiply-adds: the deposit sums are not the reference's order anyway
-              const float2 vxy = make_float2(vx, vy);
-              const float2 a1 = mul2(vxy, bc2(dx));  // v dx
-              const float2 a2 = mul2(a1, bc2(dx));   // v dx^2
-              const float z1 = vz * dx, z2 = z1 * dx;
-              const float dy2 = dy * dy;
-              accJxy[0] = add2(accJxy[0], vxy);
-              accJxy[1] = add2(accJxy[1], a1);
-              accJxy[2] = add2(accJxy[2], a2);
-              accJxy[3] = fma2(bc2(dy), vxy, accJxy[3]);
-              accJxy[4] = fma2(bc2(dy), a1, accJxy[4]);
-              accJxy[5] = fma2(bc2(dy), a2, accJxy[5]);
-              accJxy[6] = fma2(bc2(dy2), vxy, accJxy[6]);
-              accJxy[7] = fma2(bc2(dy2), a1, accJxy[7]);
-              accJxy[8] = fma2(bc2(dy2), a2, accJxy[8]);
-              accJz[0] += vz;
-              accJz[1] += z1;
-              accJz[2] += z2;
-              accJz[3] = __fmaf_rn(dy, vz, accJz[3]);
-              accJz[4] = __fmaf_rn(dy, z1, accJz[4]);
-              accJz[5] = __fmaf_rn(dy, z2, accJz[5]);
-              accJz[6] = __fmaf_rn(dy2, vz, accJz[6]);
-              accJz[7] = __fmaf_rn(dy2, z1, accJz[7]);
-              accJz[8] = __fmaf_rn(dy2, z2, accJz[8]);
-            } else if (!jcross) {
-              float w[9];
-              tsc_weights_x2(dx, dy, w);
-              const float2 vxy = make_float2(vx, vy);
-  #pragma unroll
-              for (int k = 0; k < 9; ++k) {
-                {  // Kahan summation: y = w v - comp; t = acc + y; comp = (t - acc) - y
-                  const float2 y = fma2(bc2(w[k]), vxy, make_float2(-cmpJxy[k].x, -cmpJxy[k].y));
-                  const float2 t = add2(accJxy[k], y);
-                  cmpJxy[k] = sub2(sub2(t, accJxy[k]), y);
-                  accJxy[k] = t;
-                  const float yz = __fmaf_rn(w[k], vz, -cmpJz[k]);
-                  const float tz = __fadd_rn(accJz[k], yz);
-                  cmpJz[k] = __fsub_rn(__fsub_rn(tz, accJz[k]), yz);
-                  accJz[k] = tz;
-                }
-              }
-            } else {
-              jxc = ix;
-              jyc = iy;
-              jdx = dx;
-              jdy = dy;
-            }
-            // second half: position, boundaries, density (src/lib.rs:486-488)
-            move_half(c1, px, py, ix, iy, dx, dy);
-            if (!(SPX_INNER_SKIP && inner_tile)) bc_of<BC>(a, nx, ny, ix, iy, dx, px);
-            // a particle that stays but finds the low range full joins its own
-            // cell's arrivals like a mover
-            mover = ix != ox || iy != oy || kept >= KL;
-            if (!mover) {
-              // density moments (the count is `kept`): sum dx, dy, dx^2, dy^2, dx dy, dy dx^2, dx dy^2, dx^2 dy^2
-              const float2 dd = make_float2(dx, dy);
-              const float2 sq = mul2(dd, dd);
-              rm1 = add2(rm1, dd);
-              rm2 = add2(rm2, sq);
-              rm11 = __fmaf_rn(dx, dy, rm11);
-              rm12 = fma2(make_float2(dy, dx), sq, rm12);
-              rm22 = __fmaf_rn(sq.x, sq.y, rm22);
-              const int o = kept * TC + c;
-              sdx[o] = dx;
-              sdy[o] = dy;
-              spx[o] = px;
-              spy[o] = py;
-              spz[o] = pz;
-              if (o != idx) stg[o] = tg;
-              ++kept;
-            }
-          }
-        }
-        if (MOVE) {
-          const unsigned mj = __ballot_sync(0xffffffffu, jcross);
-          if (mj) {
-            if (jcross) {
-              const int e = nq_j + __popc(mj & lt_mask);
-              qj[0 * QCAP + e] = __uint_as_float((uint32_t)jxc | ((uint32_t)jyc << 16));
-              qj[1 * QCAP + e] = jdx;
-              qj[2 * QCAP + e] = jdy;
-              qj[3 * QCAP + e] = vx;
-              qj[4 * QCAP + e] = vy;
-              qj[5 * QCAP + e] = vz;
-            }
-            nq_j += __popc(mj);
-            __syncwarp();
-            if (nq_j >= 32) drain_j();
-          }
-          const unsigned mm = __ballot_sync(0xffffffffu, mover);
-          if (mm) {
-            if (mover) {
-              const int e = nq_m + __popc(mm & lt_mask);
-              qm[0 * QCAP + e] = __uint_as_float((uint32_t)ix | ((uint32_t)iy << 16));
-              qm[1 * QCAP + e] = dx;
-              qm[2 * QCAP + e] = dy;
-              qm[3 * QCAP + e] = px;
-              qm[4 * QCAP + e] = py;
-              qm[5 * QCAP + e] = pz;
-              qm[6 * QCAP + e] = __uint_as_float(tg);
-            }
-            nq_m += __popc(mm);
-            __syncwarp();
-            if (nq_m >= 32) drain_m();
-          }
         }
       }
     }
