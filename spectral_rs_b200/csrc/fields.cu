@@ -480,25 +480,28 @@ __global__ void k_kspace(KArgs a, Grid g) {
 // update (Ampere, divergence correction, Faraday, Nyquist, B average: the expressions of
 // k_kspace) and the inverse column transforms of B(t) and E.  A thread holds the same 8
 // points of the strip after every forward transform, so the k-space update runs on them
-// in registers as each field arrives; E (3 fields) waits in shared memory at those points
-// and B_wrk is read and rewritten in place.  Shared memory: 6 slots of the strip (E, then
-// B(t)), one of which is the forward transforms' exchange buffer until B(t) is written.
+// as each field arrives, from shared memory only: E waits in three strip slots, B_wrk is
+// staged into three more by asynchronous copies issued at the start (they land while the
+// first transforms run) and is replaced there by B(t); a seventh slot is the transforms'
+// exchange buffer.  The next field's inputs are loaded while the current one transforms.
 // Per cell it reads 7 + 3 and writes 3 + 6 complex values: 152 B against 360 B for the
-// three separate passes.
-constexpr int FUSED_SLOTS = 6;
-// strips of 2048 points (256 threads) while the columns are at most 2048 long; a single
-// 4096-point column (512 threads); 8192-point columns do not fit (three-kernel path)
+// three separate passes.  Strips of 1024 points (128 threads, 61 KB: three CTAs per SM);
+// columns longer than 1024 points take the three-kernel path.
+constexpr int FUSED_SLOTS = 7;
 __host__ __device__ inline int fused_logW(int logNy, int logNx) {
-  int lw = logNy <= 11 ? 11 - logNy : 0;
+  int lw = 10 - logNy;
+  if (lw < 0) lw = 0;
   return lw > logNx ? logNx : lw;
 }
-bool cols_fused_fits(int logNy) { return logNy <= 12; }
+bool cols_fused_fits(int logNy) { return logNy <= 10; }
 
-// Register budgets measured with -Xptxas -v: 1024-point columns compile without spills
-// under the two-CTA bound (64 registers), the other lengths under the one-CTA bound (a
-// 256-thread CTA at 128 registers still leaves room for the two CTAs shared memory allows).
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+
 template <int LOGN>
-__global__ void __launch_bounds__(512, LOGN == 10 ? 2 : 1) k_cols_kspace(const __grid_constant__ KArgs a, Grid g0,
+__global__ void __launch_bounds__(128, 3) k_cols_kspace(const __grid_constant__ KArgs a, Grid g0,
                                                          const float2* __restrict__ tw) {
   extern __shared__ float2 sm[];
   Grid g = g0;
@@ -513,88 +516,98 @@ __global__ void __launch_bounds__(512, LOGN == 10 ? 2 : 1) k_cols_kspace(const _
   float2* const S0 = sm;             // E_x
   float2* const S1 = sm + slot;      // E_y
   float2* const S2 = sm + 2 * slot;  // E_z
-  float2* const S3 = sm + 3 * slot;  // J parking, then B_x(t)
-  float2* const S4 = sm + 4 * slot;  // rho parking, then B_y(t)
-  float2* const S5 = sm + 5 * slot;  // B_z(t); until then the forward exchange buffer
-  // the points this thread holds after a forward transform: (column pt(m), row py(m)),
-  // recomputed where used (shifts and masks) rather than kept in registers
+  float2* const S3 = sm + 3 * slot;  // B_x at t-1/2 (staged), then B_x(t)
+  float2* const S4 = sm + 4 * slot;  // B_y
+  float2* const S5 = sm + 5 * slot;  // B_z
+  float2* const X = sm + 6 * slot;   // exchange buffer of the forward transforms
+  {  // stage this strip of B_wrk: element (t, e) at spad(e W + t), as the transforms lay it out
+    const int npts = N << logW;
+    for (int q = threadIdx.x; q < npts; q += blockDim.x) {
+      const int e = q >> logW, t = q & (W - 1);
+      const size_t gi = (size_t)e * nx + x0 + t;
+      const int si = spad(e * W + t);
+      cp_async8(S3 + si, a.bwx + gi);
+      cp_async8(S4 + si, a.bwy + gi);
+      cp_async8(S5 + si, a.bwz + gi);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+  // the points this thread holds after a forward transform: (column pt(m), row py(m))
   auto pt = [&](int m) { int t, y; out_pos(m, logN, logW, true, t, y); return t; };
   auto py = [&](int m) { int t, y; out_pos(m, logN, logW, true, t, y); return y; };
-  int jt, jj;  // first-pass inputs: elements (jt, jj + r N/8)
-  bfly_tj<8>(0, logN, logW, true, jt, jj);
-  float2 v[8];
-  auto fwd = [&](const float2* __restrict__ src) {
-#pragma unroll
-    for (int r = 0; r < 8; ++r) v[r] = src[(size_t)(jj + r * (N >> 3)) * nx + x0 + jt];
-    block_fft_regs(v, S5, logN, logW, W, 1, true, tw);
-  };
   auto at = [&](int m) { return spad(py(m) * W + pt(m)); };
   auto gidx = [&](int m) { return (size_t)py(m) * nx + x0 + pt(m); };
-  const float cdt = a.cdt, ckc = a.ckc;
-  // each transform's outputs are parked at the thread's own points of a free slot, then the
-  // k-space update walks those points one at a time (the same thread wrote them: no barrier)
-  auto park = [&](float2* dst) {
+  int jt, jj;  // first-pass inputs: elements (jt, jj + r N/8)
+  bfly_tj<8>(0, logN, logW, true, jt, jj);
+  float2 v[8], nv[8];
+  auto load = [&](float2 (&d)[8], const float2* __restrict__ src) {
 #pragma unroll
-    for (int m = 0; m < 8; ++m) dst[at(m)] = v[m];
+    for (int r = 0; r < 8; ++r) d[r] = src[(size_t)(jj + r * (N >> 3)) * nx + x0 + jt];
   };
-  // Ampere (mod.rs:130-173); J_x, J_y are zeroed at k = 0, J_z is not (mod.rs:106-107)
-  fwd(a.ex);
-  park(S0);
+  // forward transform of the loaded field, loading the next one meanwhile
+  auto fwd = [&](const float2* __restrict__ next) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) v[r] = nv[r];
+    if (next) load(nv, next);
+    block_fft_regs(v, X, logN, logW, W, 1, true, tw);
+  };
+  const float cdt = a.cdt, ckc = a.ckc;
+  load(nv, a.ex);
   fwd(a.jx);
-  park(S3);
-#pragma unroll 1
+#pragma unroll
+  for (int m = 0; m < 8; ++m) S0[at(m)] = v[m];
+  fwd(a.ey);
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  __syncthreads();  // B_wrk staged by every thread
+  // Ampere (mod.rs:130-173); J_x, J_y are zeroed at k = 0, J_z is not (mod.rs:106-107)
+#pragma unroll
   for (int m = 0; m < 8; ++m) {
-    const size_t idx = gidx(m);
     const float ky = wave_kx(py(m), N);
-    const float2 Jx = idx == 0 ? make_float2(0.f, 0.f) : S3[at(m)];
-    const float2 Bz = a.bwz[idx];
+    const float2 Jx = gidx(m) == 0 ? make_float2(0.f, 0.f) : v[m];
+    const float2 Bz = S5[at(m)];
     S0[at(m)] = c_add(S0[at(m)], c_sub(c_mul(make_float2(0.0f * ky, cdt * ky), Bz), make_float2(ckc * Jx.x, ckc * Jx.y)));
   }
-  fwd(a.ey);
-  park(S1);
   fwd(a.jy);
-  park(S3);
-#pragma unroll 1
+#pragma unroll
+  for (int m = 0; m < 8; ++m) S1[at(m)] = v[m];
+  fwd(a.ez);
+#pragma unroll
   for (int m = 0; m < 8; ++m) {
-    const size_t idx = gidx(m);
     const float kx = wave_kx(x0 + pt(m), nx);
-    const float2 Jy = idx == 0 ? make_float2(0.f, 0.f) : S3[at(m)];
-    const float2 Bz = a.bwz[idx];
+    const float2 Jy = gidx(m) == 0 ? make_float2(0.f, 0.f) : v[m];
+    const float2 Bz = S5[at(m)];
     S1[at(m)] = c_add(S1[at(m)], c_sub(c_mul(make_float2(0.0f * kx, -cdt * kx), Bz), make_float2(ckc * Jy.x, ckc * Jy.y)));
   }
-  fwd(a.ez);
-  park(S2);
   fwd(a.jz);
-  park(S3);
-#pragma unroll 1
+#pragma unroll
+  for (int m = 0; m < 8; ++m) S2[at(m)] = v[m];
+  fwd(a.rho);
+#pragma unroll
   for (int m = 0; m < 8; ++m) {
-    const size_t idx = gidx(m);
     const float kx = wave_kx(x0 + pt(m), nx), ky = wave_kx(py(m), N);
-    const float2 Bx = a.bwx[idx], By = a.bwy[idx], Jz = S3[at(m)];
+    const float2 Bx = S3[at(m)], By = S4[at(m)], Jz = v[m];
     const float2 kb = c_sub(make_float2(kx * By.x, kx * By.y), make_float2(ky * Bx.x, ky * Bx.y));
     const float2 Ez = c_add(S2[at(m)], c_mul(make_float2(0.0f, cdt), kb));
     S2[at(m)] = c_sub(Ez, make_float2(ckc * Jz.x, ckc * Jz.y));
   }
-  fwd(a.rho);  // after this the exchange buffer S5 is free for B_z(t)
-  park(S4);
-#pragma unroll 1
+  fwd(nullptr);  // rho
+#pragma unroll
   for (int m = 0; m < 8; ++m) {
     const size_t idx = gidx(m);
     const int i = py(m), j = x0 + pt(m);
     const float kx = wave_kx(j, nx), ky = wave_kx(i, N);
-    const float2 Rho = S4[at(m)];
     float2 Ex = S0[at(m)], Ey = S1[at(m)], Ez = S2[at(m)];
     // divergence correction with k_norm = 1/k^2, k = 0 kept (mod.rs:177-207)
     if (idx != 0) {
       const float kn = 1.0f / (kx * kx + ky * ky);
       float2 t = c_add(c_add(make_float2(kx * Ex.x, kx * Ex.y), make_float2(ky * Ey.x, ky * Ey.y)),
-                       c_mul(make_float2(0.f, 1.f), Rho));
+                       c_mul(make_float2(0.f, 1.f), v[m]));
       t = c_scale(t, kn);
       Ex = c_sub(Ex, c_scale(t, kx));
       Ey = c_sub(Ey, c_scale(t, ky));
     }
     // Faraday to t+1/2 (mod.rs:211-225)
-    const float2 Bx = a.bwx[idx], By = a.bwy[idx], Bz = a.bwz[idx];
+    const float2 Bx = S3[at(m)], By = S4[at(m)], Bz = S5[at(m)];
     float2 nBx = c_sub(Bx, c_mul(make_float2(0.0f * ky, cdt * ky), Ez));
     float2 nBy = c_add(By, c_mul(make_float2(0.0f * kx, cdt * kx), Ez));
     float2 nBz = c_add(Bz, c_mul(make_float2(0.0f, cdt),
@@ -611,7 +624,7 @@ __global__ void __launch_bounds__(512, LOGN == 10 ? 2 : 1) k_cols_kspace(const _
     a.bwx[idx] = nBx;
     a.bwy[idx] = nBy;
     a.bwz[idx] = nBz;
-    // B at integer time (mod.rs:270-278); rho's parking place becomes B_y(t)
+    // B at integer time (mod.rs:270-278), in place of the staged B_wrk
     S3[at(m)] = c_scale(c_add(Bx, nBx), 0.5f);
     S4[at(m)] = c_scale(c_add(By, nBy), 0.5f);
     S5[at(m)] = c_scale(c_add(Bz, nBz), 0.5f);
@@ -931,9 +944,8 @@ void fields_set_kernel_attributes() {
   fft_set_kernel_attributes<0>();
   fft_attr((const void*)k_filter_fused);
   for (const void* f : {(const void*)k_cols_kspace<0>, (const void*)k_cols_kspace<6>, (const void*)k_cols_kspace<7>,
-                        (const void*)k_cols_kspace<8>, (const void*)k_cols_kspace<9>, (const void*)k_cols_kspace<10>,
-                        (const void*)k_cols_kspace<11>, (const void*)k_cols_kspace<12>})
-    SPX_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+                        (const void*)k_cols_kspace<8>, (const void*)k_cols_kspace<9>, (const void*)k_cols_kspace<10>})
+    SPX_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
 }
 
 template <int IN, int OUT, bool INV, int LOGN>
@@ -1007,8 +1019,6 @@ static void launch_cols_kspace(const Grid& g, const KArgs& k, const float2* tw, 
     case 8: launch_cols_kspace_n<8>(g, k, tw, st); break;
     case 9: launch_cols_kspace_n<9>(g, k, tw, st); break;
     case 10: launch_cols_kspace_n<10>(g, k, tw, st); break;
-    case 11: launch_cols_kspace_n<11>(g, k, tw, st); break;
-    case 12: launch_cols_kspace_n<12>(g, k, tw, st); break;
     default: launch_cols_kspace_n<0>(g, k, tw, st); break;
   }
 }
@@ -1103,7 +1113,7 @@ int field_update(FieldBuffers& fb, cudaStream_t st) {
     // transforms of B(t) and E in one pass over column strips
     launch_cols_kspace(g, k, fb.tw_y, st);
     ++launches;
-  } else {  // 8192-point columns: the same as three passes
+  } else {  // columns of 2048 points and more: the same as three passes
     const int fwd_ids[7] = {SP_JX, SP_JY, SP_JZ, SP_RHO, SP_EX, SP_EY, SP_EZ};
     ColArgs c{};
     for (int i = 0; i < 7; ++i) c.data[i] = fb.spec[fwd_ids[i]];
