@@ -15,7 +15,7 @@ Sources (paths relative to the reference project):
   src/lib.rs          build_test_sim (:219-244): 24x12 grid, dt 0.1, delta 5,
                       c 3, dens 2, gamma_inj 5, n_pass 4; E_TOL (:28-32)
 
-Usage:  python tests/golden/extract_golden.py [/path/to/reference]
+Usage:  python tests/golden/extract_golden.py /path/to/spectral_rs  (the reference checkout; required)
 """
 import json
 import os
@@ -126,4 +126,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/extract_golden.py /path/to/spectral_rs")
+    main(sys.argv[1])
