@@ -178,14 +178,28 @@ def traffic_per_launch(particles, cells, name="k_slot_traffic.json"):
         return None
 
 
+def profile_counters(name):
+    """Counters of the committed ncu capture of a kernel (profiles/<name>), or {}."""
+    try:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
 def roofline(particles, cells, kern_ms, kernel, traffic_file):
     peak, peak_kind = measured_peak()
     alg = B_PER_PARTICLE * particles + B_PER_CELL * cells
     achieved = alg / (kern_ms / 1e3) / 1e9
+    prof = profile_counters(traffic_file)
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic_per_launch(particles, cells, traffic_file), "peak_kind": peak_kind,
             "kernel": kernel, "kernel_ms": kern_ms, "alg_bytes_per_launch": alg,
-            "alg_bytes": f"{B_PER_PARTICLE:g} B x {particles} particles + {B_PER_CELL:g} B x {cells} cells"}
+            "alg_bytes": f"{B_PER_PARTICLE:g} B x {particles} particles + {B_PER_CELL:g} B x {cells} cells",
+            # from the committed ncu capture (smsp__inst_executed / particles, and the lane
+            # efficiency smsp__thread_inst_executed_per_inst_executed / 32)
+            "warp_inst_per_particle": prof.get("warp_inst_per_particle"),
+            "lane_efficiency": prof.get("lane_efficiency"), "counters_from": prof.get("source")}
 
 
 def _events(stream):
