@@ -474,177 +474,6 @@ __global__ void k_kspace(KArgs a, Grid g) {
   }
 }
 
-// ---------------------------------------------------------------- fused column pass
-// The column half of Flds::update (src/flds/mod.rs:101-307 between the row passes) in one
-// kernel per strip of W columns: the forward column transforms of J, rho and E, the k-space
-// update (Ampere, divergence correction, Faraday, Nyquist, B average: the expressions of
-// k_kspace) and the inverse column transforms of B(t) and E.  A thread holds the same 8
-// points of the strip after every forward transform, so the k-space update runs on them
-// as each field arrives, from shared memory only: E waits in three strip slots, B_wrk is
-// staged into three more by asynchronous copies issued at the start (they land while the
-// first transforms run) and is replaced there by B(t); a seventh slot is the transforms'
-// exchange buffer.  The next field's inputs are loaded while the current one transforms.
-// Per cell it reads 7 + 3 and writes 3 + 6 complex values: 152 B against 360 B for the
-// three separate passes.  Strips of 1024 points (128 threads, 61 KB: three CTAs per SM);
-// columns longer than 1024 points take the three-kernel path.
-constexpr int FUSED_SLOTS = 7;
-__host__ __device__ inline int fused_logW(int logNy, int logNx) {
-  int lw = 10 - logNy;
-  if (lw < 0) lw = 0;
-  return lw > logNx ? logNx : lw;
-}
-bool cols_fused_fits(int logNy) { return logNy <= 10; }
-
-__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gmem_src) : "memory");
-}
-
-template <int LOGN>
-__global__ void __launch_bounds__(128, 3) k_cols_kspace(const __grid_constant__ KArgs a, Grid g0,
-                                                         const float2* __restrict__ tw) {
-  extern __shared__ float2 sm[];
-  Grid g = g0;
-  if (LOGN) {
-    g.log2ny = LOGN;
-    g.ny = 1 << LOGN;
-  }
-  const int logN = g.log2ny, N = g.ny, nx = g.nx;
-  const int logW = fused_logW(logN, g.log2nx), W = 1 << logW;
-  const int x0 = blockIdx.x << logW;
-  const size_t slot = fft_smem_elems(logN, logW);
-  float2* const S0 = sm;             // E_x
-  float2* const S1 = sm + slot;      // E_y
-  float2* const S2 = sm + 2 * slot;  // E_z
-  float2* const S3 = sm + 3 * slot;  // B_x at t-1/2 (staged), then B_x(t)
-  float2* const S4 = sm + 4 * slot;  // B_y
-  float2* const S5 = sm + 5 * slot;  // B_z
-  float2* const X = sm + 6 * slot;   // exchange buffer of the forward transforms
-  {  // stage this strip of B_wrk: element (t, e) at spad(e W + t), as the transforms lay it out
-    const int npts = N << logW;
-    for (int q = threadIdx.x; q < npts; q += blockDim.x) {
-      const int e = q >> logW, t = q & (W - 1);
-      const size_t gi = (size_t)e * nx + x0 + t;
-      const int si = spad(e * W + t);
-      cp_async8(S3 + si, a.bwx + gi);
-      cp_async8(S4 + si, a.bwy + gi);
-      cp_async8(S5 + si, a.bwz + gi);
-    }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-  }
-  // the points this thread holds after a forward transform: (column pt(m), row py(m))
-  auto pt = [&](int m) { int t, y; out_pos(m, logN, logW, true, t, y); return t; };
-  auto py = [&](int m) { int t, y; out_pos(m, logN, logW, true, t, y); return y; };
-  auto at = [&](int m) { return spad(py(m) * W + pt(m)); };
-  auto gidx = [&](int m) { return (size_t)py(m) * nx + x0 + pt(m); };
-  int jt, jj;  // first-pass inputs: elements (jt, jj + r N/8)
-  bfly_tj<8>(0, logN, logW, true, jt, jj);
-  float2 v[8], nv[8];
-  auto load = [&](float2 (&d)[8], const float2* __restrict__ src) {
-#pragma unroll
-    for (int r = 0; r < 8; ++r) d[r] = src[(size_t)(jj + r * (N >> 3)) * nx + x0 + jt];
-  };
-  // forward transform of the loaded field, loading the next one meanwhile
-  auto fwd = [&](const float2* __restrict__ next) {
-#pragma unroll
-    for (int r = 0; r < 8; ++r) v[r] = nv[r];
-    if (next) load(nv, next);
-    block_fft_regs(v, X, logN, logW, W, 1, true, tw);
-  };
-  const float cdt = a.cdt, ckc = a.ckc;
-  load(nv, a.ex);
-  fwd(a.jx);
-#pragma unroll
-  for (int m = 0; m < 8; ++m) S0[at(m)] = v[m];
-  fwd(a.ey);
-  asm volatile("cp.async.wait_group 0;" ::: "memory");
-  __syncthreads();  // B_wrk staged by every thread
-  // Ampere (mod.rs:130-173); J_x, J_y are zeroed at k = 0, J_z is not (mod.rs:106-107)
-#pragma unroll
-  for (int m = 0; m < 8; ++m) {
-    const float ky = wave_kx(py(m), N);
-    const float2 Jx = gidx(m) == 0 ? make_float2(0.f, 0.f) : v[m];
-    const float2 Bz = S5[at(m)];
-    S0[at(m)] = c_add(S0[at(m)], c_sub(c_mul(make_float2(0.0f * ky, cdt * ky), Bz), make_float2(ckc * Jx.x, ckc * Jx.y)));
-  }
-  fwd(a.jy);
-#pragma unroll
-  for (int m = 0; m < 8; ++m) S1[at(m)] = v[m];
-  fwd(a.ez);
-#pragma unroll
-  for (int m = 0; m < 8; ++m) {
-    const float kx = wave_kx(x0 + pt(m), nx);
-    const float2 Jy = gidx(m) == 0 ? make_float2(0.f, 0.f) : v[m];
-    const float2 Bz = S5[at(m)];
-    S1[at(m)] = c_add(S1[at(m)], c_sub(c_mul(make_float2(0.0f * kx, -cdt * kx), Bz), make_float2(ckc * Jy.x, ckc * Jy.y)));
-  }
-  fwd(a.jz);
-#pragma unroll
-  for (int m = 0; m < 8; ++m) S2[at(m)] = v[m];
-  fwd(a.rho);
-#pragma unroll
-  for (int m = 0; m < 8; ++m) {
-    const float kx = wave_kx(x0 + pt(m), nx), ky = wave_kx(py(m), N);
-    const float2 Bx = S3[at(m)], By = S4[at(m)], Jz = v[m];
-    const float2 kb = c_sub(make_float2(kx * By.x, kx * By.y), make_float2(ky * Bx.x, ky * Bx.y));
-    const float2 Ez = c_add(S2[at(m)], c_mul(make_float2(0.0f, cdt), kb));
-    S2[at(m)] = c_sub(Ez, make_float2(ckc * Jz.x, ckc * Jz.y));
-  }
-  fwd(nullptr);  // rho
-#pragma unroll
-  for (int m = 0; m < 8; ++m) {
-    const size_t idx = gidx(m);
-    const int i = py(m), j = x0 + pt(m);
-    const float kx = wave_kx(j, nx), ky = wave_kx(i, N);
-    float2 Ex = S0[at(m)], Ey = S1[at(m)], Ez = S2[at(m)];
-    // divergence correction with k_norm = 1/k^2, k = 0 kept (mod.rs:177-207)
-    if (idx != 0) {
-      const float kn = 1.0f / (kx * kx + ky * ky);
-      float2 t = c_add(c_add(make_float2(kx * Ex.x, kx * Ex.y), make_float2(ky * Ey.x, ky * Ey.y)),
-                       c_mul(make_float2(0.f, 1.f), v[m]));
-      t = c_scale(t, kn);
-      Ex = c_sub(Ex, c_scale(t, kx));
-      Ey = c_sub(Ey, c_scale(t, ky));
-    }
-    // Faraday to t+1/2 (mod.rs:211-225)
-    const float2 Bx = S3[at(m)], By = S4[at(m)], Bz = S5[at(m)];
-    float2 nBx = c_sub(Bx, c_mul(make_float2(0.0f * ky, cdt * ky), Ez));
-    float2 nBy = c_add(By, c_mul(make_float2(0.0f * kx, cdt * kx), Ez));
-    float2 nBz = c_add(Bz, c_mul(make_float2(0.0f, cdt),
-                                 c_sub(make_float2(ky * Ex.x, ky * Ex.y), make_float2(kx * Ey.x, kx * Ey.y))));
-    // Nyquist column kx = nx/2 and row ky = ny/2 (mod.rs:230-266)
-    if (j == nx / 2 || i == N / 2) {
-      const float2 z = make_float2(0.f, 0.f);
-      nBx = nBy = nBz = z;
-      Ex = Ey = Ez = z;
-    }
-    S0[at(m)] = Ex;
-    S1[at(m)] = Ey;
-    S2[at(m)] = Ez;
-    a.bwx[idx] = nBx;
-    a.bwy[idx] = nBy;
-    a.bwz[idx] = nBz;
-    // B at integer time (mod.rs:270-278), in place of the staged B_wrk
-    S3[at(m)] = c_scale(c_add(Bx, nBx), 0.5f);
-    S4[at(m)] = c_scale(c_add(By, nBy), 0.5f);
-    S5[at(m)] = c_scale(c_add(Bz, nBz), 0.5f);
-  }
-  __syncthreads();
-  // inverse column transforms (ifft(x) = conj(fft(conj(x)))), each slot its own exchange buffer
-  float2* const src[6] = {S3, S4, S5, S0, S1, S2};
-  float2* const dst[6] = {a.bax, a.bay, a.baz, a.ex, a.ey, a.ez};
-#pragma unroll 1
-  for (int f = 0; f < 6; ++f) {
-#pragma unroll
-    for (int r = 0; r < 8; ++r) v[r] = c_conj(src[f][spad((jj + r * (N >> 3)) * W + jt)]);
-    __syncthreads();  // every thread holds its inputs before the slot is overwritten
-    block_fft_regs(v, src[f], logN, logW, W, 1, true, tw);
-    float2* __restrict__ d = dst[f];
-#pragma unroll
-    for (int m = 0; m < 8; ++m) d[gidx(m)] = c_conj(v[m]);
-  }
-}
-
 // ---------------------------------------------------------------- ghost frame kernels
 struct FieldList {
   float* f[SPX_NUM_FIELDS];
@@ -943,9 +772,6 @@ static void fft_set_kernel_attributes() {
 void fields_set_kernel_attributes() {
   fft_set_kernel_attributes<0>();
   fft_attr((const void*)k_filter_fused);
-  for (const void* f : {(const void*)k_cols_kspace<0>, (const void*)k_cols_kspace<6>, (const void*)k_cols_kspace<7>,
-                        (const void*)k_cols_kspace<8>, (const void*)k_cols_kspace<9>, (const void*)k_cols_kspace<10>})
-    SPX_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
 }
 
 template <int IN, int OUT, bool INV, int LOGN>
@@ -1002,25 +828,6 @@ static void launch_cols(const Grid& g, const ColArgs& a, int nf, const float2* t
 #define SPX_COLS(L) launch_cols_n<INV, L>(g, a, nf, tw, st)
   FFT_DISPATCH(g.log2ny, SPX_COLS)
 #undef SPX_COLS
-}
-
-template <int LOGN>
-static void launch_cols_kspace_n(const Grid& g, const KArgs& k, const float2* tw, cudaStream_t st) {
-  const int logW = fused_logW(g.log2ny, g.log2nx);
-  const int threads = std::max(1, (g.ny << logW) / 8);
-  const size_t smem = sizeof(float2) * FUSED_SLOTS * fft_smem_elems(g.log2ny, logW);
-  k_cols_kspace<LOGN><<<g.nx >> logW, threads, smem, st>>>(k, g, tw);
-}
-
-static void launch_cols_kspace(const Grid& g, const KArgs& k, const float2* tw, cudaStream_t st) {
-  switch (g.log2ny) {
-    case 6: launch_cols_kspace_n<6>(g, k, tw, st); break;
-    case 7: launch_cols_kspace_n<7>(g, k, tw, st); break;
-    case 8: launch_cols_kspace_n<8>(g, k, tw, st); break;
-    case 9: launch_cols_kspace_n<9>(g, k, tw, st); break;
-    case 10: launch_cols_kspace_n<10>(g, k, tw, st); break;
-    default: launch_cols_kspace_n<0>(g, k, tw, st); break;
-  }
 }
 
 void FieldBuffers::allocate(const Grid& grid) {
@@ -1099,35 +906,33 @@ int field_update(FieldBuffers& fb, cudaStream_t st) {
     a.scale[3] = 1.0f / (float)fb.dens;
     launch_rows<0, 0, false>(g, a, 7, fb.tw_x, st);
     ++launches;
-  }
-  KArgs k;
-  k.jx = fb.spec[SP_JX]; k.jy = fb.spec[SP_JY]; k.jz = fb.spec[SP_JZ]; k.rho = fb.spec[SP_RHO];
-  k.ex = fb.spec[SP_EX]; k.ey = fb.spec[SP_EY]; k.ez = fb.spec[SP_EZ];
-  k.bwx = fb.spec[SP_BWX]; k.bwy = fb.spec[SP_BWY]; k.bwz = fb.spec[SP_BWZ];
-  k.bax = fb.spec[SP_BAX]; k.bay = fb.spec[SP_BAY]; k.baz = fb.spec[SP_BAZ];
-  k.ckc = fb.dt / (float)fb.dens;  // mod.rs:127
-  k.cdt = fb.dt * fb.c;            // mod.rs:128
-  const int spec_ids[6] = {SP_BAX, SP_BAY, SP_BAZ, SP_EX, SP_EY, SP_EZ};
-  if (cols_fused_fits(g.log2ny)) {
-    // 3. forward column transforms, k-space update (mod.rs:105-278) and inverse column
-    // transforms of B(t) and E in one pass over column strips
-    launch_cols_kspace(g, k, fb.tw_y, st);
-    ++launches;
-  } else {  // columns of 2048 points and more: the same as three passes
-    const int fwd_ids[7] = {SP_JX, SP_JY, SP_JZ, SP_RHO, SP_EX, SP_EY, SP_EZ};
     ColArgs c{};
-    for (int i = 0; i < 7; ++i) c.data[i] = fb.spec[fwd_ids[i]];
+    for (int i = 0; i < 7; ++i) c.data[i] = fb.spec[dst_ids[i]];
     launch_cols<false>(g, c, 7, fb.tw_y, st);
-    const size_t n = g.spectral_size();
-    k_kspace<<<(int)std::min<size_t>((n + 255) / 256, 148 * 16), 256, 0, st>>>(k, g);
-    ColArgs ci{};
-    for (int i = 0; i < 6; ++i) ci.data[i] = fb.spec[spec_ids[i]];
-    launch_cols<true>(g, ci, 6, fb.tw_y, st);
-    launches += 3;
+    ++launches;
   }
-  // 4. inverse row transforms, 1/(nx ny), back to the spatial fields with their ghosts (mod.rs:281-307)
+  // 3. k-space update (mod.rs:105-278)
   {
+    KArgs k;
+    k.jx = fb.spec[SP_JX]; k.jy = fb.spec[SP_JY]; k.jz = fb.spec[SP_JZ]; k.rho = fb.spec[SP_RHO];
+    k.ex = fb.spec[SP_EX]; k.ey = fb.spec[SP_EY]; k.ez = fb.spec[SP_EZ];
+    k.bwx = fb.spec[SP_BWX]; k.bwy = fb.spec[SP_BWY]; k.bwz = fb.spec[SP_BWZ];
+    k.bax = fb.spec[SP_BAX]; k.bay = fb.spec[SP_BAY]; k.baz = fb.spec[SP_BAZ];
+    k.ckc = fb.dt / (float)fb.dens;  // mod.rs:127
+    k.cdt = fb.dt * fb.c;            // mod.rs:128
+    const size_t n = g.spectral_size();
+    int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+    k_kspace<<<blocks, 256, 0, st>>>(k, g);
+    ++launches;
+  }
+  // 4. inverse transforms of B(t) and E, back to the spatial fields (mod.rs:281-307)
+  {
+    const int spec_ids[6] = {SP_BAX, SP_BAY, SP_BAZ, SP_EX, SP_EY, SP_EZ};
     const int sp_ids[6] = {SPX_BX, SPX_BY, SPX_BZ, SPX_EX, SPX_EY, SPX_EZ};
+    ColArgs c{};
+    for (int i = 0; i < 6; ++i) c.data[i] = fb.spec[spec_ids[i]];
+    launch_cols<true>(g, c, 6, fb.tw_y, st);
+    ++launches;
     RowArgs a{};
     const float norm = 1.0f / (float)((uint64_t)g.nx * (uint64_t)g.ny);  // fft_2d.rs:170
     for (int i = 0; i < 6; ++i) {

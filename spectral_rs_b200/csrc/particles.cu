@@ -11,29 +11,10 @@
 #include <algorithm>
 
 #include "particles.cuh"
-#include "exact_math.cuh"
 
 namespace spx {
 
 // ---------------------------------------------------------------- per-particle maths
-#ifndef SPX_FASTRCP
-#define SPX_FASTRCP 0  // 1: reciprocal and sqrt of the push from exact_math.cuh (IEEE-equal on its domain)
-#endif
-// 1/x and sqrt(x) with IEEE round-to-nearest results (the reference's powi(-1) and sqrt)
-__device__ __forceinline__ float p_rcp(float x) {
-#if SPX_FASTRCP
-  return rcp_exact(x);
-#else
-  return 1.0f / x;
-#endif
-}
-__device__ __forceinline__ float p_sqrt(float x) {
-#if SPX_FASTRCP
-  return sqrt_exact(x);
-#else
-  return sqrtf(x);
-#endif
-}
 // Second-order (TSC) weights, src/lib.rs:339-347, left-to-right as in Rust.
 __device__ __forceinline__ void tsc_weights(float dx, float dy, float (&w)[9]) {
   w[0] = 0.5f * (0.5f - dy) * (0.5f - dy) * 0.5f * (0.5f - dx) * (0.5f - dx);
@@ -159,11 +140,11 @@ __device__ __forceinline__ void boris(const float (&g)[6], float beta, float alp
   const float2 bxy = mul2(make_float2(g[3], g[4]), bc2(alpha));
   const float ux = px + exy.x, uy = py + exy.y, uz = pz + ezt;
   const float2 uu = mul2(make_float2(ux, uy), make_float2(ux, uy));
-  const float gt = p_rcp(p_sqrt(1.0f + (uu.x + uu.y + uz * uz) * csqinv));
+  const float gt = 1.0f / sqrtf(1.0f + (uu.x + uu.y + uz * uz) * csqinv);
   const float2 bt = mul2(bxy, bc2(gt));  // (bxt, byt)
   const float bxt = bt.x, byt = bt.y, bzt = (g[5] * alpha) * gt;
   const float2 bb = mul2(bt, bt);
-  const float boris = 2.0f * p_rcp(1.0f + bb.x + bb.y + bzt * bzt);
+  const float boris = 2.0f * (1.0f / (1.0f + bb.x + bb.y + bzt * bzt));
   // u' = u + u x B
   const float2 p1 = mul2(make_float2(uy, uz), make_float2(bzt, bxt));  // (uy bzt, uz bxt)
   const float2 p2 = mul2(make_float2(uz, ux), make_float2(byt, bzt));  // (uz byt, ux bzt)
@@ -181,12 +162,12 @@ __device__ __forceinline__ void boris(const float (&g)[6], float beta, float alp
   py = uy + bxy2.y + exy.y;
   pz = uz + bz2 + ezt;
   const float2 pp = mul2(make_float2(px, py), make_float2(px, py));
-  psa = p_sqrt(1.0f + (pp.x + pp.y + pz * pz) * csqinv);
+  psa = sqrtf(1.0f + (pp.x + pp.y + pz * pz) * csqinv);
 }
 
 __device__ __forceinline__ float gamma_of(float px, float py, float pz, float csqinv) {
   const float2 pp = mul2(make_float2(px, py), make_float2(px, py));
-  return p_sqrt(1.0f + (pp.x + pp.y + pz * pz) * csqinv);  // src/prtls.rs:440
+  return sqrtf(1.0f + (pp.x + pp.y + pz * pz) * csqinv);  // src/prtls.rs:440
 }
 
 // update_position (src/prtls.rs:103-119) for one particle; inv = 1/psa.
@@ -672,7 +653,7 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
           spy[idx] = py;
           spz[idx] = pz;
         } else {
-          const float inv = p_rcp(psa);
+          const float inv = 1.0f / psa;
           const float c1 = half_dt * inv;
           // first half: position, boundaries, current (src/lib.rs:480-484)
           move_half(c1, px, py, ix, iy, dx, dy);
@@ -1016,7 +997,7 @@ __device__ __forceinline__ void slot_overflow(const StepArgs& a, int s) {
       continue;
     }
     const float q = S.charge;
-    const float inv = p_rcp(psa);
+    const float inv = 1.0f / psa;
     const float c1 = 0.5f * a.p.dt * inv;
     move_half(c1, px, py, ix, iy, dx, dy);
     apply_bc(a.p, nx, ny, ix, iy, dx, px, a.derr);
@@ -1534,7 +1515,7 @@ __global__ void k_plain_move_deposit(PlainSpecies P, uint64_t n, float q, Grid g
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     float x = P.x[i], y = P.y[i], px = P.px[i], py = P.py[i], pz = P.pz[i];
     const float psa = gamma_of(px, py, pz, p.csqinv);
-    const float inv = p_rcp(psa);
+    const float inv = 1.0f / psa;
     const float c1 = 0.5f * p.dt * inv;
     x += c1 * px;
     y += c1 * py;

@@ -25,6 +25,7 @@ sys.path.insert(0, ROOT)
 
 STUDY = dict(size_x=128, size_y=128, delta=0, dt=0.1, c=3.0, dens=64, gamma_inj=1.0206207261596576, n_pass=4,
              periodic_x=True, ppc=32, vth=0.01, steps=2000, every=10, seed=33)
+OUT = "two_stream_energy.json"
 
 
 def beams(study):
@@ -64,13 +65,20 @@ def run_oracle(dtype):
 
 
 def main():
+    # optional: a larger crop, e.g. `python tests/golden/make_two_stream.py 512`
+    # writes two_stream_energy_512.json (the same plasma on 512 x 512 cells)
+    global OUT
+    if len(sys.argv) > 1:
+        n = int(sys.argv[1])
+        STUDY.update(size_x=n, size_y=n)
+        OUT = f"two_stream_energy_{n}.json"
     t0 = time.time()
     out = {"study": STUDY}
     for name, dt in (("fp64", np.float64), ("fp32", np.float32)):
         h = run_oracle(dt)
         out[name] = {"E": [x[0] for x in h], "B": [x[1] for x in h]}
         print(name, "done", round(time.time() - t0, 1), "s", flush=True)
-    with open(os.path.join(HERE, "two_stream_energy.json"), "w") as f:
+    with open(os.path.join(HERE, OUT), "w") as f:
         json.dump(out, f)
 
 
