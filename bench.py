@@ -725,7 +725,7 @@ def run_ensemble(args):
                                "drift_beta": [round(members[i]["beta"], 4) for i in idx],
                                "vth": 0.1, "c": 3.0, "dt": 0.1, "n_pass": 4, "delta": 8, "walls": "right + left",
                                "path": "split, batched (persistent work-queue particle kernel, one graph per step)",
-                               "tile": list(tile) if tile else [16, 16],
+                               "tile": list(tile) if tile else [8, 8],
                                "parallelism": f"member list partitioned over {world} ranks" if world > 1 else "single",
                                "l2": _l2_note(r["particles"])})
         line.update({"roofline": r["roofline"], "phase_ms_per_step": r["phase_ms_per_step"], "plain_fp32": plain,

@@ -234,7 +234,7 @@ SPX_API uint64_t spx_last_launch_count(const spx_ctx* ctx);
  * spx_batch_sim returns the context of simulation i, used as any spx_ctx for
  * species set-up (spx_add_species / spx_init_species) and for getters; after
  * spx_batch_prepare the simulations must only be stepped through the batch.
- * All simulations use the same tile shape (16 x 16 unless params set one). */
+ * All simulations use the same tile shape (8 x 8 unless params set one). */
 typedef struct spx_batch spx_batch;
 SPX_API int spx_batch_create(int32_t n_sims, const spx_params* params, spx_batch** out);
 SPX_API int spx_batch_destroy(spx_batch* batch);

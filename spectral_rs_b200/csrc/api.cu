@@ -1268,7 +1268,9 @@ extern "C" int spx_batch_create(int32_t n, const spx_params* params, spx_batch**
       spx_params p = params[i];
       if (p.path == SPX_PATH_PLAIN) throw spx::Error(SPX_ERR_ARG, "a batch runs the split path");
       if (p.compensated) throw spx::Error(SPX_ERR_ARG, "compensated currents are a single-simulation option");
-      if (p.tile_x <= 0 && p.tile_y <= 0) p.tile_x = p.tile_y = 16;  // one tile shape for the whole batch
+      // one tile shape for the whole batch: 8 x 8 (measured on the 64-shock ensemble: 3 % faster
+      // than 16 x 16; smaller CTAs wait less for their slowest warp at the tile's barriers)
+      if (p.tile_x <= 0 && p.tile_y <= 0) p.tile_x = p.tile_y = 8;
       spx_ctx* c = nullptr;
       int rc = spx_create(&p, &c);
       if (rc) throw spx::Error(rc, std::string("simulation ") + std::to_string(i) + ": " + g_create_err);

@@ -362,19 +362,6 @@ __host__ __device__ inline size_t slot_smem_floats(int TX, int TY, bool push, bo
   return win + eb + q;
 }
 
-// Shared memory of one warp unit (slot_tile with WU): windows of 32/TX tile rows, its
-// queues; a multiple of 4 floats so that every unit's float4 window stays 16-byte aligned.
-__host__ __device__ inline size_t slot_unit_floats(int TX, bool push, bool move, bool comp = false) {
-  const int SR = 32 / TX;
-  const size_t win = (size_t)win_planes(move, comp) * (TX + 4) * (SR + 4);
-  const size_t eb = push ? eb_floats(TX, SR) : 0;
-  const size_t q = move ? (size_t)QWARP : 0;
-  return (win + eb + q + 3) & ~(size_t)3;
-}
-#ifndef SPX_WARP_UNITS
-#define SPX_WARP_UNITS 0  // 1: particle kernels work in warp units (see slot_tile)
-#endif
-
 // The queue drains run rarely (once per ~32 queued particles of a warp); as
 // separate functions they keep their registers out of the main loop's budget.
 __device__ __noinline__ void drain_j_fn(const StepArgs& a, const float* qj, int nq, int lane, float* win, int WX,
@@ -464,26 +451,14 @@ __device__ __forceinline__ void bc_of(const StepArgs& a, int nx, int ny, int& ix
 // BC: see bc_of.  T16: tiles of 16 x 16 cells (compile-time index arithmetic; else from a).
 // Species [s0, s1) of the step (all of them, or one per CTA when a small grid
 // splits the species across CTAs).
-// WU: the work unit is one warp's 32 consecutive cells of the tile (`unit` selects them:
-// tile rows [unit * 32/TX, (unit + 1) * 32/TX)), with its own E/B window, deposit window and
-// queues at `smem`, synchronized by the warp alone; else the whole tile, one thread per cell,
-// synchronized by the CTA (unit is then 0).
-template <bool PUSH, bool MOVE, bool COMP = false, int BC = BC_ANY, bool T16 = false, bool WU = false>
+template <bool PUSH, bool MOVE, bool COMP = false, int BC = BC_ANY, bool T16 = false>
 __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, float* smem, const int s0,
-                                          const int s1, const int unit = 0) {
+                                          const int s1) {
   const int TXc = T16 ? 16 : a.TX, TYc = T16 ? 16 : a.TY, logTXc = T16 ? 4 : a.logTX;
   const int TC = TXc * TYc;
   const int tx = tile % a.NTX, ty = tile / a.NTX;
-  const int lane = threadIdx.x & 31, warp = WU ? 0 : threadIdx.x >> 5;
-  const int c = WU ? unit * 32 + lane : threadIdx.x;  // cell within the tile
-  const int u = WU ? lane : threadIdx.x, US = WU ? 32 : TC;  // thread within the unit, unit size
-  const int ry0 = WU ? (unit * 32) >> logTXc : 0, SR = WU ? 32 >> logTXc : TYc;  // the unit's tile rows
-  auto unit_sync = [&]() {
-    if (WU)
-      __syncwarp();
-    else
-      __syncthreads();
-  };
+  const int c = threadIdx.x;
+  const int lane = c & 31, warp = c >> 5;
   const int lx = c & (TXc - 1), ly = c >> logTXc;
   const int ox = tx * TXc + lx + 1, oy = ty * TYc + ly + 1;  // owner cell (reference coords)
   const int W = a.g.W, nx = a.g.nx, ny = a.g.ny;
@@ -498,9 +473,9 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
     const bool in_x = px_ ? (X0 - 2 >= 1 && X1 + 2 <= nx) : (X0 - 2 >= a.p.delta + 2 && X1 + 2 <= a.p.wall_loc - 1);
     inner_tile = in_x && Y0 - 2 >= 1 && Y1 + 2 <= ny;
   }
-  // deposit window: the unit + 2 cells
-  const int WX = TXc + 4, WY = SR + 4, WN = WX * WY;
-  const int wx0 = tx * TXc + 1 - 2, wy0 = ty * TYc + ry0 + 1 - 2;
+  // deposit window: tile + 2 cells
+  const int WX = TXc + 4, WY = TYc + 4, WN = WX * WY;
+  const int wx0 = tx * TXc + 1 - 2, wy0 = ty * TYc + 1 - 2;
   float* win = smem;
   float* wjx = win;
   float* wjy = win + WN;
@@ -508,8 +483,8 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
   float* wrho = win + 3 * WN;
   float* wdens = win + 4 * WN;
   constexpr int NWP = MOVE ? (COMP ? 8 : 5) : 0;  // deposit window planes
-  // E/B window: the unit + 1 cell
-  const int EX = TXc + 2, EY = SR + 2;
+  // E/B window: tile + 1 cell
+  const int EX = TXc + 2, EY = TYc + 2;
   float4* eb4 = reinterpret_cast<float4*>(smem + NWP * WN);  // 16-byte aligned: WN is a multiple of 4
   float2* eb2 = reinterpret_cast<float2*>(eb4 + EX * EY);
   float* after_eb = smem + NWP * WN + (PUSH ? 6 * EX * EY : 0);
@@ -517,17 +492,17 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
   float* qj = qbase;                   // [QWORDS][QCAP]
   float* qm = qbase + QWORDS * QCAP;   // [QWORDS][QCAP]
   if (MOVE)
-    for (int i = u; i < NWP * WN; i += US) win[i] = 0.f;
+    for (int i = c; i < NWP * WN; i += TC) win[i] = 0.f;
   if (PUSH) {
-    for (int i = u; i < EY * EX; i += US) {
+    for (int i = c; i < EY * EX; i += TC) {
       const int r = i / EX, q = i - r * EX;
-      const size_t g = (size_t)(ty * TYc + ry0 + r) * W + (tx * TXc + q);
+      const size_t g = (size_t)(ty * TYc + r) * W + (tx * TXc + q);
       eb4[i] = make_float4(__ldg(a.f.E[0] + g), __ldg(a.f.E[1] + g), __ldg(a.f.E[2] + g), __ldg(a.f.B[0] + g));
       eb2[i] = make_float2(__ldg(a.f.B[1] + g), __ldg(a.f.B[2] + g));
     }
   }
-  unit_sync();
-  const int ebo = (ly - ry0) * EX + lx;  // top-left of this cell's 3x3 neighbourhood
+  __syncthreads();
+  const int ebo = ly * EX + lx;  // top-left of this cell's 3x3 neighbourhood
   float2 accJxy[9];
   float accJz[9];
   float2 cmpJxy[9];  // compensation terms (COMP): the low-order bits the running sums lost
@@ -829,9 +804,9 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
         }
       }
   }
-  unit_sync();
+  __syncthreads();
   // window -> global (clipped to the ghosted grid)
-  for (int i = u; i < 5 * WN; i += US) {
+  for (int i = c; i < 5 * WN; i += TC) {
     float v = win[i];
     if (COMP && i < 3 * WN) v += win[i + 5 * WN];  // one rounding of sum + compensation
     if (v == 0.f) continue;
@@ -853,16 +828,6 @@ __global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS) k_slot(const __grid_
   slot_tile<PUSH, MOVE, false, BC, T16>(a, blockIdx.x, smem, s0, s1);
 }
 
-// One simulation, warp units: CTA = tile, warp w = the tile's cells [32w, 32w + 32), no CTA barrier.
-template <bool PUSH, bool MOVE, int BC, bool T16>
-__global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS) k_slot_wu(const __grid_constant__ StepArgs a) {
-  extern __shared__ float smem[];
-  const int s0 = gridDim.y > 1 ? (int)blockIdx.y : 0, s1 = gridDim.y > 1 ? s0 + 1 : a.ns;
-  const int w = threadIdx.x >> 5;
-  const size_t uf = slot_unit_floats(T16 ? 16 : a.TX, PUSH, MOVE);
-  slot_tile<PUSH, MOVE, false, BC, T16, true>(a, blockIdx.x, smem + w * uf, s0, s1, w);
-}
-
 // Compensated current sums: the extra registers allow one 256-thread CTA per SM.
 template <bool PUSH, int BC>
 __global__ void __launch_bounds__(256, 1) k_slot_comp(const __grid_constant__ StepArgs a) {
@@ -879,15 +844,7 @@ static void launch_slot(bool push, bool move, bool comp, dim3 grid, int threads,
     k_slot_comp<true, BC><<<grid, threads, smem, st>>>(a);
   else if (comp)
     k_slot_comp<false, BC><<<grid, threads, smem, st>>>(a);
-  else if (SPX_WARP_UNITS && a.TX <= 32) {
-    const size_t su = (size_t)(threads / 32) * slot_unit_floats(a.TX, push, move) * sizeof(float);
-    if (push && move)
-      k_slot_wu<true, true, BC, T16><<<grid, threads, su, st>>>(a);
-    else if (push)
-      k_slot_wu<true, false, BC, T16><<<grid, threads, su, st>>>(a);
-    else if (move)
-      k_slot_wu<false, true, BC, T16><<<grid, threads, su, st>>>(a);
-  } else if (push && move)
+  else if (push && move)
     k_slot<true, true, BC, T16><<<grid, threads, smem, st>>>(a);
   else if (push)
     k_slot<true, false, BC, T16><<<grid, threads, smem, st>>>(a);
@@ -912,28 +869,6 @@ __global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS)
     const int2 item = items[it];
     slot_tile<PUSH, MOVE, false, BC, T16>(args[item.x], item.y, smem, 0, args[item.x].ns);
     __syncthreads();  // the shared windows are reused by the next item
-  }
-}
-
-// Many simulations, warp units: every warp takes (simulation, tile, unit) items from the
-// work queue on its own (the tiles' 32-cell units in the list's order, heaviest tiles
-// first), so no warp waits for the other warps of its CTA.
-template <bool PUSH, bool MOVE, int BC, bool T16>
-__global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS)
-    k_slot_batch_wu(const StepArgs* __restrict__ args, const int2* __restrict__ items, int nitems, int* counter,
-                    int units_per_tile, int tx_cells) {
-  extern __shared__ float smem[];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  float* const my = smem + w * slot_unit_floats(T16 ? 16 : tx_cells, PUSH, MOVE);
-  const int total = nitems * units_per_tile;
-  for (;;) {
-    int it = 0;
-    if (lane == 0) it = atomicAdd(counter, 1);
-    it = __shfl_sync(0xffffffffu, it, 0);
-    if (it >= total) break;
-    const int2 item = items[it / units_per_tile];
-    slot_tile<PUSH, MOVE, false, BC, T16, true>(args[item.x], item.y, my, 0, args[item.x].ns, it % units_per_tile);
-    __syncwarp();  // the unit's windows are reused by the warp's next item
   }
 }
 
@@ -1081,18 +1016,14 @@ static SpeciesArgs species_args(Species& sp) {
 template <int BC, bool T16>
 static void set_batch_attributes() {
   for (const void* f : {(const void*)k_slot_batch<true, true, BC, T16>, (const void*)k_slot_batch<true, false, BC, T16>,
-                        (const void*)k_slot_batch<false, true, BC, T16>,
-                        (const void*)k_slot_batch_wu<true, true, BC, T16>,
-                        (const void*)k_slot_batch_wu<true, false, BC, T16>,
-                        (const void*)k_slot_batch_wu<false, true, BC, T16>})
+                        (const void*)k_slot_batch<false, true, BC, T16>})
     SPX_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
 }
 template <int BC, bool T16>
 static void set_single_attributes() {
   for (const void* f : {(const void*)k_slot<true, true, BC, T16>, (const void*)k_slot<true, false, BC, T16>,
                         (const void*)k_slot<false, true, BC, T16>, (const void*)k_slot_comp<true, BC>,
-                        (const void*)k_slot_comp<false, BC>, (const void*)k_slot_wu<true, true, BC, T16>,
-                        (const void*)k_slot_wu<true, false, BC, T16>, (const void*)k_slot_wu<false, true, BC, T16>})
+                        (const void*)k_slot_comp<false, BC>})
     SPX_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
 }
 
@@ -1227,18 +1158,7 @@ void slot_batch_build(SlotBatch& b, const std::vector<SlotBatchSim>& sims) {
 
 template <int BC, bool T16>
 static void launch_batch(bool push, bool move, const SlotBatch& b, int TC, size_t smem, cudaStream_t st,
-                         const StepArgs* args, int TX) {
-  if (SPX_WARP_UNITS && TX <= 32) {
-    const size_t su = (size_t)(TC / 32) * slot_unit_floats(TX, push, move) * sizeof(float);
-    const int upt = TC / 32;
-    if (push && move)
-      k_slot_batch_wu<true, true, BC, T16><<<b.grid, TC, su, st>>>(args, b.d_items, b.nitems, b.d_counter, upt, TX);
-    else if (push)
-      k_slot_batch_wu<true, false, BC, T16><<<b.grid, TC, su, st>>>(args, b.d_items, b.nitems, b.d_counter, upt, TX);
-    else
-      k_slot_batch_wu<false, true, BC, T16><<<b.grid, TC, su, st>>>(args, b.d_items, b.nitems, b.d_counter, upt, TX);
-    return;
-  }
+                         const StepArgs* args) {
   if (push && move)
     k_slot_batch<true, true, BC, T16><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
   else if (push)
@@ -1250,7 +1170,7 @@ static void launch_batch(bool push, bool move, const SlotBatch& b, int TC, size_
 int slot_batch_step(SlotBatch& b, std::vector<SlotBatchSim>& sims, bool push, bool move, cudaStream_t st) {
   const int par = sims[0].sp[0].slot.ocur;
   const StepArgs* args = b.d_args[par];
-  const int TC = sims[0].pg.TC(), TX = sims[0].pg.TX;
+  const int TC = sims[0].pg.TC();
   const size_t smem = slot_smem_floats(sims[0].pg.TX, sims[0].pg.TY, push, move) * sizeof(float);
   int launches = 0;
   k_batch_reset<<<(b.nsims + 255) / 256, 256, 0, st>>>(args, b.nsims, b.d_counter);
@@ -1263,14 +1183,14 @@ int slot_batch_step(SlotBatch& b, std::vector<SlotBatchSim>& sims, bool push, bo
   }
   const int bc = all_periodic ? BC_PERIODIC : all_wall ? BC_WALL : BC_ANY;
   if (bc == BC_PERIODIC)
-    t16 ? launch_batch<BC_PERIODIC, true>(push, move, b, TC, smem, st, args, TX)
-        : launch_batch<BC_PERIODIC, false>(push, move, b, TC, smem, st, args, TX);
+    t16 ? launch_batch<BC_PERIODIC, true>(push, move, b, TC, smem, st, args)
+        : launch_batch<BC_PERIODIC, false>(push, move, b, TC, smem, st, args);
   else if (bc == BC_WALL)
-    t16 ? launch_batch<BC_WALL, true>(push, move, b, TC, smem, st, args, TX)
-        : launch_batch<BC_WALL, false>(push, move, b, TC, smem, st, args, TX);
+    t16 ? launch_batch<BC_WALL, true>(push, move, b, TC, smem, st, args)
+        : launch_batch<BC_WALL, false>(push, move, b, TC, smem, st, args);
   else
-    t16 ? launch_batch<BC_ANY, true>(push, move, b, TC, smem, st, args, TX)
-        : launch_batch<BC_ANY, false>(push, move, b, TC, smem, st, args, TX);
+    t16 ? launch_batch<BC_ANY, true>(push, move, b, TC, smem, st, args)
+        : launch_batch<BC_ANY, false>(push, move, b, TC, smem, st, args);
   ++launches;
   const dim3 og(16, b.nsims);
   if (push && move)
