@@ -242,8 +242,10 @@ SPX_API const char* spx_batch_last_error(const spx_batch* batch);
 SPX_API spx_ctx* spx_batch_sim(spx_batch* batch, int32_t sim);
 SPX_API int spx_batch_prepare(spx_batch* batch);
 SPX_API int spx_batch_step(spx_batch* batch, uint32_t n);
-/* Timing (CUDA events, uncaptured steps when enabled): out2[0] particle phase,
- * out2[1] whole steps, ms summed over the last spx_batch_step call. */
+/* Timing (CUDA events, uncaptured steps when enabled): out2[0] particle phase
+ * (from the zeroed sources to the deposited ones: the work-queue reset, the
+ * particle kernel and its overflow fallback), out2[1] whole steps, ms summed
+ * over the last spx_batch_step call. */
 SPX_API int spx_batch_set_timing(spx_batch* batch, int32_t enable);
 SPX_API int spx_batch_get_timing(spx_batch* batch, float* out2);
 SPX_API void* spx_batch_get_stream(const spx_batch* batch);

@@ -1233,7 +1233,7 @@ struct spx_batch {
   std::map<uint32_t, StepGraph> graphs;
   std::string err;
   bool timing = false;
-  cudaEvent_t t0 = nullptr, t1 = nullptr, t2 = nullptr;
+  cudaEvent_t t0 = nullptr, tz = nullptr, t1 = nullptr, t2 = nullptr;  // step start, sources zeroed, particles, end
   float last_ms[2] = {0, 0};  // particle phase, whole step (summed over the last call)
   uint64_t last_launches = 0;
 };
@@ -1285,6 +1285,7 @@ extern "C" int spx_batch_create(int32_t n, const spx_params* params, spx_batch**
     b->ev_join.resize(n);
     for (auto& e : b->ev_join) SPX_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     SPX_CUDA_TRY(cudaEventCreate(&b->t0));
+    SPX_CUDA_TRY(cudaEventCreate(&b->tz));
     SPX_CUDA_TRY(cudaEventCreate(&b->t1));
     SPX_CUDA_TRY(cudaEventCreate(&b->t2));
   } catch (const spx::Error& e) {
@@ -1304,7 +1305,7 @@ extern "C" int spx_batch_destroy(spx_batch* b) {
   b->up.release();
   if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   for (auto e : b->ev_join) cudaEventDestroy(e);
-  for (auto e : {b->t0, b->t1, b->t2})
+  for (auto e : {b->t0, b->tz, b->t1, b->t2})
     if (e) cudaEventDestroy(e);
   if (b->st) cudaStreamDestroy(b->st);
   delete b;
@@ -1359,6 +1360,7 @@ static int batch_step_body(spx_batch* b, bool timed) {
   fork();
   for (spx_ctx* c : b->sims) zero_sources(c);
   join();
+  if (timed) SPX_CUDA_TRY(cudaEventRecord(b->tz, b->st));
   std::vector<SlotBatchSim> sims = batch_sims(b);
   const bool pending = b->sims[0]->pending_push;
   launches += slot_batch_step(b->sb, sims, pending, true, b->st);
@@ -1442,7 +1444,7 @@ extern "C" int spx_batch_step(spx_batch* b, uint32_t steps) {
         launches += batch_step_body(b, true);
         SPX_CUDA_TRY(cudaEventSynchronize(b->t2));
         float p = 0, t = 0;
-        SPX_CUDA_TRY(cudaEventElapsedTime(&p, b->t0, b->t1));
+        SPX_CUDA_TRY(cudaEventElapsedTime(&p, b->tz, b->t1));
         SPX_CUDA_TRY(cudaEventElapsedTime(&t, b->t0, b->t2));
         acc[0] += p;
         acc[1] += t;
