@@ -19,15 +19,17 @@ from conftest import ROOT
 
 pytestmark = pytest.mark.gpu
 FIXTURE = os.path.join(ROOT, "tests", "golden", "two_stream_energy.json")
+# the same plasma on a 512 x 512 crop (make_two_stream.py 512), when generated
+FIXTURE_512 = os.path.join(ROOT, "tests", "golden", "two_stream_energy_512.json")
 
 
-def _run_gpu(path):
+def _run_gpu(path, fixture=FIXTURE):
     import sys
     sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
     import make_two_stream as mts
     from spectral_rs_b200 import Sim
     from spectral_rs_b200.config import Config, Setup, Output
-    with open(FIXTURE) as f:
+    with open(fixture) as f:
         study = json.load(f)["study"]
     mts.STUDY.update(study)
     p, bs = mts.beams(study)
@@ -53,15 +55,16 @@ def _growth_rate(e, every, dt):
     return t, le
 
 
-@pytest.fixture(scope="module")
-def ref():
-    with open(FIXTURE) as f:
-        return json.load(f)
+def _fixtures():
+    return [FIXTURE] + ([FIXTURE_512] if os.path.exists(FIXTURE_512) else [])
 
 
+@pytest.mark.parametrize("fixture", _fixtures(), ids=lambda f: os.path.basename(f))
 @pytest.mark.parametrize("path", ["split", "split_compensated", "plain"])
-def test_two_stream_energy_vs_fp64(ref, path):
-    e_gpu, study = _run_gpu(path)
+def test_two_stream_energy_vs_fp64(fixture, path):
+    with open(fixture) as f:
+        ref = json.load(f)
+    e_gpu, study = _run_gpu(path, fixture)
     e64 = np.array(ref["fp64"]["E"])
     e32 = np.array(ref["fp32"]["E"])
     assert len(e_gpu) == len(e64)
@@ -80,6 +83,7 @@ def test_two_stream_energy_vs_fp64(ref, path):
     rel = np.abs(e_gpu - e64) / e64
     rel32 = np.abs(e32 - e64) / e64
     lin_end = win[-1]
+    path = f"{path} {study['size_x']}x{study['size_y']}"
     print(f"\n[{path}] growth rate (1/omega_pe): fp64 {g64:.5f}  gpu fp32 {ggp:.5f}  oracle fp32 {g32:.5f}")
     print(f"[{path}] rel. field-energy error vs fp64: end of linear phase (step {(lin_end + 1) * every}) "
           f"{rel[lin_end]:.2e} (oracle fp32 {rel32[lin_end]:.2e}); step {len(e64) * every}: {rel[-1]:.2e} "
