@@ -16,8 +16,16 @@ build):
   C4        two members of the 64-member shock ensemble (one 1024 x 256, one
             128 x 128) stepped inside the batch, against live oracles.
 
-Tolerances (fields are compared against FP64, scaled by the field's max |value|):
-  - GPU field error <= 10x the FP32 oracle's own error (floor 1e-5);
+Tolerances (fields against FP64 over the interior cells; Dens's ghost frame holds raw,
+unfolded deposits and is left out):
+  - RMS error ||gpu - fp64|| / ||fp64|| <= 10x the FP32 oracle's (floor 1e-6), every field;
+  - max error / max |fp64| <= 10x the FP32 oracle's (floor 1e-5) for Dens; for the fields
+    the filter and the solver reach (J, E, B) the floor is 5e-3: the first filter pass reads
+    the ghost rows' raw deposits (field.rs:376-426 after field.rs:260-373), so a particle that
+    one rounding puts on the other side of the periodic edge (same place to one ulp) moves
+    the reference's own fields near that edge by ~1e-3 at 64 per cell
+    (test_known_answers.py::test_periodic_edge_representation).  Atomic deposit order makes
+    such crossings differ from run to run;
   - cell-index mismatch against the FP32 oracle <= 1e-4 of the particles;
   - momenta within 1e-3 of max |p| of the FP32 oracle;
   - energy histories: see each test.
@@ -78,18 +86,23 @@ def _add(sim, species):
 
 
 def _compare(tag, get_gpu, o32, o64, prtls=None):
-    """Fields against FP64 (within 10x the FP32 oracle's error), particles against FP32."""
+    """Fields against FP64 (RMS within 10x the FP32 oracle's, max-norm as the module
+    docstring states), particles against FP32."""
     report = {}
     for name in FIELDS:
-        g, r = get_gpu(name).astype(np.float64), o64.spatial(name)
-        r32 = o32.spatial(name).astype(np.float64)
+        g = get_gpu(name)[1:-1, 1:-1].astype(np.float64)
+        r = o64.spatial(name)[1:-1, 1:-1]
+        r32 = o32.spatial(name)[1:-1, 1:-1].astype(np.float64)
         scale = max(np.max(np.abs(r)), 1e-30)
-        err_gpu, err_ref = np.max(np.abs(g - r)) / scale, np.max(np.abs(r32 - r)) / scale
-        report[name] = (err_gpu, err_ref)
-    print(f"\n[{tag}] field error vs fp64 (gpu, oracle fp32): " +
-          ", ".join(f"{k} {a:.1e}/{b:.1e}" for k, (a, b) in report.items()))
-    for name, (err_gpu, err_ref) in report.items():
-        assert err_gpu <= max(10 * err_ref, 1e-5), (tag, name, err_gpu, err_ref)
+        norm = max(float(np.sqrt(np.sum(r * r))), 1e-30)
+        report[name] = (np.max(np.abs(g - r)) / scale, np.max(np.abs(r32 - r)) / scale,
+                        float(np.sqrt(np.sum((g - r) ** 2))) / norm, float(np.sqrt(np.sum((r32 - r) ** 2))) / norm)
+    print(f"\n[{tag}] field error vs fp64, max (gpu/oracle fp32) | rms (gpu/oracle fp32): " +
+          ", ".join(f"{k} {a:.1e}/{b:.1e} | {c:.1e}/{d:.1e}" for k, (a, b, c, d) in report.items()))
+    for name, (mx_gpu, mx_ref, rms_gpu, rms_ref) in report.items():
+        assert rms_gpu <= max(10 * rms_ref, 1e-6), (tag, name, "rms", rms_gpu, rms_ref)
+        floor = 1e-5 if name == "Dens" else 5e-3
+        assert mx_gpu <= max(10 * mx_ref, floor), (tag, name, "max", mx_gpu, mx_ref)
     for s, pr in enumerate(prtls or []):
         g, r = pr.state(), o32.state(s)
         mism = np.mean((g["ix"] != r["ix"]) | (g["iy"] != r["iy"]))

@@ -244,3 +244,37 @@ def test_courant_stability_boundary():
     The benchmark workloads therefore use c = 3, dt = 0.1."""
     assert _thermal_energy_growth(3.0, 150) < 10.0
     assert _thermal_energy_growth(4.5, 150) > 1e6
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_periodic_edge_representation(dtype):
+    """One particle at rest on the periodic y edge, stored as (iy = 1, dy = -0.5) or as
+    (iy = ny, dy = the largest value below 0.5): the same place to within one ulp.  The
+    fold (field.rs:260-373) makes the interior deposits equal, but the ghost rows keep
+    their raw deposits (the reference never clears them) and the first filter pass
+    (field.rs:376-426) reads them as neighbours, so the filtered sources and the next E
+    differ by O(1/ppc) at the edge rows.  A 1-ulp difference in a particle's position that
+    moves it across the periodic edge therefore changes the reference's own fields near
+    that edge at the 1e-3 level of a 64-per-cell plasma; parity tests of long runs bound
+    the field error by its RMS and by a max-norm that allows for this."""
+    p = test_params(size_x=16, size_y=8, delta=0, c=3.0, dt=0.1, dens=1, periodic_x=True)
+    below = np.nextafter(dtype(0.5), dtype(0.0))
+    res = []
+    for iy, dy in ((1, dtype(-0.5)), (p.size_y, below)):
+        o = orc.OracleSim.from_params(p, dtype=dtype)
+        z = np.zeros(1, dtype=dtype)
+        o.add_species(-1.0, 1.0, 0.0, np.array([5], np.uint64), np.array([iy], np.uint64), z, np.array([dy], dtype),
+                      z, z, z, np.ones(1, dtype))
+        o.move_and_deposit(0)
+        o.fold_sources()
+        dens, rho = o.spatial("Dens").astype(np.float64), o.spatial("Rho").astype(np.float64)
+        o.fields_update()
+        res.append((dens, rho, o.spatial("Ey").astype(np.float64)))
+    (d0, r0, e0), (d1, r1, e1) = res
+    tol = 1e-12 if dtype == np.float64 else 1e-6
+    assert np.max(np.abs(d0[1:-1, 1:-1] - d1[1:-1, 1:-1])) < tol       # folded interior: the same
+    assert np.max(np.abs(d0[[0, -1]] - d1[[0, -1]])) > 0.3              # raw ghost rows: not (0.5 x 0.75)
+    f0 = orc.field_op(p.size_x, p.size_y, 2, r0, n_pass=1, dtype=dtype).astype(np.float64)
+    f1 = orc.field_op(p.size_x, p.size_y, 2, r1, n_pass=1, dtype=dtype).astype(np.float64)
+    assert np.max(np.abs(f0[1:-1, 1:-1] - f1[1:-1, 1:-1])) > 0.02      # one filter pass sees the ghosts
+    assert np.max(np.abs(e0 - e1)) > 1e-3 * np.max(np.abs(e0))         # and so does E
