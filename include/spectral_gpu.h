@@ -228,8 +228,10 @@ SPX_API uint64_t spx_last_launch_count(const spx_ctx* ctx);
  * Many simulations with their own grids, species and parameters (uneven
  * ensembles, e.g. parameter scans of shocks) advance together: the particle phase of
  * all of them is one persistent kernel over a work queue of (simulation, tile)
- * items ordered by decreasing work, the field phase of each runs on its own
- * stream, and one step of the batch is one CUDA graph launch.  There is no
+ * items ordered by decreasing work, the field phase is one launch per kernel
+ * for each group of simulations that share a grid and filter pass count (each
+ * member's fields bit-identical to its own spx_fields_update), and one step of
+ * the batch is one CUDA graph launch.  There is no
  * counterpart in the reference (one simulation per process).
  * spx_batch_sim returns the context of simulation i, used as any spx_ctx for
  * species set-up (spx_add_species / spx_init_species) and for getters; after

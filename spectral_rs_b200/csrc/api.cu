@@ -1225,9 +1225,8 @@ extern "C" int spx_fft2d(uint64_t nx, uint64_t ny, int32_t inverse, float* data)
 struct spx_batch {
   std::vector<spx_ctx*> sims;
   cudaStream_t st = nullptr;
-  cudaEvent_t ev_fork = nullptr;
-  std::vector<cudaEvent_t> ev_join;
   SlotBatch sb;
+  FieldBatch* fbat = nullptr;  // the members' field phase, grouped by grid
   UploadRing up;  // one upload ring lent to every member (they add species one after another)
   bool built = false;
   std::map<uint32_t, StepGraph> graphs;
@@ -1281,9 +1280,6 @@ extern "C" int spx_batch_create(int32_t n, const spx_params* params, spx_batch**
         throw spx::Error(SPX_ERR_ARG, "all simulations of a batch need the same tile shape");
     }
     SPX_CUDA_TRY(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
-    SPX_CUDA_TRY(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
-    b->ev_join.resize(n);
-    for (auto& e : b->ev_join) SPX_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     SPX_CUDA_TRY(cudaEventCreate(&b->t0));
     SPX_CUDA_TRY(cudaEventCreate(&b->tz));
     SPX_CUDA_TRY(cudaEventCreate(&b->t1));
@@ -1301,10 +1297,10 @@ extern "C" int spx_batch_destroy(spx_batch* b) {
   if (b->st) cudaStreamSynchronize(b->st);
   for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second.exec);
   b->sb.release();
+  field_batch_release(b->fbat);
+  b->fbat = nullptr;
   for (spx_ctx* c : b->sims) spx_destroy(c);
   b->up.release();
-  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
-  for (auto e : b->ev_join) cudaEventDestroy(e);
   for (auto e : {b->t0, b->tz, b->t1, b->t2})
     if (e) cudaEventDestroy(e);
   if (b->st) cudaStreamDestroy(b->st);
@@ -1332,6 +1328,11 @@ extern "C" int spx_batch_prepare(spx_batch* b) {
   try {
     b->sb.release();
     slot_batch_build(b->sb, batch_sims(b));
+    field_batch_release(b->fbat);
+    b->fbat = nullptr;
+    std::vector<FieldBuffers*> fbs;
+    for (spx_ctx* c : b->sims) fbs.push_back(&c->fb);
+    b->fbat = field_batch_build(fbs);
     for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second.exec);
     b->graphs.clear();
     capture_batch_steady_state(b);
@@ -1343,35 +1344,19 @@ extern "C" int spx_batch_prepare(spx_batch* b) {
 }
 
 // One step of every simulation.  Returns kernel launches.
+// The sources of every member are zeroed and, after the particle phase, folded
+// and advanced by the batched field phase (one launch per kernel and grid group).
 static int batch_step_body(spx_batch* b, bool timed) {
   int launches = 0;
-  const int n = (int)b->sims.size();
-  auto fork = [&]() {
-    SPX_CUDA_TRY(cudaEventRecord(b->ev_fork, b->st));
-    for (spx_ctx* c : b->sims) SPX_CUDA_TRY(cudaStreamWaitEvent(c->st, b->ev_fork, 0));
-  };
-  auto join = [&]() {
-    for (int i = 0; i < n; ++i) {
-      SPX_CUDA_TRY(cudaEventRecord(b->ev_join[i], b->sims[i]->st));
-      SPX_CUDA_TRY(cudaStreamWaitEvent(b->st, b->ev_join[i], 0));
-    }
-  };
   if (timed) SPX_CUDA_TRY(cudaEventRecord(b->t0, b->st));
-  fork();
-  for (spx_ctx* c : b->sims) zero_sources(c);
-  join();
+  launches += field_batch_zero_sources(b->fbat, b->st);
   if (timed) SPX_CUDA_TRY(cudaEventRecord(b->tz, b->st));
   std::vector<SlotBatchSim> sims = batch_sims(b);
   const bool pending = b->sims[0]->pending_push;
   launches += slot_batch_step(b->sb, sims, pending, true, b->st);
   if (timed) SPX_CUDA_TRY(cudaEventRecord(b->t1, b->st));
-  fork();
-  for (spx_ctx* c : b->sims) {
-    launches += fold_all(c);
-    launches += field_update(c->fb, c->st);
-    c->pending_push = true;
-  }
-  join();
+  launches += field_batch_update(b->fbat, b->st);
+  for (spx_ctx* c : b->sims) c->pending_push = true;
   if (timed) SPX_CUDA_TRY(cudaEventRecord(b->t2, b->st));
   return launches;
 }

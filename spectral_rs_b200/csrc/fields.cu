@@ -21,6 +21,8 @@
 #include <cmath>
 #include <vector>
 
+#include <cstring>
+
 #include "fields.cuh"
 
 namespace spx {
@@ -315,8 +317,10 @@ __device__ __forceinline__ void store_ghosted(float* dst, const Grid& g, int row
 constexpr int FFT_LOGN_MIN = 6, FFT_LOGN_MAX = 13;
 
 template <int IN, int OUT, bool INV, bool SMALL, int LOGN>
-__global__ void FFT_BOUNDS(SMALL) k_rows(const __grid_constant__ RowArgs a, Grid g0, const float2* __restrict__ tw) {
+__global__ void FFT_BOUNDS(SMALL) k_rows(const __grid_constant__ RowArgs a0, const RowArgs* __restrict__ tab, Grid g0,
+                                         const float2* __restrict__ tw) {
   extern __shared__ float2 sm[];
+  const RowArgs& a = tab ? tab[blockIdx.z] : a0;  // a batch: member blockIdx.z's fields
   Grid g = g0;
   if (LOGN) {
     g.log2nx = LOGN;
@@ -382,8 +386,10 @@ struct ColArgs {
   float2* data[8];
 };
 template <bool INV, bool SMALL, int LOGN>
-__global__ void FFT_BOUNDS(SMALL) k_cols(const __grid_constant__ ColArgs a, Grid g0, const float2* __restrict__ tw) {
+__global__ void FFT_BOUNDS(SMALL) k_cols(const __grid_constant__ ColArgs a0, const ColArgs* __restrict__ tab, Grid g0,
+                                         const float2* __restrict__ tw) {
   extern __shared__ float2 sm[];
+  const ColArgs& a = tab ? tab[blockIdx.z] : a0;
   Grid g = g0;
   if (LOGN) {
     g.log2ny = LOGN;
@@ -420,7 +426,8 @@ struct KArgs {
   float2 *jx, *jy, *jz, *rho, *ex, *ey, *ez, *bwx, *bwy, *bwz, *bax, *bay, *baz;
   float cdt, ckc;
 };
-__global__ void k_kspace(KArgs a, Grid g) {
+__global__ void k_kspace(const __grid_constant__ KArgs a0, const KArgs* __restrict__ tab, Grid g) {
+  const KArgs& a = tab ? tab[blockIdx.y] : a0;
   const size_t n = (size_t)g.nx * g.ny;
   for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
     const int i = (int)(idx >> g.log2nx), j = (int)(idx & (g.nx - 1));
@@ -484,8 +491,8 @@ struct ConstFieldList {
 
 // Field::deposit_ghosts, one thread per interior cell of the frame; additions in
 // the reference's order (rows, columns, corners), so results are bit-exact.
-__global__ void k_fold(const __grid_constant__ FieldList L, Grid g) {
-  float* F = L.f[blockIdx.y];
+__global__ void k_fold(const __grid_constant__ FieldList L, const FieldList* __restrict__ tab, Grid g) {
+  float* F = tab ? tab[blockIdx.z].f[blockIdx.y] : L.f[blockIdx.y];
   const int nx = g.nx, ny = g.ny, W = g.W;
   const int nper = 2 * nx + 2 * (ny - 2);
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nper; p += gridDim.x * blockDim.x) {
@@ -607,10 +614,13 @@ __device__ __forceinline__ void filter_column(const float* src, int sp, float* d
 }
 
 __global__ void __launch_bounds__(256) k_filter_fused(const __grid_constant__ ConstFieldList S,
-                                                      const __grid_constant__ FieldList D, Grid g, int npass) {
+                                                      const __grid_constant__ FieldList D,
+                                                      const ConstFieldList* __restrict__ stab,
+                                                      const FieldList* __restrict__ dtab, int nf, Grid g, int npass) {
   extern __shared__ float fs[];
-  const float* in = S.f[blockIdx.z];
-  float* out = D.f[blockIdx.z];
+  // a batch: blockIdx.z = member * nf + field
+  const float* in = stab ? stab[blockIdx.z / nf].f[blockIdx.z % nf] : S.f[blockIdx.z];
+  float* out = dtab ? dtab[blockIdx.z / nf].f[blockIdx.z % nf] : D.f[blockIdx.z];
   const int W = g.W, nx = g.nx, ny = g.ny;
   const int h = npass - 1;
   const int TW = FILT_EW - 2 * h;                // output tile width
@@ -682,7 +692,7 @@ void launch_fold(const Grid& g, float* const* fields, int nf, cudaStream_t st) {
   for (int i = 0; i < nf; ++i) L.f[i] = fields[i];
   int nper = 2 * g.nx + 2 * (g.ny - 2);
   int blocks = (nper + 255) / 256;
-  k_fold<<<dim3(blocks, nf), 256, 0, st>>>(L, g);
+  k_fold<<<dim3(blocks, nf), 256, 0, st>>>(L, nullptr, g);
 }
 
 void launch_update_ghosts(const Grid& g, float* const* fields, int nf, cudaStream_t st) {
@@ -705,7 +715,7 @@ void launch_filter_fused(const Grid& g, float* const* src, float* const* dst, in
   const size_t smem = filter_fused_smem_floats((int)npass) * sizeof(float);
   const int tw = FILT_EW - 2 * ((int)npass - 1);
   dim3 grd((g.nx + tw - 1) / tw, (g.ny + FILT_TY - 1) / FILT_TY, nf);
-  k_filter_fused<<<grd, 256, smem, st>>>(S, D, g, (int)npass);
+  k_filter_fused<<<grd, 256, smem, st>>>(S, D, nullptr, nullptr, nf, g, (int)npass);
 }
 
 void launch_filter_pass(const Grid& g, float* const* src, float* const* dst, int nf, cudaStream_t st) {
@@ -774,32 +784,35 @@ void fields_set_kernel_attributes() {
   fft_attr((const void*)k_filter_fused);
 }
 
+// tab: a batch of nm simulations of grid g (member blockIdx.z's arguments), else a alone (nm = 1)
 template <int IN, int OUT, bool INV, int LOGN>
-static void launch_rows_n(const Grid& g, const RowArgs& a, int nf, const float2* tw, cudaStream_t st) {
+static void launch_rows_n(const Grid& g, const RowArgs& a, const RowArgs* tab, int nf, int nm, const float2* tw,
+                          cudaStream_t st) {
   const int logB = row_logB(g.log2nx);
   const int threads = std::max(1, (g.nx << logB) / 8);
   const size_t smem = sizeof(float2) * fft_smem_elems(g.log2nx, logB);
   const int blocks = (g.ny + (1 << logB) - 1) >> logB;
   if constexpr (LOGN > 0) {
-    k_rows<IN, OUT, INV, rows_small(LOGN), LOGN><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
+    k_rows<IN, OUT, INV, rows_small(LOGN), LOGN><<<dim3(blocks, nf, nm), threads, smem, st>>>(a, tab, g, tw);
   } else {
     if (threads <= 512)
-      k_rows<IN, OUT, INV, true, 0><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
+      k_rows<IN, OUT, INV, true, 0><<<dim3(blocks, nf, nm), threads, smem, st>>>(a, tab, g, tw);
     else
-      k_rows<IN, OUT, INV, false, 0><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
+      k_rows<IN, OUT, INV, false, 0><<<dim3(blocks, nf, nm), threads, smem, st>>>(a, tab, g, tw);
   }
 }
 
 template <bool INV, int LOGN>
-static void launch_cols_n(const Grid& g, const ColArgs& a, int nf, const float2* tw, cudaStream_t st) {
+static void launch_cols_n(const Grid& g, const ColArgs& a, const ColArgs* tab, int nf, int nm, const float2* tw,
+                          cudaStream_t st) {
   const int logW = col_logW(g.log2ny, g.log2nx);
   const int threads = std::max(1, (g.ny << logW) / 8);
   const size_t smem = sizeof(float2) * fft_smem_elems(g.log2ny, logW);
   const int blocks = g.nx >> logW;
   if (threads <= 512)
-    k_cols<INV, true, LOGN><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
+    k_cols<INV, true, LOGN><<<dim3(blocks, nf, nm), threads, smem, st>>>(a, tab, g, tw);
   else
-    k_cols<INV, false, LOGN><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
+    k_cols<INV, false, LOGN><<<dim3(blocks, nf, nm), threads, smem, st>>>(a, tab, g, tw);
 }
 
 // Dispatch on the transform length: 2^6 .. 2^13 compiled per length, shorter ones generic.
@@ -817,15 +830,17 @@ static void launch_cols_n(const Grid& g, const ColArgs& a, int nf, const float2*
   }
 
 template <int IN, int OUT, bool INV>
-static void launch_rows(const Grid& g, const RowArgs& a, int nf, const float2* tw, cudaStream_t st) {
-#define SPX_ROWS(L) launch_rows_n<IN, OUT, INV, L>(g, a, nf, tw, st)
+static void launch_rows(const Grid& g, const RowArgs& a, int nf, const float2* tw, cudaStream_t st,
+                        const RowArgs* tab = nullptr, int nm = 1) {
+#define SPX_ROWS(L) launch_rows_n<IN, OUT, INV, L>(g, a, tab, nf, nm, tw, st)
   FFT_DISPATCH(g.log2nx, SPX_ROWS)
 #undef SPX_ROWS
 }
 
 template <bool INV>
-static void launch_cols(const Grid& g, const ColArgs& a, int nf, const float2* tw, cudaStream_t st) {
-#define SPX_COLS(L) launch_cols_n<INV, L>(g, a, nf, tw, st)
+static void launch_cols(const Grid& g, const ColArgs& a, int nf, const float2* tw, cudaStream_t st,
+                        const ColArgs* tab = nullptr, int nm = 1) {
+#define SPX_COLS(L) launch_cols_n<INV, L>(g, a, tab, nf, nm, tw, st)
   FFT_DISPATCH(g.log2ny, SPX_COLS)
 #undef SPX_COLS
 }
@@ -862,13 +877,84 @@ void FieldBuffers::release() {
   tw_x = tw_y = nullptr;
 }
 
+// The arguments of Flds::update's kernels for one simulation (shared by its own
+// field_update and by a batch's tables, so both launch the same work).
+static void source_lists(const FieldBuffers& fb, FieldList& zero, ConstFieldList& fsrc, FieldList& fdst) {
+  zero = FieldList{};
+  fsrc = ConstFieldList{};
+  fdst = FieldList{};
+  const int ids[5] = {SPX_JX, SPX_JY, SPX_JZ, SPX_DSTY, SPX_DENS};
+  for (int i = 0; i < 5; ++i) zero.f[i] = fb.spatial[ids[i]];
+  for (int i = 0; i < 4; ++i) {
+    fsrc.f[i] = fb.spatial[ids[i]];
+    fdst.f[i] = fb.filt_tmp[i];
+  }
+}
+// copy_to_spectral (+ dsty/dens) fused with the row FFTs (mod.rs:66-85, 101-103, 122-124);
+// fused: the sources come filtered from filt_tmp and are stored back into the fields
+// with their periodic ghosts, the state the reference leaves.
+static RowArgs rows_fwd_args(const FieldBuffers& fb, bool fused) {
+  RowArgs a{};
+  const int src_ids[7] = {SPX_JX, SPX_JY, SPX_JZ, SPX_DSTY, SPX_EX, SPX_EY, SPX_EZ};
+  const int dst_ids[7] = {SP_JX, SP_JY, SP_JZ, SP_RHO, SP_EX, SP_EY, SP_EZ};
+  for (int i = 0; i < 7; ++i) {
+    a.src[i] = fb.spatial[src_ids[i]];
+    a.dst[i] = fb.spec[dst_ids[i]];
+    a.back[i] = nullptr;
+    a.scale[i] = 1.0f;
+  }
+  if (fused)
+    for (int i = 0; i < 4; ++i) {
+      a.src[i] = fb.filt_tmp[i];
+      a.back[i] = fb.spatial[src_ids[i]];
+    }
+  a.scale[3] = 1.0f / (float)fb.dens;
+  return a;
+}
+static ColArgs cols_fwd_args(const FieldBuffers& fb) {
+  const int dst_ids[7] = {SP_JX, SP_JY, SP_JZ, SP_RHO, SP_EX, SP_EY, SP_EZ};
+  ColArgs c{};
+  for (int i = 0; i < 7; ++i) c.data[i] = fb.spec[dst_ids[i]];
+  return c;
+}
+static KArgs kspace_args(const FieldBuffers& fb) {
+  KArgs k;
+  k.jx = fb.spec[SP_JX]; k.jy = fb.spec[SP_JY]; k.jz = fb.spec[SP_JZ]; k.rho = fb.spec[SP_RHO];
+  k.ex = fb.spec[SP_EX]; k.ey = fb.spec[SP_EY]; k.ez = fb.spec[SP_EZ];
+  k.bwx = fb.spec[SP_BWX]; k.bwy = fb.spec[SP_BWY]; k.bwz = fb.spec[SP_BWZ];
+  k.bax = fb.spec[SP_BAX]; k.bay = fb.spec[SP_BAY]; k.baz = fb.spec[SP_BAZ];
+  k.ckc = fb.dt / (float)fb.dens;  // mod.rs:127
+  k.cdt = fb.dt * fb.c;            // mod.rs:128
+  return k;
+}
+// inverse transforms of B(t) and E, back to the spatial fields (mod.rs:281-307)
+static const int kInvSpec[6] = {SP_BAX, SP_BAY, SP_BAZ, SP_EX, SP_EY, SP_EZ};
+static ColArgs cols_inv_args(const FieldBuffers& fb) {
+  ColArgs c{};
+  for (int i = 0; i < 6; ++i) c.data[i] = fb.spec[kInvSpec[i]];
+  return c;
+}
+static RowArgs rows_inv_args(const FieldBuffers& fb) {
+  const int sp_ids[6] = {SPX_BX, SPX_BY, SPX_BZ, SPX_EX, SPX_EY, SPX_EZ};
+  RowArgs a{};
+  const float norm = 1.0f / (float)((uint64_t)fb.g.nx * (uint64_t)fb.g.ny);  // fft_2d.rs:170
+  for (int i = 0; i < 6; ++i) {
+    a.src[i] = fb.spec[kInvSpec[i]];
+    a.dst[i] = fb.spatial[sp_ids[i]];
+    a.scale[i] = norm;
+  }
+  return a;
+}
+static int kspace_blocks(const Grid& g, int nm) {
+  const size_t n = g.spectral_size();
+  return (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, (size_t)148 * 16 / (size_t)nm));
+}
+
 int field_update(FieldBuffers& fb, cudaStream_t st) {
   const Grid& g = fb.g;
   int launches = 0;
   // 1. n_pass binomial passes on jx, jy, jz, dsty (mod.rs:90-94).  Fused: all
-  // passes in one kernel into filt_tmp; the row transforms below read the
-  // filtered interior from there and store it back into the fields with their
-  // periodic ghosts, which is the state the reference leaves.
+  // passes in one kernel into filt_tmp.
   float* srcs[4] = {fb.spatial[SPX_JX], fb.spatial[SPX_JY], fb.spatial[SPX_JZ], fb.spatial[SPX_DSTY]};
   const bool fused = filter_fused_fits(fb.n_pass);
   if (fused) {
@@ -887,61 +973,192 @@ int field_update(FieldBuffers& fb, cudaStream_t st) {
         SPX_CUDA_TRY(cudaMemcpyAsync(oth[i], cur[i], g.spatial_size() * sizeof(float), cudaMemcpyDeviceToDevice, st));
     }
   }
-  // 2. copy_to_spectral (+ dsty/dens) fused with the row FFTs (mod.rs:66-85, 101-103, 122-124)
-  {
-    RowArgs a{};
-    const int src_ids[7] = {SPX_JX, SPX_JY, SPX_JZ, SPX_DSTY, SPX_EX, SPX_EY, SPX_EZ};
-    const int dst_ids[7] = {SP_JX, SP_JY, SP_JZ, SP_RHO, SP_EX, SP_EY, SP_EZ};
-    for (int i = 0; i < 7; ++i) {
-      a.src[i] = fb.spatial[src_ids[i]];
-      a.dst[i] = fb.spec[dst_ids[i]];
-      a.back[i] = nullptr;
-      a.scale[i] = 1.0f;
-    }
-    if (fused)
-      for (int i = 0; i < 4; ++i) {
-        a.src[i] = fb.filt_tmp[i];
-        a.back[i] = srcs[i];
-      }
-    a.scale[3] = 1.0f / (float)fb.dens;
-    launch_rows<0, 0, false>(g, a, 7, fb.tw_x, st);
-    ++launches;
-    ColArgs c{};
-    for (int i = 0; i < 7; ++i) c.data[i] = fb.spec[dst_ids[i]];
-    launch_cols<false>(g, c, 7, fb.tw_y, st);
-    ++launches;
-  }
+  // 2. forward transforms
+  launch_rows<0, 0, false>(g, rows_fwd_args(fb, fused), 7, fb.tw_x, st);
+  launch_cols<false>(g, cols_fwd_args(fb), 7, fb.tw_y, st);
+  launches += 2;
   // 3. k-space update (mod.rs:105-278)
-  {
-    KArgs k;
-    k.jx = fb.spec[SP_JX]; k.jy = fb.spec[SP_JY]; k.jz = fb.spec[SP_JZ]; k.rho = fb.spec[SP_RHO];
-    k.ex = fb.spec[SP_EX]; k.ey = fb.spec[SP_EY]; k.ez = fb.spec[SP_EZ];
-    k.bwx = fb.spec[SP_BWX]; k.bwy = fb.spec[SP_BWY]; k.bwz = fb.spec[SP_BWZ];
-    k.bax = fb.spec[SP_BAX]; k.bay = fb.spec[SP_BAY]; k.baz = fb.spec[SP_BAZ];
-    k.ckc = fb.dt / (float)fb.dens;  // mod.rs:127
-    k.cdt = fb.dt * fb.c;            // mod.rs:128
-    const size_t n = g.spectral_size();
-    int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
-    k_kspace<<<blocks, 256, 0, st>>>(k, g);
-    ++launches;
+  k_kspace<<<kspace_blocks(g, 1), 256, 0, st>>>(kspace_args(fb), nullptr, g);
+  ++launches;
+  // 4. inverse transforms
+  launch_cols<true>(g, cols_inv_args(fb), 6, fb.tw_y, st);
+  launch_rows<1, 1, true>(g, rows_inv_args(fb), 6, fb.tw_x, st);
+  launches += 2;
+  SPX_CUDA_TRY(cudaGetLastError());
+  return launches;
+}
+
+// ---------------------------------------------------------------- batches
+// The field phase of many simulations.  Members with the same grid and filter
+// pass count form a group; each kernel of the phase (source zeroing, ghost fold,
+// fused filter, the four transforms, the k-space update) runs once per group over
+// all its members (blockIdx.z, or blockIdx.y for k_kspace, picks the member),
+// reading the member's buffers and constants from a device table built once.
+// The kernels and their arithmetic are the single simulation's, so every member's
+// fields are bit-identical to its own field_update.  Groups run concurrently on
+// streams of their own.
+__global__ void k_zero_fields(const FieldList* __restrict__ tab, size_t n4) {
+  float4* f = reinterpret_cast<float4*>(tab[blockIdx.z].f[blockIdx.y]);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x)
+    f[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+struct FieldGroup {
+  Grid g{};
+  uint32_t n_pass = 0;
+  std::vector<FieldBuffers*> fbs;
+  void* dev = nullptr;  // one allocation for the tables below
+  FieldList* zero = nullptr;       // jx, jy, jz, dsty, dens: zeroed and folded
+  ConstFieldList* fsrc = nullptr;  // filter inputs
+  FieldList* fdst = nullptr;       // filter outputs (filt_tmp)
+  RowArgs* rf = nullptr;
+  ColArgs* cf = nullptr;
+  KArgs* ks = nullptr;
+  ColArgs* ci = nullptr;
+  RowArgs* ri = nullptr;
+  cudaStream_t st = nullptr;
+  cudaEvent_t done = nullptr;
+};
+struct FieldBatch {
+  std::vector<FieldGroup> groups;
+  cudaEvent_t fork = nullptr;
+};
+
+void field_batch_release(FieldBatch* b) {
+  if (!b) return;
+  for (FieldGroup& G : b->groups) {
+    if (G.st) cudaStreamSynchronize(G.st);
+    if (G.dev) cudaFree(G.dev);
+    if (G.done) cudaEventDestroy(G.done);
+    if (G.st) cudaStreamDestroy(G.st);
   }
-  // 4. inverse transforms of B(t) and E, back to the spatial fields (mod.rs:281-307)
-  {
-    const int spec_ids[6] = {SP_BAX, SP_BAY, SP_BAZ, SP_EX, SP_EY, SP_EZ};
-    const int sp_ids[6] = {SPX_BX, SPX_BY, SPX_BZ, SPX_EX, SPX_EY, SPX_EZ};
-    ColArgs c{};
-    for (int i = 0; i < 6; ++i) c.data[i] = fb.spec[spec_ids[i]];
-    launch_cols<true>(g, c, 6, fb.tw_y, st);
-    ++launches;
-    RowArgs a{};
-    const float norm = 1.0f / (float)((uint64_t)g.nx * (uint64_t)g.ny);  // fft_2d.rs:170
-    for (int i = 0; i < 6; ++i) {
-      a.src[i] = fb.spec[spec_ids[i]];
-      a.dst[i] = fb.spatial[sp_ids[i]];
-      a.scale[i] = norm;
+  if (b->fork) cudaEventDestroy(b->fork);
+  delete b;
+}
+
+FieldBatch* field_batch_build(const std::vector<FieldBuffers*>& members) {
+  FieldBatch* b = new FieldBatch();
+  try {
+    for (FieldBuffers* fb : members) {
+      FieldGroup* G = nullptr;
+      for (FieldGroup& h : b->groups)  // (a group's members * 4 filtered fields index gridDim.z <= 65535)
+        if (h.g.nx == fb->g.nx && h.g.ny == fb->g.ny && h.n_pass == fb->n_pass && h.fbs.size() < 16383) G = &h;
+      if (!G) {
+        b->groups.emplace_back();
+        G = &b->groups.back();
+        G->g = fb->g;
+        G->n_pass = fb->n_pass;
+      }
+      G->fbs.push_back(fb);
     }
-    launch_rows<1, 1, true>(g, a, 6, fb.tw_x, st);
-    ++launches;
+    SPX_CUDA_TRY(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    for (FieldGroup& G : b->groups) {
+      const size_t nm = G.fbs.size();
+      auto up = [](size_t v) { return (v + 255) & ~(size_t)255; };
+      const size_t sz[8] = {up(nm * sizeof(FieldList)), up(nm * sizeof(ConstFieldList)), up(nm * sizeof(FieldList)),
+                            up(nm * sizeof(RowArgs)),   up(nm * sizeof(ColArgs)),        up(nm * sizeof(KArgs)),
+                            up(nm * sizeof(ColArgs)),   up(nm * sizeof(RowArgs))};
+      size_t total = 0;
+      for (size_t v : sz) total += v;
+      std::vector<unsigned char> host(total, 0);
+      SPX_CUDA_TRY(cudaMalloc(&G.dev, total));
+      unsigned char* d = static_cast<unsigned char*>(G.dev);
+      size_t off[8];
+      for (int k = 0, o = 0; k < 8; o += (int)sz[k], ++k) off[k] = (size_t)o;
+      G.zero = reinterpret_cast<FieldList*>(d + off[0]);
+      G.fsrc = reinterpret_cast<ConstFieldList*>(d + off[1]);
+      G.fdst = reinterpret_cast<FieldList*>(d + off[2]);
+      G.rf = reinterpret_cast<RowArgs*>(d + off[3]);
+      G.cf = reinterpret_cast<ColArgs*>(d + off[4]);
+      G.ks = reinterpret_cast<KArgs*>(d + off[5]);
+      G.ci = reinterpret_cast<ColArgs*>(d + off[6]);
+      G.ri = reinterpret_cast<RowArgs*>(d + off[7]);
+      const bool fused = filter_fused_fits(G.n_pass);
+      for (size_t m = 0; m < nm; ++m) {
+        const FieldBuffers& fb = *G.fbs[m];
+        FieldList z;
+        ConstFieldList fs;
+        FieldList fd;
+        source_lists(fb, z, fs, fd);
+        const RowArgs rf = rows_fwd_args(fb, fused), ri = rows_inv_args(fb);
+        const ColArgs cf = cols_fwd_args(fb), ci = cols_inv_args(fb);
+        const KArgs ks = kspace_args(fb);
+        std::memcpy(&host[off[0] + m * sizeof(FieldList)], &z, sizeof z);
+        std::memcpy(&host[off[1] + m * sizeof(ConstFieldList)], &fs, sizeof fs);
+        std::memcpy(&host[off[2] + m * sizeof(FieldList)], &fd, sizeof fd);
+        std::memcpy(&host[off[3] + m * sizeof(RowArgs)], &rf, sizeof rf);
+        std::memcpy(&host[off[4] + m * sizeof(ColArgs)], &cf, sizeof cf);
+        std::memcpy(&host[off[5] + m * sizeof(KArgs)], &ks, sizeof ks);
+        std::memcpy(&host[off[6] + m * sizeof(ColArgs)], &ci, sizeof ci);
+        std::memcpy(&host[off[7] + m * sizeof(RowArgs)], &ri, sizeof ri);
+      }
+      SPX_CUDA_TRY(cudaMemcpy(G.dev, host.data(), total, cudaMemcpyHostToDevice));
+      SPX_CUDA_TRY(cudaStreamCreateWithFlags(&G.st, cudaStreamNonBlocking));
+      SPX_CUDA_TRY(cudaEventCreateWithFlags(&G.done, cudaEventDisableTiming));
+    }
+  } catch (...) {
+    field_batch_release(b);
+    throw;
+  }
+  return b;
+}
+
+int field_batch_groups(const FieldBatch* b) { return b ? (int)b->groups.size() : 0; }
+
+int field_batch_zero_sources(FieldBatch* b, cudaStream_t st) {
+  int launches = 0;
+  for (FieldGroup& G : b->groups) {
+    const size_t n = G.g.spatial_size();
+    const int nm = (int)G.fbs.size();
+    if (n % 4 == 0) {
+      const int bx = (int)std::max<size_t>(1, std::min<size_t>((n / 4 + 255) / 256, 64));
+      k_zero_fields<<<dim3(bx, 5, nm), 256, 0, st>>>(G.zero, n / 4);
+      ++launches;
+    } else {  // odd ghosted sizes: per field
+      for (FieldBuffers* fb : G.fbs)
+        for (int f : {SPX_JX, SPX_JY, SPX_JZ, SPX_DSTY, SPX_DENS}) {
+          SPX_CUDA_TRY(cudaMemsetAsync(fb->spatial[f], 0, n * sizeof(float), st));
+          ++launches;
+        }
+    }
+  }
+  SPX_CUDA_TRY(cudaGetLastError());
+  return launches;
+}
+
+int field_batch_update(FieldBatch* b, cudaStream_t st) {
+  int launches = 0;
+  SPX_CUDA_TRY(cudaEventRecord(b->fork, st));
+  for (FieldGroup& G : b->groups) {
+    cudaStream_t gs = G.st;
+    SPX_CUDA_TRY(cudaStreamWaitEvent(gs, b->fork, 0));
+    const Grid& g = G.g;
+    const int nm = (int)G.fbs.size();
+    // Field::deposit_ghosts of the five sources (src/flds/field.rs:260-373)
+    {
+      const int nper = 2 * g.nx + 2 * (g.ny - 2);
+      k_fold<<<dim3((nper + 255) / 256, 5, nm), 256, 0, gs>>>(FieldList{}, G.zero, g);
+      ++launches;
+    }
+    if (!filter_fused_fits(G.n_pass)) {  // more passes than the fused filter holds: member by member
+      for (FieldBuffers* fb : G.fbs) launches += field_update(*fb, gs);
+    } else {
+      const FieldBuffers& f0 = *G.fbs[0];  // twiddle tables depend on the grid only
+      {
+        const size_t smem = filter_fused_smem_floats((int)G.n_pass) * sizeof(float);
+        const int tw = FILT_EW - 2 * ((int)G.n_pass - 1);
+        const dim3 grd((g.nx + tw - 1) / tw, (g.ny + FILT_TY - 1) / FILT_TY, 4 * nm);
+        k_filter_fused<<<grd, 256, smem, gs>>>(ConstFieldList{}, FieldList{}, G.fsrc, G.fdst, 4, g, (int)G.n_pass);
+      }
+      launch_rows<0, 0, false>(g, RowArgs{}, 7, f0.tw_x, gs, G.rf, nm);
+      launch_cols<false>(g, ColArgs{}, 7, f0.tw_y, gs, G.cf, nm);
+      k_kspace<<<dim3(kspace_blocks(g, nm), nm), 256, 0, gs>>>(KArgs{}, G.ks, g);
+      launch_cols<true>(g, ColArgs{}, 6, f0.tw_y, gs, G.ci, nm);
+      launch_rows<1, 1, true>(g, RowArgs{}, 6, f0.tw_x, gs, G.ri, nm);
+      launches += 6;
+    }
+    SPX_CUDA_TRY(cudaEventRecord(G.done, gs));
+    SPX_CUDA_TRY(cudaStreamWaitEvent(st, G.done, 0));
   }
   SPX_CUDA_TRY(cudaGetLastError());
   return launches;

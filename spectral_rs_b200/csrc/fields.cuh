@@ -45,6 +45,18 @@ void launch_filter_fused(const Grid& g, float* const* src, float* const* dst, in
                          cudaStream_t st);
 // Flds::update (src/flds/mod.rs:87-309).  Returns the number of kernel launches.
 int field_update(FieldBuffers& fb, cudaStream_t st);
+// The field phase of a batch of simulations (one launch per kernel and group of
+// members with the same grid and filter pass count; same arithmetic as
+// field_update).  Built once over members whose buffers stay where they are.
+struct FieldBatch;
+FieldBatch* field_batch_build(const std::vector<FieldBuffers*>& members);
+void field_batch_release(FieldBatch* b);
+int field_batch_groups(const FieldBatch* b);
+// Zero jx, jy, jz, dsty and dens of every member (before the particle phase).
+int field_batch_zero_sources(FieldBatch* b, cudaStream_t st);
+// Fold the ghost frames of the sources, then Flds::update, for every member;
+// ordered after the work already queued on st, and st after it.  Returns launches.
+int field_batch_update(FieldBatch* b, cudaStream_t st);
 // Fft2D::fft / inv_fft on one complex array in place (tests).
 int fft2d_inplace(const Grid& g, float2* data, const float2* tw_x, const float2* tw_y, bool inverse,
                   cudaStream_t st);

@@ -131,48 +131,35 @@ __device__ __forceinline__ void moments_to_stencil(const float (&m)[9], float (&
 
 // Boris push of src/prtls.rs:412-440 given the gathered fields g[0..5] = E, B.
 // Every operation is the reference's, in its order (Rust evaluates a + b * c - d * e
-// as (a + (b*c)) - (d*e)); independent multiplications run in pairs as packed
-// FP32x2 products, and every sum that consumes a product stays scalar.
+// as (a + (b*c)) - (d*e)).  Scalar: its products pair operands in ever different
+// combinations, and packing them cost more register moves than it saved (measured:
+// 0.7 % more instructions per particle with packed products).
 __device__ __forceinline__ void boris(const float (&g)[6], float beta, float alpha, float csqinv, float& px,
                                       float& py, float& pz, float& psa) {
-  const float2 exy = mul2(make_float2(g[0], g[1]), bc2(beta));  // (ext, eyt)
-  const float ezt = g[2] * beta;
-  const float2 bxy = mul2(make_float2(g[3], g[4]), bc2(alpha));
-  const float ux = px + exy.x, uy = py + exy.y, uz = pz + ezt;
-  const float2 uu = mul2(make_float2(ux, uy), make_float2(ux, uy));
-  const float gt = 1.0f / sqrtf(1.0f + (uu.x + uu.y + uz * uz) * csqinv);
-  const float2 bt = mul2(bxy, bc2(gt));  // (bxt, byt)
-  const float bxt = bt.x, byt = bt.y, bzt = (g[5] * alpha) * gt;
-  const float2 bb = mul2(bt, bt);
-  const float boris = 2.0f * (1.0f / (1.0f + bb.x + bb.y + bzt * bzt));
+  const float ext = g[0] * beta, eyt = g[1] * beta, ezt = g[2] * beta;
+  const float bx0 = g[3] * alpha, by0 = g[4] * alpha;
+  const float ux = px + ext, uy = py + eyt, uz = pz + ezt;
+  const float gt = 1.0f / sqrtf(1.0f + (ux * ux + uy * uy + uz * uz) * csqinv);
+  const float bxt = bx0 * gt, byt = by0 * gt, bzt = (g[5] * alpha) * gt;
+  const float boris = 2.0f * (1.0f / (1.0f + bxt * bxt + byt * byt + bzt * bzt));
   // u' = u + u x B
-  const float2 p1 = mul2(make_float2(uy, uz), make_float2(bzt, bxt));  // (uy bzt, uz bxt)
-  const float2 p2 = mul2(make_float2(uz, ux), make_float2(byt, bzt));  // (uz byt, ux bzt)
-  const float2 p3 = mul2(make_float2(ux, uy), make_float2(byt, bxt));  // (ux byt, uy bxt)
-  const float uxt = ux + p1.x - p2.x;
-  const float uyt = uy + p1.y - p2.y;
-  const float uzt = uz + p3.x - p3.y;
+  const float uxt = ux + uy * bzt - uz * byt;
+  const float uyt = uy + uz * bxt - ux * bzt;
+  const float uzt = uz + ux * byt - uy * bxt;
   // p = u + boris (u' x B) + E
-  const float2 q1 = mul2(make_float2(uyt, uzt), make_float2(bzt, bxt));  // (uyt bzt, uzt bxt)
-  const float2 q2 = mul2(make_float2(uzt, uxt), make_float2(byt, bzt));  // (uzt byt, uxt bzt)
-  const float2 q3 = mul2(make_float2(uxt, uyt), make_float2(byt, bxt));  // (uxt byt, uyt bxt)
-  const float2 bxy2 = mul2(bc2(boris), make_float2(q1.x - q2.x, q1.y - q2.y));
-  const float bz2 = boris * (q3.x - q3.y);
-  px = ux + bxy2.x + exy.x;
-  py = uy + bxy2.y + exy.y;
-  pz = uz + bz2 + ezt;
-  const float2 pp = mul2(make_float2(px, py), make_float2(px, py));
-  psa = sqrtf(1.0f + (pp.x + pp.y + pz * pz) * csqinv);
+  px = ux + boris * (uyt * bzt - uzt * byt) + ext;
+  py = uy + boris * (uzt * bxt - uxt * bzt) + eyt;
+  pz = uz + boris * (uxt * byt - uyt * bxt) + ezt;
+  psa = sqrtf(1.0f + (px * px + py * py + pz * pz) * csqinv);
 }
 
 __device__ __forceinline__ float gamma_of(float px, float py, float pz, float csqinv) {
-  const float2 pp = mul2(make_float2(px, py), make_float2(px, py));
-  return sqrtf(1.0f + (pp.x + pp.y + pz * pz) * csqinv);  // src/prtls.rs:440
+  return sqrtf(1.0f + (px * px + py * py + pz * pz) * csqinv);  // src/prtls.rs:440
 }
 
 // update_position (src/prtls.rs:103-119) for one particle; inv = 1/psa.
 __device__ __forceinline__ void move_half(float c1, float px, float py, int& ix, int& iy, float& dx, float& dy) {
-  const float2 d = mul2(bc2(c1), make_float2(px, py));
+  const float2 d = make_float2(c1 * px, c1 * py);
   dx += d.x;
   if (dx >= 0.5f) {
     dx -= 1.0f;
@@ -634,9 +621,8 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
           move_half(c1, px, py, ix, iy, dx, dy);
           if (!inner_tile) bc_of<BC>(a, nx, ny, ix, iy, dx, px);
           {
-            const float2 vxy = mul2(mul2(bc2(q), make_float2(px, py)), bc2(inv));
-            vx = vxy.x;
-            vy = vxy.y;
+            vx = (q * px) * inv;
+            vy = (q * py) * inv;
           }
           vz = q * pz * inv;
           jcross = ix != ox || iy != oy;

@@ -32,8 +32,23 @@ def _member(kind, size_x, size_y, dens, n_pass):
 # mixed boundaries run the batch kernel's generic form, uniform ones its periodic / wall forms
 @pytest.mark.parametrize("kinds", [("periodic", "wall", "periodic"), ("periodic",) * 3, ("wall",) * 3])
 def test_batch_matches_single_simulations(kinds):
+    _batch_vs_singles([_member(kinds[0], 64, 32, 8, 4), _member(kinds[1], 128, 64, 4, 2),
+                       _member(kinds[2], 32, 32, 16, 4)])
+
+
+def test_batch_members_sharing_a_grid():
+    """The field phase runs once per group of members with one grid and pass count
+    (blockIdx.z = member): members of a group differ in density (the per-member
+    constants of the tables) and boundaries, pass counts split groups, and a pass count
+    beyond the fused filter (or none) takes the member-by-member fallback."""
+    _batch_vs_singles([_member("periodic", 64, 32, 8, 4), _member("wall", 64, 32, 4, 4),
+                       _member("periodic", 64, 32, 16, 4), _member("periodic", 64, 32, 8, 2),
+                       _member("periodic", 32, 32, 8, 0), _member("wall", 32, 32, 4, 17),
+                       _member("periodic", 32, 32, 8, 4)])
+
+
+def _batch_vs_singles(cfgs):
     from spectral_rs_b200 import Sim, Batch
-    cfgs = [_member(kinds[0], 64, 32, 8, 4), _member(kinds[1], 128, 64, 4, 2), _member(kinds[2], 32, 32, 16, 4)]
     species = []
     for k, cfg in enumerate(cfgs):
         p = cfg.params
