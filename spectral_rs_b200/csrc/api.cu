@@ -449,8 +449,14 @@ extern "C" int spx_add_species(spx_ctx* c, float charge, float mass, float vth, 
     if (c->plain) {
       for (float** p : {&s.plain.x, &s.plain.y, &s.plain.px, &s.plain.py, &s.plain.pz})
         SPX_CUDA_TRY(cudaMalloc(p, std::max<uint64_t>(n, 1) * 4));
-    } else if (c->prm.periodic_x) {
-      guess = capacity_for(c, n, (uint32_t)((n + c->pg.ncells() - 1) / c->pg.ncells()));
+    } else if (c->prm.slot_capacity >= 0) {
+      // the largest occupancy of a uniform plasma of mean m over N cells stays below
+      // m + sqrt(2 m ln N) (Poisson tail): slots for that are allocated while the copies
+      // run (allocating GBs of slots costs about as long as copying the particles) and
+      // replaced below only when the counts need more
+      const double m = (double)n / (double)c->pg.ncells();
+      const double ln = std::log(std::max(2.0, (double)c->pg.ncells()));
+      guess = capacity_for(c, n, (uint32_t)std::ceil(m + std::sqrt(2.0 * m * ln) + 2.0));
       slot_allocate(s, c->pg, guess.KL, guess.H, n);
     }
     uint32_t bad = 0;
@@ -463,9 +469,9 @@ extern "C" int spx_add_species(spx_ctx* c, float charge, float mass, float vth, 
     // pass 2: offsets and momenta into their slots (or the plain arrays)
     if (!c->plain) {
       const Capacity cap = choose_capacity(c, n);
-      if (cap.KL != guess.KL || cap.H != guess.H) {
+      if (cap.KL > guess.KL || cap.H > guess.H) {
         slot_release(s);
-        slot_allocate(s, c->pg, cap.KL, cap.H, n);
+        slot_allocate(s, c->pg, std::max(cap.KL, guess.KL), std::max(cap.H, guess.H), n);
       }
       slot_scatter_begin(s, c->pg, c->d_counts, c->st);
     }
