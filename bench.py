@@ -670,13 +670,15 @@ def e2e_ensemble(members, idx, steps):
     t2 = time.perf_counter()
     b.step(steps)
     t3 = time.perf_counter()
-    off, diags = 0, []
-    for sim in b.sims:
-        c = sim.size_x * sim.size_y
-        for name in names:
-            sim.flds.spatial(name, with_ghosts=False, out=pin_o[off:off + c].reshape(sim.size_y, sim.size_x))
+    off = 0
+    for name in names:  # one spx_batch_get_field per field: every member's copy, one synchronisation
+        outs = []
+        for sim in b.sims:
+            c = sim.size_x * sim.size_y
+            outs.append(pin_o[off:off + c].reshape(sim.size_y, sim.size_x))
             off += c
-        diags.append(sim.diag())
+        b.get_field(name, with_ghosts=False, out=outs)
+    diags = [sim.diag() for sim in b.sims]
     dt = time.perf_counter() - t0
     b.close()
     h2d = 40 * n  # ix, iy (8 B each), dx, dy, px, py, pz, psa (4 B each) per particle
@@ -685,7 +687,8 @@ def e2e_ensemble(members, idx, steps):
             "d2h_bytes_per_step": d2h / steps, "wall_s": dt,
             "split_s": {"upload": t1 - t0, "prepare": t2 - t1, "steps": t3 - t2, "readback": t0 + dt - t3},
             "scope": "pinned host arrays -> spx_add_species (2 per member) -> spx_batch_prepare -> "
-                     "spx_batch_step(K) -> 10 fields per member (into pinned host buffers) + spx_diag per member"}
+                     "spx_batch_step(K) -> 10 fields of every member (spx_batch_get_field into pinned host "
+                     "buffers) + spx_diag per member"}
 
 
 def run_ensemble(args):

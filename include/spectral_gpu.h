@@ -250,6 +250,11 @@ SPX_API int spx_batch_step(spx_batch* batch, uint32_t n);
  * over the last spx_batch_step call. */
 SPX_API int spx_batch_set_timing(spx_batch* batch, int32_t enable);
 SPX_API int spx_batch_get_timing(spx_batch* batch, float* out2);
+/* Field `field` of every simulation of the batch, out[i] for simulation i (each
+ * laid out as spx_get_field's output), queued together and synchronised once
+ * (spx_get_field per simulation synchronises per call).  Page-locked outputs
+ * let the copies run back to back. */
+SPX_API int spx_batch_get_field(spx_batch* batch, int32_t field, int32_t with_ghosts, float* const* out);
 SPX_API void* spx_batch_get_stream(const spx_batch* batch);
 /* Kernels launched by the last spx_batch_step call (inside its graphs, one by one). */
 SPX_API uint64_t spx_batch_last_launch_count(const spx_batch* batch);

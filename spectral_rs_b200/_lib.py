@@ -32,7 +32,7 @@ EXPORTS = [
     "spx_field_op", "spx_fft2d", "spx_set_timing", "spx_get_timing", "spx_last_launch_count",
     "spx_get_stream", "spx_get_counters", "spx_filter_noalloc", "spx_noalloc_last_error",
     "spx_batch_create", "spx_batch_destroy", "spx_batch_last_error", "spx_batch_sim", "spx_batch_prepare",
-    "spx_batch_step", "spx_batch_set_timing", "spx_batch_get_timing", "spx_batch_get_stream",
+    "spx_batch_step", "spx_batch_set_timing", "spx_batch_get_timing", "spx_batch_get_field", "spx_batch_get_stream",
     "spx_batch_last_launch_count",
 ]
 
@@ -120,6 +120,7 @@ def load():
         "spx_batch_step": (ctypes.c_int, [P, ctypes.c_uint32]),
         "spx_batch_set_timing": (ctypes.c_int, [P, ctypes.c_int32]),
         "spx_batch_get_timing": (ctypes.c_int, [P, P]),
+        "spx_batch_get_field": (ctypes.c_int, [P, ctypes.c_int32, ctypes.c_int32, P]),
         "spx_batch_get_stream": (ctypes.c_void_p, [P]),
         "spx_batch_last_launch_count": (ctypes.c_uint64, [P]),
     }

@@ -435,6 +435,14 @@ extern "C" int spx_add_species(spx_ctx* c, float charge, float mass, float vth, 
           k_pack_check<<<148 * 4, 256, 0, c->st>>>(m, off, bx, bx + m, c->g.nx, c->g.ny, cell + off, c->d_u32);
           if (!c->plain) slot_count(c->pg, m, cell + off, c->d_counts, c->st, false);
         });
+    // the first bad index and (slots) the fullest cell's count, read back together below
+    uint32_t hb[2] = {0, 0};
+    if (!c->plain) {
+      SPX_CUDA_TRY(cudaMemsetAsync(c->d_u32 + 1, 0, sizeof(uint32_t), c->st));
+      Species tmp;
+      tmp.slot.nlow = c->d_counts;
+      slot_max_occupancy(tmp, c->pg, c->d_u32 + 1, c->st);
+    }
     // the destination arrays are allocated while pass 1's copies run: the plain
     // arrays, or (periodic grids) the slots for the occupancy of a uniform
     // species, replaced below if the counts ask for more
@@ -459,16 +467,18 @@ extern "C" int spx_add_species(spx_ctx* c, float charge, float mass, float vth, 
       guess = capacity_for(c, n, (uint32_t)std::ceil(m + std::sqrt(2.0 * m * ln) + 2.0));
       slot_allocate(s, c->pg, guess.KL, guess.H, n);
     }
-    uint32_t bad = 0;
-    SPX_CUDA_TRY(cudaMemcpyAsync(&bad, c->d_u32, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
+    // (a read-back into pageable memory returns once the copy is done, so it comes after
+    // the allocation)
+    SPX_CUDA_TRY(cudaMemcpyAsync(hb, c->d_u32, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->st));
     SPX_CUDA_TRY(cudaStreamSynchronize(c->st));
+    const uint32_t bad = hb[0];
     if (bad != 0xFFFFFFFFu) {
       release();
       return fail(c, SPX_ERR_BOUNDS, "particle " + std::to_string(bad) + " outside the grid");
     }
     // pass 2: offsets and momenta into their slots (or the plain arrays)
     if (!c->plain) {
-      const Capacity cap = choose_capacity(c, n);
+      const Capacity cap = capacity_for(c, n, hb[1]);
       if (cap.KL > guess.KL || cap.H > guess.H) {
         slot_release(s);
         slot_allocate(s, c->pg, std::max(cap.KL, guess.KL), std::max(cap.H, guess.H), n);
@@ -1489,6 +1499,30 @@ extern "C" int spx_batch_get_timing(spx_batch* b, float* out2) {
   if (!b || !out2) return SPX_ERR_ARG;
   out2[0] = b->last_ms[0];
   out2[1] = b->last_ms[1];
+  return SPX_OK;
+}
+
+extern "C" int spx_batch_get_field(spx_batch* b, int32_t field, int32_t with_ghosts, float* const* out) {
+  if (!b || !out) return SPX_ERR_ARG;
+  if (field < 0 || field >= SPX_NUM_FIELDS) return bfail(b, SPX_ERR_ARG, "no such field");
+  for (size_t i = 0; i < b->sims.size(); ++i)
+    if (!out[i]) return bfail(b, SPX_ERR_ARG, "null output for simulation " + std::to_string(i));
+  try {
+    // every member's copy queued on the batch stream, one synchronisation for all
+    for (size_t i = 0; i < b->sims.size(); ++i) {
+      spx_ctx* c = b->sims[i];
+      SPX_CUDA_TRY(cudaStreamSynchronize(c->st));  // work queued on the member's own stream
+      const float* src = c->fb.spatial[field];
+      if (with_ghosts)
+        SPX_CUDA_TRY(cudaMemcpyAsync(out[i], src, c->g.spatial_size() * 4, cudaMemcpyDeviceToHost, b->st));
+      else  // interior rows (save_fld_spatial, src/save/mod.rs:14-17)
+        SPX_CUDA_TRY(cudaMemcpy2DAsync(out[i], c->g.nx * 4, src + c->g.W + 1, c->g.W * 4, c->g.nx * 4, c->g.ny,
+                                       cudaMemcpyDeviceToHost, b->st));
+    }
+    SPX_CUDA_TRY(cudaStreamSynchronize(b->st));
+  } catch (const spx::Error& e) {
+    return bfail(b, e.code, e.msg);
+  }
   return SPX_OK;
 }
 

@@ -367,6 +367,22 @@ class Batch:
         self._chk(self.lib.spx_batch_get_timing(self._b, _lib.ptr(out)))
         return out
 
+    def get_field(self, name, with_ghosts=True, out=None):
+        """Field `name` of every member (spx_batch_get_field): a list of float32 (rows, cols)
+        arrays, into `out` when given (one C-contiguous float32 array per member, e.g.
+        page-locked buffers)."""
+        shapes = [((s.size_y + 2, s.size_x + 2) if with_ghosts else (s.size_y, s.size_x)) for s in self.sims]
+        if out is None:
+            out = [np.empty(sh, dtype=np.float32) for sh in shapes]
+        if len(out) != len(shapes):
+            raise ValueError(f"out must hold {len(shapes)} arrays")
+        for o, sh in zip(out, shapes):
+            if o.shape != sh or o.dtype != np.float32 or not o.flags["C_CONTIGUOUS"]:
+                raise ValueError(f"each out array must be C-contiguous float32 of its member's shape {sh}")
+        ptrs = (ctypes.c_void_p * len(out))(*[o.ctypes.data for o in out])
+        self._chk(self.lib.spx_batch_get_field(self._b, _lib.FIELD_IDS[name], 1 if with_ghosts else 0, ptrs))
+        return out
+
     def stream(self):
         return int(self.lib.spx_batch_get_stream(self._b) or 0)
 

@@ -73,6 +73,10 @@ def _batch_vs_singles(cfgs):
         b.set_timing(False)
         b.step(5)
         assert b.timing()[1] > 0
+        for ghosts in (True, False):  # the batched read-back equals each member's own
+            for name in ("Ex", "Jy", "Dens"):
+                for x, bs in zip(b.get_field(name, with_ghosts=ghosts), b.sims):
+                    assert np.array_equal(x, bs.flds.spatial(name, with_ghosts=ghosts)), (name, ghosts)
         for s, bs in zip(singles, b.sims):
             for name in ("Ex", "Ey", "Bz", "Jx", "Dens"):
                 x, y = bs.flds.spatial(name), s.flds.spatial(name)
