@@ -481,11 +481,19 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
   if (MOVE)
     for (int i = c; i < NWP * WN; i += TC) win[i] = 0.f;
   if (PUSH) {
+    // thread c stages window cells c, c + TC, ...: its (row, column) advances without divisions
+    const int s_r = TC / EX, s_q = TC - s_r * EX;
+    int r = c / EX, q = c - (c / EX) * EX;
     for (int i = c; i < EY * EX; i += TC) {
-      const int r = i / EX, q = i - r * EX;
       const size_t g = (size_t)(ty * TYc + r) * W + (tx * TXc + q);
       eb4[i] = make_float4(__ldg(a.f.E[0] + g), __ldg(a.f.E[1] + g), __ldg(a.f.E[2] + g), __ldg(a.f.B[0] + g));
       eb2[i] = make_float2(__ldg(a.f.B[1] + g), __ldg(a.f.B[2] + g));
+      q += s_q;
+      r += s_r;
+      if (q >= EX) {
+        q -= EX;
+        ++r;
+      }
     }
   }
   __syncthreads();
@@ -791,17 +799,27 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
       }
   }
   __syncthreads();
-  // window -> global (clipped to the ghosted grid)
-  for (int i = c; i < 5 * WN; i += TC) {
-    float v = win[i];
-    if (COMP && i < 3 * WN) v += win[i + 5 * WN];  // one rounding of sum + compensation
-    if (v == 0.f) continue;
-    const int plane = i / WN, k = i - plane * WN;
-    const int wy = k / WX, wx = k - wy * WX;
-    const int gx = wx0 + wx, gy = wy0 + wy;
-    if (gx < 0 || gx > nx + 1 || gy < 0 || gy > ny + 1) continue;
+  // window -> global (clipped to the ghosted grid): thread c flushes cells c, c + TC, ... of
+  // each plane, its (row, column) advanced without divisions
+  const int s_wy = TC / WX, s_wx = TC - s_wy * WX;
+  const int c_wy = c / WX, c_wx = c - c_wy * WX;
+#pragma unroll 1
+  for (int plane = 0; plane < 5; ++plane) {
     float* d = plane == 0 ? a.f.J[0] : plane == 1 ? a.f.J[1] : plane == 2 ? a.f.J[2] : plane == 3 ? a.f.dsty : a.f.dens;
-    atomicAdd(d + (size_t)gy * W + gx, v);
+    const float* wp = win + plane * WN;
+    int wx = c_wx, wy = c_wy;
+    for (int k = c; k < WN; k += TC) {
+      float v = wp[k];
+      if (COMP && plane < 3) v += wp[k + 5 * WN];  // one rounding of sum + compensation
+      const int gx = wx0 + wx, gy = wy0 + wy;
+      if (v != 0.f && gx >= 0 && gx <= nx + 1 && gy >= 0 && gy <= ny + 1) atomicAdd(d + (size_t)gy * W + gx, v);
+      wx += s_wx;
+      wy += s_wy;
+      if (wx >= WX) {
+        wx -= WX;
+        ++wy;
+      }
+    }
   }
 }
 
