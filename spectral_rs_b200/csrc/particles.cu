@@ -435,13 +435,14 @@ __device__ __forceinline__ void bc_of(const StepArgs& a, int nx, int ny, int& ix
   }
 }
 
-// BC: see bc_of.  T16: tiles of 16 x 16 cells (compile-time index arithmetic; else from a).
+// BC: see bc_of.  TS: square tiles of TS x TS cells known at compile time (16 or 8: the
+// index arithmetic folds), 0: the tile shape from a.
 // Species [s0, s1) of the step (all of them, or one per CTA when a small grid
 // splits the species across CTAs).
-template <bool PUSH, bool MOVE, bool COMP = false, int BC = BC_ANY, bool T16 = false>
+template <bool PUSH, bool MOVE, bool COMP = false, int BC = BC_ANY, int TS = 0>
 __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, float* smem, const int s0,
                                           const int s1) {
-  const int TXc = T16 ? 16 : a.TX, TYc = T16 ? 16 : a.TY, logTXc = T16 ? 4 : a.logTX;
+  const int TXc = TS ? TS : a.TX, TYc = TS ? TS : a.TY, logTXc = TS == 16 ? 4 : TS == 8 ? 3 : a.logTX;
   const int TC = TXc * TYc;
   const int tx = tile % a.NTX, ty = tile / a.NTX;
   const int c = threadIdx.x;
@@ -824,12 +825,12 @@ __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, flo
 }
 
 // One simulation: one CTA per tile.
-template <bool PUSH, bool MOVE, int BC, bool T16>
+template <bool PUSH, bool MOVE, int BC, int TS>
 __global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS) k_slot(const __grid_constant__ StepArgs a) {
   extern __shared__ float smem[];
   // gridDim.y > 1: CTA (tile, s) handles species s of the tile only
   const int s0 = gridDim.y > 1 ? (int)blockIdx.y : 0, s1 = gridDim.y > 1 ? s0 + 1 : a.ns;
-  slot_tile<PUSH, MOVE, false, BC, T16>(a, blockIdx.x, smem, s0, s1);
+  slot_tile<PUSH, MOVE, false, BC, TS>(a, blockIdx.x, smem, s0, s1);
 }
 
 // Compensated current sums: the extra registers allow one 256-thread CTA per SM.
@@ -840,8 +841,8 @@ __global__ void __launch_bounds__(256, 1) k_slot_comp(const __grid_constant__ St
   slot_tile<PUSH, true, true, BC>(a, blockIdx.x, smem, s0, s1);
 }
 
-// the instantiation for (push, move, compensated, boundaries, 16 x 16 tiles)
-template <int BC, bool T16>
+// the instantiation for (push, move, compensated, boundaries, tile shape)
+template <int BC, int TS>
 static void launch_slot(bool push, bool move, bool comp, dim3 grid, int threads, size_t smem, cudaStream_t st,
                         const StepArgs& a) {
   if (comp && push)
@@ -849,17 +850,17 @@ static void launch_slot(bool push, bool move, bool comp, dim3 grid, int threads,
   else if (comp)
     k_slot_comp<false, BC><<<grid, threads, smem, st>>>(a);
   else if (push && move)
-    k_slot<true, true, BC, T16><<<grid, threads, smem, st>>>(a);
+    k_slot<true, true, BC, TS><<<grid, threads, smem, st>>>(a);
   else if (push)
-    k_slot<true, false, BC, T16><<<grid, threads, smem, st>>>(a);
+    k_slot<true, false, BC, TS><<<grid, threads, smem, st>>>(a);
   else if (move)
-    k_slot<false, true, BC, T16><<<grid, threads, smem, st>>>(a);
+    k_slot<false, true, BC, TS><<<grid, threads, smem, st>>>(a);
 }
 
 // Many simulations: persistent CTAs take (simulation, tile) items from a work
 // queue (an atomic counter over a list sorted by decreasing work), so uneven
 // grids and particle counts share one launch and balance across the SMs.
-template <bool PUSH, bool MOVE, int BC, bool T16>
+template <bool PUSH, bool MOVE, int BC, int TS>
 __global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS)
     k_slot_batch(const StepArgs* __restrict__ args, const int2* __restrict__ items, int nitems, int* counter) {
   extern __shared__ float smem[];
@@ -871,7 +872,7 @@ __global__ void __launch_bounds__(256, SPX_SLOT_MIN_BLOCKS)
     __syncthreads();
     if (it >= nitems) break;
     const int2 item = items[it];
-    slot_tile<PUSH, MOVE, false, BC, T16>(args[item.x], item.y, smem, 0, args[item.x].ns);
+    slot_tile<PUSH, MOVE, false, BC, TS>(args[item.x], item.y, smem, 0, args[item.x].ns);
     __syncthreads();  // the shared windows are reused by the next item
   }
 }
@@ -1017,31 +1018,37 @@ static SpeciesArgs species_args(Species& sp) {
   return A;
 }
 
-template <int BC, bool T16>
+template <int BC, int TS>
 static void set_batch_attributes() {
-  for (const void* f : {(const void*)k_slot_batch<true, true, BC, T16>, (const void*)k_slot_batch<true, false, BC, T16>,
-                        (const void*)k_slot_batch<false, true, BC, T16>})
+  for (const void* f : {(const void*)k_slot_batch<true, true, BC, TS>, (const void*)k_slot_batch<true, false, BC, TS>,
+                        (const void*)k_slot_batch<false, true, BC, TS>})
     SPX_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
 }
-template <int BC, bool T16>
+template <int BC, int TS>
 static void set_single_attributes() {
-  for (const void* f : {(const void*)k_slot<true, true, BC, T16>, (const void*)k_slot<true, false, BC, T16>,
-                        (const void*)k_slot<false, true, BC, T16>, (const void*)k_slot_comp<true, BC>,
+  for (const void* f : {(const void*)k_slot<true, true, BC, TS>, (const void*)k_slot<true, false, BC, TS>,
+                        (const void*)k_slot<false, true, BC, TS>, (const void*)k_slot_comp<true, BC>,
                         (const void*)k_slot_comp<false, BC>})
     SPX_CUDA_TRY(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
 }
 
+template <int TS>
+static void set_attributes() {
+  set_single_attributes<BC_PERIODIC, TS>();
+  set_single_attributes<BC_WALL, TS>();
+  set_batch_attributes<BC_ANY, TS>();
+  set_batch_attributes<BC_PERIODIC, TS>();
+  set_batch_attributes<BC_WALL, TS>();
+}
 void slot_set_kernel_attributes() {
-  set_single_attributes<BC_PERIODIC, false>();
-  set_single_attributes<BC_PERIODIC, true>();
-  set_single_attributes<BC_WALL, false>();
-  set_single_attributes<BC_WALL, true>();
-  set_batch_attributes<BC_ANY, false>();
-  set_batch_attributes<BC_ANY, true>();
-  set_batch_attributes<BC_PERIODIC, false>();
-  set_batch_attributes<BC_PERIODIC, true>();
-  set_batch_attributes<BC_WALL, false>();
-  set_batch_attributes<BC_WALL, true>();
+  set_attributes<0>();
+  set_attributes<8>();
+  set_attributes<16>();
+}
+
+// compile-time tile side of a tile shape: 16, 8, or 0 (any other shape)
+static int tile_side(const ParticleGeom& pg) {
+  return pg.TX == 16 && pg.TY == 16 ? 16 : pg.TX == 8 && pg.TY == 8 ? 8 : 0;
 }
 
 int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysParams& pp, const FieldPtrs& fp,
@@ -1065,20 +1072,20 @@ int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysPar
   const int TC = pg.TC();
   const bool comp = pp.compensated && move;
   const size_t smem = slot_smem_floats(pg.TX, pg.TY, push, move, comp) * sizeof(float);
-  const bool t16 = pg.TX == 16 && pg.TY == 16;
+  const int ts = tile_side(pg);
   // a grid whose tiles fill less than one wave of CTAs (148 SMs x 512 threads)
   // takes one CTA per (tile, species): the species' particles are independent and
   // the CTAs' deposit windows are added into the fields with atomics anyway
   const bool split = a.ns > 1 && (size_t)pg.ntiles() * TC < (size_t)148 * 512;
   const dim3 grid(pg.ntiles(), split ? a.ns : 1);
-  if (pp.periodic_x && t16)
-    launch_slot<BC_PERIODIC, true>(push, move, comp, grid, TC, smem, st, a);
-  else if (pp.periodic_x)
-    launch_slot<BC_PERIODIC, false>(push, move, comp, grid, TC, smem, st, a);
-  else if (t16)
-    launch_slot<BC_WALL, true>(push, move, comp, grid, TC, smem, st, a);
+  if (pp.periodic_x)
+    ts == 16 ? launch_slot<BC_PERIODIC, 16>(push, move, comp, grid, TC, smem, st, a)
+    : ts == 8 ? launch_slot<BC_PERIODIC, 8>(push, move, comp, grid, TC, smem, st, a)
+              : launch_slot<BC_PERIODIC, 0>(push, move, comp, grid, TC, smem, st, a);
   else
-    launch_slot<BC_WALL, false>(push, move, comp, grid, TC, smem, st, a);
+    ts == 16 ? launch_slot<BC_WALL, 16>(push, move, comp, grid, TC, smem, st, a)
+    : ts == 8 ? launch_slot<BC_WALL, 8>(push, move, comp, grid, TC, smem, st, a)
+              : launch_slot<BC_WALL, 0>(push, move, comp, grid, TC, smem, st, a);
   ++launches;
   for (int s = 0; s < a.ns; ++s) {
     // the overflow fallback reads its count on the device; a small fixed grid covers it
@@ -1160,15 +1167,15 @@ void slot_batch_build(SlotBatch& b, const std::vector<SlotBatchSim>& sims) {
   b.grid = std::max(1, std::min(b.nitems, std::max(per_sm, 1) * nsm));
 }
 
-template <int BC, bool T16>
+template <int BC, int TS>
 static void launch_batch(bool push, bool move, const SlotBatch& b, int TC, size_t smem, cudaStream_t st,
                          const StepArgs* args) {
   if (push && move)
-    k_slot_batch<true, true, BC, T16><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
+    k_slot_batch<true, true, BC, TS><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
   else if (push)
-    k_slot_batch<true, false, BC, T16><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
+    k_slot_batch<true, false, BC, TS><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
   else
-    k_slot_batch<false, true, BC, T16><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
+    k_slot_batch<false, true, BC, TS><<<b.grid, TC, smem, st>>>(args, b.d_items, b.nitems, b.d_counter);
 }
 
 int slot_batch_step(SlotBatch& b, std::vector<SlotBatchSim>& sims, bool push, bool move, cudaStream_t st) {
@@ -1179,22 +1186,24 @@ int slot_batch_step(SlotBatch& b, std::vector<SlotBatchSim>& sims, bool push, bo
   int launches = 0;
   k_batch_reset<<<(b.nsims + 255) / 256, 256, 0, st>>>(args, b.nsims, b.d_counter);
   ++launches;
-  const bool t16 = sims[0].pg.TX == 16 && sims[0].pg.TY == 16;  // one tile shape for the whole batch
+  const int ts = tile_side(sims[0].pg);  // one tile shape for the whole batch
   bool all_periodic = true, all_wall = true;
   for (auto& m : sims) {
     all_periodic = all_periodic && m.pp.periodic_x;
     all_wall = all_wall && !m.pp.periodic_x;
   }
   const int bc = all_periodic ? BC_PERIODIC : all_wall ? BC_WALL : BC_ANY;
+#define SPX_BATCH(BCV)                                                     \
+  (ts == 16  ? launch_batch<BCV, 16>(push, move, b, TC, smem, st, args)    \
+   : ts == 8 ? launch_batch<BCV, 8>(push, move, b, TC, smem, st, args)     \
+             : launch_batch<BCV, 0>(push, move, b, TC, smem, st, args))
   if (bc == BC_PERIODIC)
-    t16 ? launch_batch<BC_PERIODIC, true>(push, move, b, TC, smem, st, args)
-        : launch_batch<BC_PERIODIC, false>(push, move, b, TC, smem, st, args);
+    SPX_BATCH(BC_PERIODIC);
   else if (bc == BC_WALL)
-    t16 ? launch_batch<BC_WALL, true>(push, move, b, TC, smem, st, args)
-        : launch_batch<BC_WALL, false>(push, move, b, TC, smem, st, args);
+    SPX_BATCH(BC_WALL);
   else
-    t16 ? launch_batch<BC_ANY, true>(push, move, b, TC, smem, st, args)
-        : launch_batch<BC_ANY, false>(push, move, b, TC, smem, st, args);
+    SPX_BATCH(BC_ANY);
+#undef SPX_BATCH
   ++launches;
   const dim3 og(16, b.nsims);
   if (push && move)
