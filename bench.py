@@ -580,6 +580,7 @@ def measure_ensemble(members, idx, steps, warmup, dist=None, sampler=None, timed
     n_particles = sum(len(p) for s in b.sims for p in s.prtls)
     cells = sum(members[i]["size_x"] * members[i]["size_y"] for i in idx)
     b.prepare()
+    device_bytes = b.sims[0].counters()["device_bytes"]  # the device's memory in use (all members)
     b.step(warmup)
     stream = torch.cuda.ExternalStream(b.stream())
     _barrier(dist)
@@ -598,7 +599,7 @@ def measure_ensemble(members, idx, steps, warmup, dist=None, sampler=None, timed
     part_ms, step_ms = (float(x) / timed_steps for x in b.timing())
     b.close()
     return {"particles": n_particles, "cells": cells, "ms": ms, "launches": launches, "clocks": clocks,
-            "phase_ms_per_step": {"particles": part_ms, "step": step_ms},
+            "device_bytes": device_bytes, "phase_ms_per_step": {"particles": part_ms, "step": step_ms},
             "roofline": roofline(n_particles, cells, part_ms,
                                  "k_slot_batch<push,move> (persistent fused push + move + deposit over all members)",
                                  "k_slot_batch_traffic.json")}
@@ -729,6 +730,7 @@ def run_ensemble(args):
                                "vth": 0.1, "c": 3.0, "dt": 0.1, "n_pass": 4, "delta": 8, "walls": "right + left",
                                "path": "split, batched (persistent work-queue particle kernel, one graph per step)",
                                "tile": list(tile) if tile else [8, 8],
+                               "device_gb": round(r["device_bytes"] / 1e9, 2),
                                "parallelism": f"member list partitioned over {world} ranks" if world > 1 else "single",
                                "l2": _l2_note(r["particles"])})
         line.update({"roofline": r["roofline"], "phase_ms_per_step": r["phase_ms_per_step"], "plain_fp32": plain,

@@ -334,9 +334,9 @@ static Capacity capacity_for(const spx_ctx* c, uint64_t n, uint32_t mx) {
   const double f = c->prm.slot_headroom > 0 ? (double)c->prm.slot_headroom : 1.25;
   int KL = (int)std::ceil(std::max(f * mx, mean + 8.0 * std::sqrt(mean))) + 8;
   // a reflecting wall piles incoming and reflected particles up (a shock
-  // compresses the plasma about fourfold): by default leave room for that from the start
-  if (!c->prm.periodic_x && !(c->prm.slot_headroom > 0))
-    KL = std::max(KL, (int)std::ceil(4.0 * mx + 8.0 * std::sqrt(4.0 * mx)) + 8);
+  // compresses the plasma about fourfold): by default leave room for that from the
+  // start, four times the fullest cell (which already holds the Poisson excess)
+  if (!c->prm.periodic_x && !(c->prm.slot_headroom > 0)) KL = std::max(KL, (int)std::ceil(4.0 * mx) + 8);
   if (c->prm.slot_capacity > 0) KL = std::max(KL, c->prm.slot_capacity);
   // arrivals of one step: a few per cent of the occupancy in a thermal plasma,
   // a few tens in a fast flow
