@@ -218,7 +218,8 @@ SPX_API void* spx_get_stream(const spx_ctx* ctx);
 /* Layout and overflow counters: out8[0] slot repacks so far, [1] particles in
  * overflow lists at the last check, [2] largest cell occupancy at the last
  * check, [3] slot capacity K of species 0, [4] tiles, [5] cells per tile,
- * [6] kernel launches of the last spx_step call, [7] device bytes held. */
+ * [6] kernel launches of the last spx_step call, [7] device memory in use (total - free:
+ * every context on the device). */
 SPX_API int spx_get_counters(const spx_ctx* ctx, uint64_t* out8);
 /* Number of kernel launches issued by the last spx_step call (the kernels of a
  * step launched as a CUDA graph counted one by one). */

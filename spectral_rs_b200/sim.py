@@ -159,7 +159,8 @@ class Sim:
         return int(self.lib.spx_last_launch_count(self._ctx))
 
     def counters(self):
-        """dict of slot-layout counters (repacks, overflow, occupancy, K, tiles, launches, device bytes)."""
+        """dict of slot-layout counters (repacks, overflow, occupancy, K, tiles, launches, device memory
+        in use: total - free, every context on the device)."""
         out = np.zeros(8, dtype=np.uint64)
         self._chk(self.lib.spx_get_counters(self._ctx, _lib.ptr(out)))
         keys = ("repacks", "overflow", "max_occupancy", "slot_capacity", "tiles", "cells_per_tile",
