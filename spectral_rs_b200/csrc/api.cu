@@ -143,8 +143,11 @@ static int fail(spx_ctx* c, int code, const std::string& m) {
   return code;
 }
 
+// Every call on a context runs on the context's device (the CUDA runtime's current
+// device is per host thread).
 #define SPX_GUARD(ctx, ...)                           \
   try {                                               \
+    SPX_CUDA_TRY(cudaSetDevice((ctx)->prm.device));   \
     __VA_ARGS__;                                      \
   } catch (const spx::Error& e) {                     \
     return fail(ctx, e.code, e.msg);                  \
@@ -1335,6 +1338,7 @@ static void capture_batch_steady_state(spx_batch* b);
 
 extern "C" int spx_batch_prepare(spx_batch* b) {
   if (!b) return SPX_ERR_ARG;
+  if (cudaSetDevice(b->sims[0]->prm.device) != cudaSuccess) return bfail(b, SPX_ERR_CUDA, "cudaSetDevice failed");
   for (size_t i = 0; i < b->sims.size(); ++i) {
     spx_ctx* c = b->sims[i];
     if (c->species.empty()) return bfail(b, SPX_ERR_STATE, "simulation " + std::to_string(i) + " has no species");
@@ -1431,6 +1435,7 @@ static void capture_batch_steady_state(spx_batch* b) {
 
 extern "C" int spx_batch_step(spx_batch* b, uint32_t steps) {
   if (!b) return SPX_ERR_ARG;
+  if (cudaSetDevice(b->sims[0]->prm.device) != cudaSuccess) return bfail(b, SPX_ERR_CUDA, "cudaSetDevice failed");
   if (!b->built) return bfail(b, SPX_ERR_STATE, "spx_batch_prepare first");
   try {
     // the batch advances in lock-step: same region parity and pending push
@@ -1508,6 +1513,7 @@ extern "C" int spx_batch_get_field(spx_batch* b, int32_t field, int32_t with_gho
   for (size_t i = 0; i < b->sims.size(); ++i)
     if (!out[i]) return bfail(b, SPX_ERR_ARG, "null output for simulation " + std::to_string(i));
   try {
+    SPX_CUDA_TRY(cudaSetDevice(b->sims[0]->prm.device));
     // every member's copy queued on the batch stream, one synchronisation for all
     for (size_t i = 0; i < b->sims.size(); ++i) {
       spx_ctx* c = b->sims[i];

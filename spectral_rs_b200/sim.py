@@ -15,12 +15,26 @@ map onto this module as follows:
 All state lives in device memory; getters copy back in the reference layout.
 """
 import ctypes
+import sys
 
 import numpy as np
 
 from . import _lib
 from .config import Config
 from .init import species_arrays
+
+
+def device_index():
+    """The CUDA device new contexts are created on: PyTorch's current device when the caller
+    has loaded torch (one process per GPU under torchrun sets it from LOCAL_RANK), else 0.
+    The library keeps its own CUDA runtime state, so the index is passed to it explicitly."""
+    torch = sys.modules.get("torch")
+    try:
+        if torch is not None and torch.cuda.is_available():
+            return int(torch.cuda.current_device())
+    except Exception:
+        pass
+    return 0
 
 
 def _layout_choice(cfg, tile):
@@ -58,7 +72,7 @@ class Sim:
             gamma_inj=p.gamma_inj, n_pass=p.n_pass, periodic_x=1 if p.periodic_x else 0,
             left_wall=1 if p.left_wall else 0,
             path=_lib.PATH_PLAIN if (path or p.path) == "plain" else _lib.PATH_SPLIT,
-            tile_x=tx, tile_y=ty, slot_capacity=p.slot_capacity, device=0,
+            tile_x=tx, tile_y=ty, slot_capacity=p.slot_capacity, device=device_index(),
             compensated=1 if p.compensated else 0, slot_headroom=headroom, arrival_slots=arrival)
         self.layout = {"tile": (tx, ty), "slot_headroom": headroom, "arrival_slots": arrival}
         self._ctx = ctypes.c_void_p()
@@ -341,7 +355,7 @@ class Batch:
                 size_x=p.size_x, size_y=p.size_y, delta=p.delta, dt=p.dt, c=p.c, dens=p.dens,
                 gamma_inj=p.gamma_inj, n_pass=p.n_pass, periodic_x=1 if p.periodic_x else 0,
                 left_wall=1 if p.left_wall else 0, path=_lib.PATH_SPLIT, tile_x=tx, tile_y=ty,
-                slot_capacity=p.slot_capacity, device=0, slot_headroom=headroom, arrival_slots=arrival)
+                slot_capacity=p.slot_capacity, device=device_index(), slot_headroom=headroom, arrival_slots=arrival)
         self._b = ctypes.c_void_p()
         code = self.lib.spx_batch_create(len(cfgs), prms, ctypes.byref(self._b))
         if code:

@@ -96,3 +96,18 @@ def test_ensemble_cpu_sample_is_bounded():
     assert idx == list(range(len(idx))) and n >= bench.CPU_SAMPLE_PARTICLES
     assert n - bench.member_particles(members[idx[-1]]) < bench.CPU_SAMPLE_PARTICLES
     assert sum(bench.member_particles(m) for m in members) == 265_764_864
+
+
+def test_device_index_follows_torch(monkeypatch):
+    """Contexts are created on the caller's torch device (one process per GPU under torchrun
+    selects it with torch.cuda.set_device(LOCAL_RANK)); without torch, device 0."""
+    import sys
+    import types
+    from spectral_rs_b200.sim import device_index
+    fake = types.SimpleNamespace(cuda=types.SimpleNamespace(is_available=lambda: True, current_device=lambda: 3))
+    monkeypatch.setitem(sys.modules, "torch", fake)
+    assert device_index() == 3
+    fake.cuda.is_available = lambda: False
+    assert device_index() == 0
+    monkeypatch.delitem(sys.modules, "torch")
+    assert device_index() == 0
