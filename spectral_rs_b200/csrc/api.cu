@@ -447,8 +447,8 @@ extern "C" int spx_add_species(spx_ctx* c, float charge, float mass, float vth, 
       slot_max_occupancy(tmp, c->pg, c->d_u32 + 1, c->st);
     }
     // the destination arrays are allocated while pass 1's copies run: the plain
-    // arrays, or (periodic grids) the slots for the occupancy of a uniform
-    // species, replaced below if the counts ask for more
+    // arrays, or the slots for a bound on the occupancy of a uniform species,
+    // replaced below only if the counts ask for more
     auto release = [&]() {
       slot_release(s);
       for (float** p : {&s.plain.x, &s.plain.y, &s.plain.px, &s.plain.py, &s.plain.pz}) {
