@@ -188,12 +188,15 @@ def profile_counters(name):
 
 
 def roofline(particles, cells, kern_ms, kernel, traffic_file):
+    """traffic_file: the committed capture of this kernel on this workload (scaled to the
+    launch), or None when no capture of the workload exists (traffic and counters null)."""
     peak, peak_kind = measured_peak()
     alg = B_PER_PARTICLE * particles + B_PER_CELL * cells
     achieved = alg / (kern_ms / 1e3) / 1e9
-    prof = profile_counters(traffic_file)
+    prof = profile_counters(traffic_file) if traffic_file else {}
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic_per_launch(particles, cells, traffic_file), "peak_kind": peak_kind,
+            "traffic": traffic_per_launch(particles, cells, traffic_file) if traffic_file else None,
+            "peak_kind": peak_kind,
             "kernel": kernel, "kernel_ms": kern_ms, "alg_bytes_per_launch": alg,
             "alg_bytes": f"{B_PER_PARTICLE:g} B x {particles} particles + {B_PER_CELL:g} B x {cells} cells",
             # from the committed ncu capture (smsp__inst_executed / particles, and the lane
@@ -417,8 +420,9 @@ def measure_single(w, steps, warmup, seed, dist=None, sampler=None, timed_steps=
     return {"particles": n_particles, "ms": ms, "launches": launches, "clocks": clocks, "counters": counters,
             "value": n_particles * steps / (ms / 1e3), "ms_per_step": ms / steps,
             "phase_ms_per_step": dict(zip(("particles", "fold", "fields", "step"), phases)),
+            # the committed k_slot capture is of the thermal plasma (a 1024 x 256 crop)
             "roofline": roofline(n_particles, cells, phases[0], "k_slot<push,move> (fused push + move + deposit)",
-                                 "k_slot_traffic.json"),
+                                 "k_slot_traffic.json" if w["name"].startswith("thermal") else None),
             "diag": {"field_energy_E": diag[0], "field_energy_B": diag[1], "kinetic": diag[2]}}
 
 

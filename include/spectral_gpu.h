@@ -112,7 +112,7 @@ SPX_API const char* spx_version(void);
  * copied at the full host-link rate, in chunks of 2^22 particles); the call
  * returns once they are no longer read.  The context keeps its upload scratch
  * (4 B per particle of the largest species added, plus 2 x 96 MB) for later
- * uploads; spx_destroy releases it (spx_batch_prepare for batch members).
+ * uploads; spx_destroy releases it (spx_batch_destroy for batch members).
  * The species id (0, 1, ...) is written to *species_out. */
 SPX_API int spx_add_species(spx_ctx* ctx, float charge, float mass, float vth, uint64_t n, const uint64_t* ix,
                     const uint64_t* iy, const float* dx, const float* dy, const float* px, const float* py,
@@ -185,7 +185,11 @@ SPX_API int spx_get_field(spx_ctx* ctx, int32_t field, int32_t with_ghosts, floa
 /* Overwrite a spatial field (with ghosts).  Used by tests to impose fields. */
 SPX_API int spx_set_field(spx_ctx* ctx, int32_t field, const float* in_with_ghosts);
 /* The persistent k-space magnetic field at t+1/2 (Flds::b_*_wrk, src/flds/mod.rs:31-33),
- * size_y*size_x interleaved complex. comp 0,1,2 = x,y,z. */
+ * size_y*size_x interleaved complex. comp 0,1,2 = x,y,z.  B is real, so its spectrum
+ * is Hermitian: the library keeps kx in [0, size_x/2) (the update zeroes column
+ * size_x/2).  spx_get_bwrk fills kx > size_x/2 with the conjugate mirror
+ * conj(B[size_y - ky][size_x - kx]) and column size_x/2 with zeros; spx_set_bwrk
+ * keeps kx in [0, size_x/2) of its input. */
 SPX_API int spx_get_bwrk(spx_ctx* ctx, int32_t comp, float* out_complex);
 SPX_API int spx_set_bwrk(spx_ctx* ctx, int32_t comp, const float* in_complex);
 

@@ -36,7 +36,8 @@ struct Error {
 // ----------------------------------------------------------------------------
 // Grid geometry in the reference layout.
 //   spatial: (ny+2) x (nx+2) floats, row-major, ghost frame at row/col 0 and n+1
-//   spectral: ny x nx float2, row-major (ky rows, kx columns)
+//   spectral: ny x nx float2, row-major (ky rows, kx columns); the field update
+//   keeps the half spectrum of its real fields, ny x nx/2 (kx in [0, nx/2))
 // ----------------------------------------------------------------------------
 struct Grid {
   int nx, ny;      // interior cells
@@ -45,6 +46,7 @@ struct Grid {
   __host__ __device__ int sidx(int row, int col) const { return row * W + col; }
   __host__ __device__ size_t spatial_size() const { return (size_t)(ny + 2) * (size_t)W; }
   __host__ __device__ size_t spectral_size() const { return (size_t)ny * (size_t)nx; }
+  __host__ __device__ size_t half_spectral_size() const { return (size_t)ny * (size_t)(nx / 2); }
 };
 
 // Wave numbers restated from src/flds/wave_num.rs:18-33 in FP32 with the same

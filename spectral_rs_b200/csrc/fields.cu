@@ -2,15 +2,19 @@
 //
 // Data layout in HBM
 //   spatial fields: reference layout, (ny+2) x (nx+2) floats with a one-cell ghost frame
-//   spectral fields: ny x nx float2, row-major (ky rows, kx columns), numpy fft2 convention
+//   spectral fields: half spectra, ny x nx/2 float2, row-major (ky rows, kx in [0, nx/2)),
+//   numpy fft2 convention; the other half is the conjugate mirror (the fields are real)
+//   and column nx/2 is zero after every update
 //
 // Kernels per Flds::update (src/flds/mod.rs:87-309):
-//   k_filter      x n_pass : 3x3 binomial stencil of jx, jy, jz, dsty, ghost frame refilled
-//   k_rows<fwd>            : copy_to_spectral (+ dsty * 1/dens) fused with the row FFTs of 7 fields
-//   k_cols<fwd>            : column FFTs of the 7 fields, strip of W columns per CTA
+//   k_filter_fused         : n_pass 3x3 binomial passes of jx, jy, jz, dsty
+//   k_rows_r2c             : copy_to_spectral (+ dsty * 1/dens) fused with the row FFTs of
+//                            7 fields, two real rows per complex transform
+//   k_cols<fwd>            : column FFTs of the 7 half spectra, strip of W columns per CTA
 //   k_kspace               : Ampere, divergence correction, Faraday, Nyquist, B average
 //   k_cols<inv>            : column inverse FFTs of B(t) and E
-//   k_rows<inv>            : row inverse FFTs, 1/(nx ny) scale, copy_to_spatial + update_ghosts fused
+//   k_rows_c2r             : row inverse FFTs (two real rows per transform), 1/(nx ny)
+//                            scale, copy_to_spatial + update_ghosts fused
 //
 // The FFT is a Stockham autosort transform (radix 8 passes, one radix 4 or 2
 // pass for the remaining factor), one radix-8 butterfly per thread per pass:
@@ -278,12 +282,22 @@ __host__ __device__ inline int col_logW(int logNy, int logNx) {
 }
 
 // ---------------------------------------------------------------- row kernels
-// IN: 0 = real ghosted spatial field (copy_to_spectral fused), 1 = complex
-// OUT: 0 = complex, 1 = real ghosted spatial field (copy_to_spatial + update_ghosts fused)
+// The spatial fields are real, so each field's 2-D spectrum is Hermitian,
+// F[ky][nx - kx] = conj F[ny - ky][kx], and the update zeroes column kx = nx/2
+// (src/flds/mod.rs:230-266).  The field update therefore keeps the spectra of
+// columns kx in [0, nx/2) only (the "half spectrum", ny x nx/2 complex), and
+// its row transforms carry two real rows of a field in one complex FFT:
+//   forward  z = a + i b, Z = fft(z): A[k] = (Z[k] + conj Z[-k]) / 2,
+//                                     B[k] = (Z[k] - conj Z[-k]) / (2i);
+//   inverse  Z[k] = A[k] + i B[k] (negative k from conj A, conj B), z = ifft(Z):
+//            a = Re z, b = Im z.
+// The reference transforms each real field as a complex one (im = 0,
+// src/flds/field.rs:78-139) and keeps Re of the inverse; the pairing computes
+// the same DFT with half the transforms, so results agree to FP32 rounding.
 struct RowArgs {
   const void* src[8];
   void* dst[8];
-  float* back[8];  // IN == 0: when set, the input value is also stored here (ghosted, periodic ghosts)
+  float* back[8];  // forward: when set, the input value is also stored here (ghosted, periodic ghosts)
   float scale[8];
 };
 
@@ -316,11 +330,11 @@ __device__ __forceinline__ void store_ghosted(float* dst, const Grid& g, int row
 // of the passes folds); LOGN = 0 reads it from the grid.
 constexpr int FFT_LOGN_MIN = 6, FFT_LOGN_MAX = 13;
 
-template <int IN, int OUT, bool INV, bool SMALL, int LOGN>
-__global__ void FFT_BOUNDS(SMALL) k_rows(const __grid_constant__ RowArgs a0, const RowArgs* __restrict__ tab, Grid g0,
-                                         const float2* __restrict__ tw) {
+// Complex row FFTs of full ny x nx arrays (Fft2D on a complex array, the tests'
+// path): CTA = B = 2^row_logB rows of one field.
+template <bool INV, bool SMALL, int LOGN>
+__global__ void FFT_BOUNDS(SMALL) k_rows(const __grid_constant__ RowArgs a, Grid g0, const float2* __restrict__ tw) {
   extern __shared__ float2 sm[];
-  const RowArgs& a = tab ? tab[blockIdx.z] : a0;  // a batch: member blockIdx.z's fields
   Grid g = g0;
   if (LOGN) {
     g.log2nx = LOGN;
@@ -332,33 +346,16 @@ __global__ void FFT_BOUNDS(SMALL) k_rows(const __grid_constant__ RowArgs a0, con
   const int logB = row_logB(logN);
   const int row0 = blockIdx.x << logB;
   const float sc = a.scale[f];
-  // first-pass inputs straight from global memory: 8 independent loads per thread
   float2 v[8];
   {
     int t, j;
     bfly_tj<8>(0, logN, logB, false, t, j);
     const int row = row0 + t;
-    if (IN == 0) {
-      // all 8 loads first, then the write-back stores (which may not be reordered above them)
-      const float* __restrict__ src = (const float*)a.src[f];
-      float u[8];
+    const float2* __restrict__ src = (const float2*)a.src[f];
 #pragma unroll
-      for (int r = 0; r < 8; ++r) u[r] = row < g.ny ? src[(size_t)(row + 1) * g.W + j + r * (N >> 3) + 1] : 0.f;
-      if (a.back[f] && row < g.ny)
-#pragma unroll
-        for (int r = 0; r < 8; ++r) store_ghosted(a.back[f], g, row, j + r * (N >> 3), u[r]);
-#pragma unroll
-      for (int r = 0; r < 8; ++r) {
-        const float2 x = make_float2(u[r] * sc, 0.f * sc);
-        v[r] = INV ? c_conj(x) : x;
-      }
-    } else {
-      const float2* __restrict__ src = (const float2*)a.src[f];
-#pragma unroll
-      for (int r = 0; r < 8; ++r) {
-        const float2 x = row < g.ny ? src[(size_t)row * N + j + r * (N >> 3)] : make_float2(0.f, 0.f);
-        v[r] = INV ? c_conj(x) : x;
-      }
+    for (int r = 0; r < 8; ++r) {
+      const float2 x = row < g.ny ? src[(size_t)row * N + j + r * (N >> 3)] : make_float2(0.f, 0.f);
+      v[r] = INV ? c_conj(x) : x;
     }
   }
   block_fft_regs(v, sm, logN, logB, 1, N, false, tw);
@@ -370,14 +367,126 @@ __global__ void FFT_BOUNDS(SMALL) k_rows(const __grid_constant__ RowArgs a0, con
     if (row >= g.ny) continue;
     float2 x = v[m];
     if (INV) x = c_conj(x);
-    if (OUT == 0) {
-      float2* dst = (float2*)a.dst[f];
-      dst[(size_t)row * N + e] = INV ? c_scale(x, sc) : x;
-    } else {
-      // spatial = Re(ifft) * (1/(nx ny)); the CTA that owns row r also fills the
-      // ghost cells that are images of row r
-      store_ghosted((float*)a.dst[f], g, row, e, x.x * sc);
+    ((float2*)a.dst[f])[(size_t)row * N + e] = INV ? c_scale(x, sc) : x;
+  }
+}
+
+// Forward row transforms of real ghosted fields into half spectra (copy_to_spectral
+// fused, src/flds/field.rs:78-106): CTA = B = 2^row_logB pairs of rows (2p, 2p+1)
+// of field blockIdx.y, one complex FFT per pair.  a.scale multiplies the input
+// (1/dens for dsty, src/flds/mod.rs:66-85).
+template <bool SMALL, int LOGN>
+__global__ void FFT_BOUNDS(SMALL) k_rows_r2c(const __grid_constant__ RowArgs a0, const RowArgs* __restrict__ tab,
+                                             Grid g0, const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  const RowArgs& a = tab ? tab[blockIdx.z] : a0;  // a batch: member blockIdx.z's fields
+  Grid g = g0;
+  if (LOGN) {
+    g.log2nx = LOGN;
+    g.nx = 1 << LOGN;
+    g.W = g.nx + 2;
+  }
+  const int f = blockIdx.y;
+  const int logN = g.log2nx, N = g.nx, H = N >> 1;
+  const int logB = row_logB(logN);
+  const int p0 = blockIdx.x << logB, npairs = g.ny >> 1;
+  const float sc = a.scale[f];
+  float2 v[8];
+  {
+    int t, j;
+    bfly_tj<8>(0, logN, logB, false, t, j);
+    const int p = p0 + t;
+    const float* __restrict__ src = (const float*)a.src[f];
+    // all 16 loads first, then the write-back stores (which may not be reordered above them)
+    float u0[8], u1[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const size_t o = (size_t)(2 * p + 1) * g.W + j + r * (N >> 3) + 1;
+      u0[r] = p < npairs ? src[o] : 0.f;
+      u1[r] = p < npairs ? src[o + g.W] : 0.f;
     }
+    if (a.back[f] && p < npairs)
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        store_ghosted(a.back[f], g, 2 * p, j + r * (N >> 3), u0[r]);
+        store_ghosted(a.back[f], g, 2 * p + 1, j + r * (N >> 3), u1[r]);
+      }
+#pragma unroll
+    for (int r = 0; r < 8; ++r) v[r] = make_float2(u0[r] * sc, u1[r] * sc);
+  }
+  block_fft_regs(v, sm, logN, logB, 1, N, false, tw);  // ends with a barrier after the last reads
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    int t, e;
+    out_pos(m, logN, logB, false, t, e);
+    sm[spad(t * N + e)] = v[m];
+  }
+  __syncthreads();
+  // unpack: (pair t, k < N/2), four per thread, consecutive k on consecutive threads
+  float2* __restrict__ dst = (float2*)a.dst[f];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int b = threadIdx.x + q * blockDim.x;
+    const int t = b >> (logN - 1), k = b & (H - 1);
+    const int p = p0 + t;
+    const float2 zk = sm[spad(t * N + k)], zm = sm[spad(t * N + ((N - k) & (N - 1)))];
+    if (p < npairs) {
+      dst[(size_t)(2 * p) * H + k] = make_float2((zk.x + zm.x) * 0.5f, (zk.y - zm.y) * 0.5f);
+      dst[(size_t)(2 * p + 1) * H + k] = make_float2((zk.y + zm.y) * 0.5f, (zm.x - zk.x) * 0.5f);
+    }
+  }
+}
+
+// Inverse row transforms of half spectra into real ghosted fields (copy_to_spatial
+// and update_ghosts fused, src/flds/field.rs:108-257): pairs of rows as above;
+// a.scale = 1/(nx ny) (src/flds/fft_2d.rs:170-171).
+template <bool SMALL, int LOGN>
+__global__ void FFT_BOUNDS(SMALL) k_rows_c2r(const __grid_constant__ RowArgs a0, const RowArgs* __restrict__ tab,
+                                             Grid g0, const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  const RowArgs& a = tab ? tab[blockIdx.z] : a0;
+  Grid g = g0;
+  if (LOGN) {
+    g.log2nx = LOGN;
+    g.nx = 1 << LOGN;
+    g.W = g.nx + 2;
+  }
+  const int f = blockIdx.y;
+  const int logN = g.log2nx, N = g.nx, H = N >> 1;
+  const int logB = row_logB(logN);
+  const int p0 = blockIdx.x << logB, npairs = g.ny >> 1;
+  const float sc = a.scale[f];
+  float2 v[8];
+  {
+    int t, j;
+    bfly_tj<8>(0, logN, logB, false, t, j);
+    const int p = p0 + t;
+    const float2* __restrict__ s0 = (const float2*)a.src[f] + (size_t)(2 * p) * H;
+    const float2* __restrict__ s1 = s0 + H;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      // inputs r < 4 lie in [0, N/2), inputs r >= 4 in [N/2, N): their conjugate partners
+      const int e = j + r * (N >> 3);
+      const int k = r < 4 ? e : (N - e) & (N - 1);
+      float2 z = make_float2(0.f, 0.f);
+      if (p < npairs && (r < 4 || e != H)) {  // column N/2 is zero
+        const float2 x = s0[k], y = s1[k];
+        z = r < 4 ? make_float2(x.x - y.y, x.y + y.x)   // A + i B
+                  : make_float2(x.x + y.y, y.x - x.y);  // conj A + i conj B
+      }
+      v[r] = c_conj(z);  // inverse as conj(fft(conj(Z)))
+    }
+  }
+  block_fft_regs(v, sm, logN, logB, 1, N, false, tw);
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    int t, e;
+    out_pos(m, logN, logB, false, t, e);
+    const int p = p0 + t;
+    if (p >= npairs) continue;
+    // Re and Im of the inverse (the conjugation of the result flips only Im)
+    store_ghosted((float*)a.dst[f], g, 2 * p, e, v[m].x * sc);
+    store_ghosted((float*)a.dst[f], g, 2 * p + 1, e, -v[m].y * sc);
   }
 }
 
@@ -421,16 +530,19 @@ __global__ void FFT_BOUNDS(SMALL) k_cols(const __grid_constant__ ColArgs a0, con
 }
 
 // ---------------------------------------------------------------- k-space update
-// src/flds/mod.rs:105-278 for one k point; num_complex operation order.
+// src/flds/mod.rs:105-278 for one k point; num_complex operation order.  Over the
+// half spectrum (kx = j in [0, nx/2), ny x nx/2 points): the update is pointwise
+// and maps a Hermitian spectrum to a Hermitian one, and it zeroes column nx/2.
 struct KArgs {
   float2 *jx, *jy, *jz, *rho, *ex, *ey, *ez, *bwx, *bwy, *bwz, *bax, *bay, *baz;
   float cdt, ckc;
 };
 __global__ void k_kspace(const __grid_constant__ KArgs a0, const KArgs* __restrict__ tab, Grid g) {
   const KArgs& a = tab ? tab[blockIdx.y] : a0;
-  const size_t n = (size_t)g.nx * g.ny;
+  const size_t n = g.half_spectral_size();
+  const int logH = g.log2nx - 1;
   for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(idx >> g.log2nx), j = (int)(idx & (g.nx - 1));
+    const int i = (int)(idx >> logH), j = (int)(idx & ((1 << logH) - 1));
     const float kx = wave_kx(j, g.nx), ky = wave_kx(i, g.ny);
     float2 Jx = a.jx[idx], Jy = a.jy[idx], Jz = a.jz[idx], Rho = a.rho[idx];
     if (idx == 0) {  // mod.rs:106-107 (j_z[0] is not zeroed)
@@ -462,8 +574,8 @@ __global__ void k_kspace(const __grid_constant__ KArgs a0, const KArgs* __restri
     float2 nBy = c_add(By, c_mul(make_float2(0.0f * kx, cdt * kx), Ez));
     float2 nBz = c_add(Bz, c_mul(make_float2(0.0f, cdt),
                                  c_sub(make_float2(ky * Ex.x, ky * Ex.y), make_float2(kx * Ey.x, kx * Ey.y))));
-    // Nyquist column kx = nx/2 and row ky = ny/2 (mod.rs:230-266)
-    if (j == g.nx / 2 || i == g.ny / 2) {
+    // Nyquist row ky = ny/2 (mod.rs:230-266); column kx = nx/2 is not stored
+    if (i == g.ny / 2) {
       const float2 z = make_float2(0.f, 0.f);
       nBx = nBy = nBz = z;
       Ex = Ey = Ez = z;
@@ -755,20 +867,18 @@ static void fft_attr(const void* f) {
 template <int LOGN>
 static void fft_set_kernel_attributes() {
   if constexpr (LOGN == 0) {
-    fft_attr((const void*)k_rows<0, 0, false, true, 0>);
-    fft_attr((const void*)k_rows<1, 0, false, true, 0>);
-    fft_attr((const void*)k_rows<1, 0, true, true, 0>);
-    fft_attr((const void*)k_rows<1, 1, true, true, 0>);
-    fft_attr((const void*)k_rows<0, 0, false, false, 0>);
-    fft_attr((const void*)k_rows<1, 0, false, false, 0>);
-    fft_attr((const void*)k_rows<1, 0, true, false, 0>);
-    fft_attr((const void*)k_rows<1, 1, true, false, 0>);
+    for (bool S : {true, false}) {
+      fft_attr(S ? (const void*)k_rows<false, true, 0> : (const void*)k_rows<false, false, 0>);
+      fft_attr(S ? (const void*)k_rows<true, true, 0> : (const void*)k_rows<true, false, 0>);
+      fft_attr(S ? (const void*)k_rows_r2c<true, 0> : (const void*)k_rows_r2c<false, 0>);
+      fft_attr(S ? (const void*)k_rows_c2r<true, 0> : (const void*)k_rows_c2r<false, 0>);
+    }
   } else {
     constexpr bool S = rows_small(LOGN);
-    fft_attr((const void*)k_rows<0, 0, false, S, LOGN>);
-    fft_attr((const void*)k_rows<1, 0, false, S, LOGN>);
-    fft_attr((const void*)k_rows<1, 0, true, S, LOGN>);
-    fft_attr((const void*)k_rows<1, 1, true, S, LOGN>);
+    fft_attr((const void*)k_rows<false, S, LOGN>);
+    fft_attr((const void*)k_rows<true, S, LOGN>);
+    fft_attr((const void*)k_rows_r2c<S, LOGN>);
+    fft_attr((const void*)k_rows_c2r<S, LOGN>);
   }
   fft_attr((const void*)k_cols<false, true, LOGN>);
   fft_attr((const void*)k_cols<true, true, LOGN>);
@@ -784,24 +894,53 @@ void fields_set_kernel_attributes() {
   fft_attr((const void*)k_filter_fused);
 }
 
-// tab: a batch of nm simulations of grid g (member blockIdx.z's arguments), else a alone (nm = 1)
-template <int IN, int OUT, bool INV, int LOGN>
-static void launch_rows_n(const Grid& g, const RowArgs& a, const RowArgs* tab, int nf, int nm, const float2* tw,
-                          cudaStream_t st) {
+// Complex row FFTs of a full array (tests).
+template <bool INV, int LOGN>
+static void launch_rows_n(const Grid& g, const RowArgs& a, int nf, const float2* tw, cudaStream_t st) {
   const int logB = row_logB(g.log2nx);
   const int threads = std::max(1, (g.nx << logB) / 8);
   const size_t smem = sizeof(float2) * fft_smem_elems(g.log2nx, logB);
   const int blocks = (g.ny + (1 << logB) - 1) >> logB;
   if constexpr (LOGN > 0) {
-    k_rows<IN, OUT, INV, rows_small(LOGN), LOGN><<<dim3(blocks, nf, nm), threads, smem, st>>>(a, tab, g, tw);
+    k_rows<INV, rows_small(LOGN), LOGN><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
   } else {
     if (threads <= 512)
-      k_rows<IN, OUT, INV, true, 0><<<dim3(blocks, nf, nm), threads, smem, st>>>(a, tab, g, tw);
+      k_rows<INV, true, 0><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
     else
-      k_rows<IN, OUT, INV, false, 0><<<dim3(blocks, nf, nm), threads, smem, st>>>(a, tab, g, tw);
+      k_rows<INV, false, 0><<<dim3(blocks, nf), threads, smem, st>>>(a, g, tw);
   }
 }
 
+// Real-pair row transforms of the field update (forward r2c or inverse c2r);
+// tab: a batch of nm simulations of grid g (member blockIdx.z's arguments), else a alone (nm = 1)
+template <bool INV, int LOGN>
+static void launch_pair_rows_n(const Grid& g, const RowArgs& a, const RowArgs* tab, int nf, int nm,
+                               const float2* tw, cudaStream_t st) {
+  const int logB = row_logB(g.log2nx);
+  const int threads = std::max(1, (g.nx << logB) / 8);
+  const size_t smem = sizeof(float2) * fft_smem_elems(g.log2nx, logB);
+  const int blocks = ((g.ny >> 1) + (1 << logB) - 1) >> logB;
+  const dim3 grid(blocks, nf, nm);
+  if constexpr (LOGN > 0) {
+    constexpr bool S = rows_small(LOGN);
+    if (INV)
+      k_rows_c2r<S, LOGN><<<grid, threads, smem, st>>>(a, tab, g, tw);
+    else
+      k_rows_r2c<S, LOGN><<<grid, threads, smem, st>>>(a, tab, g, tw);
+  } else if (threads <= 512) {
+    if (INV)
+      k_rows_c2r<true, 0><<<grid, threads, smem, st>>>(a, tab, g, tw);
+    else
+      k_rows_r2c<true, 0><<<grid, threads, smem, st>>>(a, tab, g, tw);
+  } else {
+    if (INV)
+      k_rows_c2r<false, 0><<<grid, threads, smem, st>>>(a, tab, g, tw);
+    else
+      k_rows_r2c<false, 0><<<grid, threads, smem, st>>>(a, tab, g, tw);
+  }
+}
+
+// g: the grid of the columns (for the half spectra, half_grid of the simulation's)
 template <bool INV, int LOGN>
 static void launch_cols_n(const Grid& g, const ColArgs& a, const ColArgs* tab, int nf, int nm, const float2* tw,
                           cudaStream_t st) {
@@ -829,10 +968,17 @@ static void launch_cols_n(const Grid& g, const ColArgs& a, const ColArgs* tab, i
     default: CALL(0); break;    \
   }
 
-template <int IN, int OUT, bool INV>
-static void launch_rows(const Grid& g, const RowArgs& a, int nf, const float2* tw, cudaStream_t st,
-                        const RowArgs* tab = nullptr, int nm = 1) {
-#define SPX_ROWS(L) launch_rows_n<IN, OUT, INV, L>(g, a, tab, nf, nm, tw, st)
+template <bool INV>
+static void launch_rows(const Grid& g, const RowArgs& a, int nf, const float2* tw, cudaStream_t st) {
+#define SPX_ROWS(L) launch_rows_n<INV, L>(g, a, nf, tw, st)
+  FFT_DISPATCH(g.log2nx, SPX_ROWS)
+#undef SPX_ROWS
+}
+
+template <bool INV>
+static void launch_pair_rows(const Grid& g, const RowArgs& a, int nf, const float2* tw, cudaStream_t st,
+                             const RowArgs* tab = nullptr, int nm = 1) {
+#define SPX_ROWS(L) launch_pair_rows_n<INV, L>(g, a, tab, nf, nm, tw, st)
   FFT_DISPATCH(g.log2nx, SPX_ROWS)
 #undef SPX_ROWS
 }
@@ -843,6 +989,15 @@ static void launch_cols(const Grid& g, const ColArgs& a, int nf, const float2* t
 #define SPX_COLS(L) launch_cols_n<INV, L>(g, a, tab, nf, nm, tw, st)
   FFT_DISPATCH(g.log2ny, SPX_COLS)
 #undef SPX_COLS
+}
+
+// The half-spectrum arrays as a grid of nx/2 columns (the column transforms'
+// view; the spatial pitch W is not used there).
+static Grid half_grid(const Grid& g) {
+  Grid h = g;
+  h.nx = g.nx / 2;
+  h.log2nx = g.log2nx - 1;
+  return h;
 }
 
 void FieldBuffers::allocate(const Grid& grid) {
@@ -856,7 +1011,7 @@ void FieldBuffers::allocate(const Grid& grid) {
     SPX_CUDA_TRY(cudaMalloc(&filt_tmp[i], ss));
     SPX_CUDA_TRY(cudaMemset(filt_tmp[i], 0, ss));
   }
-  const size_t cs = g.spectral_size() * sizeof(float2);
+  const size_t cs = g.half_spectral_size() * sizeof(float2);
   for (int i = 0; i < SP_COUNT; ++i) {
     SPX_CUDA_TRY(cudaMalloc(&spec[i], cs));
     SPX_CUDA_TRY(cudaMemset(spec[i], 0, cs));
@@ -946,7 +1101,7 @@ static RowArgs rows_inv_args(const FieldBuffers& fb) {
   return a;
 }
 static int kspace_blocks(const Grid& g, int nm) {
-  const size_t n = g.spectral_size();
+  const size_t n = g.half_spectral_size();
   return (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, (size_t)148 * 16 / (size_t)nm));
 }
 
@@ -974,15 +1129,15 @@ int field_update(FieldBuffers& fb, cudaStream_t st) {
     }
   }
   // 2. forward transforms
-  launch_rows<0, 0, false>(g, rows_fwd_args(fb, fused), 7, fb.tw_x, st);
-  launch_cols<false>(g, cols_fwd_args(fb), 7, fb.tw_y, st);
+  launch_pair_rows<false>(g, rows_fwd_args(fb, fused), 7, fb.tw_x, st);
+  launch_cols<false>(half_grid(g), cols_fwd_args(fb), 7, fb.tw_y, st);
   launches += 2;
   // 3. k-space update (mod.rs:105-278)
   k_kspace<<<kspace_blocks(g, 1), 256, 0, st>>>(kspace_args(fb), nullptr, g);
   ++launches;
   // 4. inverse transforms
-  launch_cols<true>(g, cols_inv_args(fb), 6, fb.tw_y, st);
-  launch_rows<1, 1, true>(g, rows_inv_args(fb), 6, fb.tw_x, st);
+  launch_cols<true>(half_grid(g), cols_inv_args(fb), 6, fb.tw_y, st);
+  launch_pair_rows<true>(g, rows_inv_args(fb), 6, fb.tw_x, st);
   launches += 2;
   SPX_CUDA_TRY(cudaGetLastError());
   return launches;
@@ -1150,11 +1305,11 @@ int field_batch_update(FieldBatch* b, cudaStream_t st) {
         const dim3 grd((g.nx + tw - 1) / tw, (g.ny + FILT_TY - 1) / FILT_TY, 4 * nm);
         k_filter_fused<<<grd, 256, smem, gs>>>(ConstFieldList{}, FieldList{}, G.fsrc, G.fdst, 4, g, (int)G.n_pass);
       }
-      launch_rows<0, 0, false>(g, RowArgs{}, 7, f0.tw_x, gs, G.rf, nm);
-      launch_cols<false>(g, ColArgs{}, 7, f0.tw_y, gs, G.cf, nm);
+      launch_pair_rows<false>(g, RowArgs{}, 7, f0.tw_x, gs, G.rf, nm);
+      launch_cols<false>(half_grid(g), ColArgs{}, 7, f0.tw_y, gs, G.cf, nm);
       k_kspace<<<dim3(kspace_blocks(g, nm), nm), 256, 0, gs>>>(KArgs{}, G.ks, g);
-      launch_cols<true>(g, ColArgs{}, 6, f0.tw_y, gs, G.ci, nm);
-      launch_rows<1, 1, true>(g, RowArgs{}, 6, f0.tw_x, gs, G.ri, nm);
+      launch_cols<true>(half_grid(g), ColArgs{}, 6, f0.tw_y, gs, G.ci, nm);
+      launch_pair_rows<true>(g, RowArgs{}, 6, f0.tw_x, gs, G.ri, nm);
       launches += 6;
     }
     SPX_CUDA_TRY(cudaEventRecord(G.done, gs));
@@ -1173,12 +1328,12 @@ int fft2d_inplace(const Grid& g, float2* data, const float2* tw_x, const float2*
   c.data[0] = data;
   if (!inverse) {
     a.scale[0] = 1.0f;
-    launch_rows<1, 0, false>(g, a, 1, tw_x, st);
+    launch_rows<false>(g, a, 1, tw_x, st);
     launch_cols<false>(g, c, 1, tw_y, st);
   } else {
     // reference order: rows then columns, then the 1/(nx ny) scale (fft_2d.rs:132-172)
     a.scale[0] = 1.0f;
-    launch_rows<1, 0, true>(g, a, 1, tw_x, st);
+    launch_rows<true>(g, a, 1, tw_x, st);
     launch_cols<true>(g, c, 1, tw_y, st);
     const size_t n = g.spectral_size();
     const float norm = 1.0f / (float)n;

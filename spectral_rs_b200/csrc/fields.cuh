@@ -6,7 +6,8 @@
 
 namespace spx {
 
-// Spectral work arrays, ny x nx float2 each (row-major, ky rows).
+// Spectral work arrays: half spectra, ny x nx/2 float2 each (row-major, ky rows,
+// kx in [0, nx/2); kx in (nx/2, nx) is the conjugate mirror, column nx/2 is zero).
 enum SpecId {
   SP_JX = 0, SP_JY, SP_JZ, SP_RHO,  // forward transforms of the filtered sources
   SP_EX, SP_EY, SP_EZ,              // E(k): forward transform, updated in place

@@ -100,8 +100,8 @@ def _field_state(nx, ny, seed):
 
 
 # includes the benchmark's row length (4096) and column lengths (1024, 2048), the 8192-point
-# rows, every column length of the fused column pass (16 .. 4096: strips of 2048 points, one
-# 4096-point column) and the 8192-point columns of the three-kernel column path
+# rows and columns, the shortest rows (8 points: a half spectrum of 4 columns) and every column
+# length from 16 to 8192
 @pytest.mark.parametrize("nx,ny,n_pass", [(64, 32, 4), (128, 64, 1), (512, 64, 4), (4096, 64, 4), (1024, 256, 2),
                                           (8192, 16, 8), (64, 1024, 4), (32, 2048, 8), (16, 4096, 4),
                                           (16, 8192, 4), (8, 128, 4), (256, 512, 4)])
@@ -139,3 +139,35 @@ def test_gpu_fields_update_vs_oracle(nx, ny, n_pass):
             g, r = sim.flds.b_wrk(c), o64.b_wrk(c)
             rel = np.max(np.abs(g - r)) / max(np.max(np.abs(r)), 1e-30)
             assert rel < 1e-5, ("bwrk", c, rel)
+
+
+@pytest.mark.parametrize("nx,ny", [(64, 32), (8, 16), (256, 128)])
+def test_gpu_bwrk_half_spectrum(nx, ny):
+    """B_wrk lives on the device as the kx < nx/2 half of a Hermitian spectrum: set keeps that
+    half bit for bit, get completes the rest by the conjugate mirror with column nx/2 zero, and
+    after field updates the array a caller reads is still the spectrum of a real field."""
+    from spectral_rs_b200 import Sim
+    from conftest import test_params
+    from spectral_rs_b200.config import Config, Setup, Output
+    p = test_params(size_x=nx, size_y=ny, delta=4, dt=0.1, c=3.0, dens=8, n_pass=4, periodic_x=True)
+    cfg = Config(p, Setup(1), Output(False, False, 1, 1, 1, 1))
+    st, bw = _field_state(nx, ny, seed=7 * nx + ny)
+    H = nx // 2
+    with Sim(cfg) as sim:
+        for c in range(3):
+            sim.flds.set_b_wrk(c, bw[c])
+            got = sim.flds.b_wrk(c)
+            assert np.array_equal(got[:, :H], bw[c][:, :H])
+            assert not np.any(got[:, H])
+            mirror = np.conj(got[(-np.arange(ny)) % ny][:, (nx - np.arange(H + 1, nx))])
+            assert np.array_equal(got[:, H + 1:], mirror)
+        for name, arr in st.items():
+            sim.flds.set_spatial(name, arr)
+        for _ in range(2):
+            sim.flds.update()
+        for c in range(3):
+            got = sim.flds.b_wrk(c).astype(np.complex128)
+            assert not np.any(got[:, H]) and not np.any(got[ny // 2])
+            # column kx = 0 and row ky = 0 are their own mirrors, held to FP32 rounding only
+            spatial = np.fft.ifft2(got)
+            assert np.max(np.abs(spatial.imag)) <= 1e-5 * max(np.max(np.abs(spatial.real)), 1e-30)
