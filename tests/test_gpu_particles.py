@@ -105,6 +105,54 @@ def test_move_and_deposit_bit_exact(periodic, tile):
     sim.close()
 
 
+def _uneven_species(p, seed, vth, gamma):
+    """Clustered occupancy: every eleventh cell holds 40 particles, the others 0-2, so a warp's
+    cells hold very different counts and its balanced rounds hand the excess of the full
+    cells to the lanes of the empty ones (helper rounds)."""
+    from spectral_rs_b200.init import draws, velocities
+    rng = np.random.default_rng(seed)
+    ix, iy = [], []
+    for y in range(1, p.size_y + 1):
+        for x in range(p.delta + 1, p.size_x - p.delta + 1):
+            n = 40 if (7 * x + 3 * y) % 11 == 0 else int(rng.integers(0, 3))
+            ix += [x] * n
+            iy += [y] * n
+    ix, iy = np.array(ix, dtype=np.uint64), np.array(iy, dtype=np.uint64)
+    n = len(ix)
+    dx = (rng.random(n, dtype=np.float32) - np.float32(0.5)).astype(np.float32)
+    dy = (rng.random(n, dtype=np.float32) - np.float32(0.5)).astype(np.float32)
+    nrm, uni = draws(n, rng)
+    px, py, pz, psa = velocities(nrm, uni, p.c, vth, gamma, 1.0)
+    return dict(ix=ix, iy=iy, dx=dx, dy=dy, px=px, py=py, pz=pz, psa=psa)
+
+
+@pytest.mark.parametrize("tile", [(8, 8), (16, 16)])
+@pytest.mark.parametrize("periodic", [True, False])
+def test_uneven_cells_bit_exact(periodic, tile):
+    """Cells with very different counts (excess particles moved in helper rounds): particle
+    state bit-exact and deposits within tolerance over three push + move cycles."""
+    cfg = _cfg(size_x=64, size_y=32, delta=6, c=4.5, dt=0.1, dens=8, periodic_x=periodic, left_wall=not periodic,
+               tile_x=tile[0], tile_y=tile[1])
+    p = cfg.params
+    specs = [(1.0, 16.0, 0.1, _uneven_species(p, 21, 0.1, 1.0050378)),
+             (-1.0, 1.0, 0.3, _uneven_species(p, 22, 0.3, 1.2))]
+    sim, o = _pair(cfg, specs)
+    _random_fields(sim, o, 23)
+    for cycle in range(3):
+        for s in range(2):
+            sim.prtls[s].boris_push()
+            o.boris_push(s)
+            _assert_state_equal(sim.prtls[s].state(), o.state(s))
+        sim.zero_sources()
+        o.zero_sources()
+        for s in range(2):
+            sim.move_and_deposit(sim.prtls[s])
+            o.move_and_deposit(s)
+            _assert_state_equal(sim.prtls[s].state(), o.state(s))
+        _assert_moments_close(sim, o)
+    sim.close()
+
+
 def test_wall_reflection_bit_exact():
     # fast particles driven into the reflecting wall (src/prtls.rs:153-188), several moves
     cfg = _cfg(size_x=32, size_y=16, delta=4, c=4.5, dt=0.1, dens=4, periodic_x=False)
