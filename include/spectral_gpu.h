@@ -81,7 +81,7 @@ typedef struct spx_params {
                           reference's assertion min(ix) > delta (src/prtls.rs:163-170)     */
   /* --- B200 additions (0 = automatic) --- */
   int32_t path;        /* SPX_PATH_SPLIT or SPX_PATH_PLAIN                                */
-  int32_t tile_x;      /* cells per tile in x (split path); power of two; 0 with tile_y 0: 8x8 */
+  int32_t tile_x;      /* cells per tile in x (split path); power of two; 0: 16 (tile_y 0: 8)   */
   int32_t tile_y;      /* cells per tile in y                                              */
   int32_t slot_capacity; /* minimum particle slots per cell and species (split path);
                           negative: exactly -slot_capacity (testing the overflow path)  */

@@ -399,8 +399,10 @@ __device__ __noinline__ void drain_m_fn(const StepArgs& a, const SpeciesArgs& S,
 #ifndef SPX_SLOT8_MIN_BLOCKS
 #define SPX_SLOT8_MIN_BLOCKS 10
 #endif
-#define SPX_SLOT_BOUNDS(TS) \
-  __launch_bounds__((TS) == 8 ? 64 : 256, (TS) == 8 ? SPX_SLOT8_MIN_BLOCKS : SPX_SLOT_MIN_BLOCKS)
+// 16x8 tiles (128-thread CTAs, tile code 168): five per SM, the same 96 registers and 20 warps
+#define SPX_SLOT_BOUNDS(TS)                                      \
+  __launch_bounds__((TS) == 8 ? 64 : (TS) == 168 ? 128 : 256,    \
+                    (TS) == 8 ? SPX_SLOT8_MIN_BLOCKS : (TS) == 168 ? SPX_SLOT8_MIN_BLOCKS / 2 : SPX_SLOT_MIN_BLOCKS)
 // apply_bc of a grid periodic in x as well as y (the reference's `periodic`
 // feature) when the kernel knows it at compile time.
 __device__ __forceinline__ void periodic_bc(int nx, int ny, int& ix, int& iy) {
@@ -443,14 +445,15 @@ __device__ __forceinline__ void bc_of(const StepArgs& a, int nx, int ny, int& ix
   }
 }
 
-// BC: see bc_of.  TS: square tiles of TS x TS cells known at compile time (16 or 8: the
+// BC: see bc_of.  TS: the tile shape known at compile time (16: 16x16, 8: 8x8, 168: 16x8; the
 // index arithmetic folds), 0: the tile shape from a.
 // Species [s0, s1) of the step (all of them, or one per CTA when a small grid
 // splits the species across CTAs).
 template <bool PUSH, bool MOVE, bool COMP = false, int BC = BC_ANY, int TS = 0>
 __device__ __forceinline__ void slot_tile(const StepArgs& a, const int tile, float* smem, const int s0,
                                           const int s1) {
-  const int TXc = TS ? TS : a.TX, TYc = TS ? TS : a.TY, logTXc = TS == 16 ? 4 : TS == 8 ? 3 : a.logTX;
+  constexpr int TSX = TS == 168 ? 16 : TS, TSY = TS == 168 ? 8 : TS;
+  const int TXc = TSX ? TSX : a.TX, TYc = TSY ? TSY : a.TY, logTXc = TSX == 16 ? 4 : TSX == 8 ? 3 : a.logTX;
   const int TC = TXc * TYc;
   const int tx = tile % a.NTX, ty = tile / a.NTX;
   const int c = threadIdx.x;
@@ -1052,11 +1055,12 @@ void slot_set_kernel_attributes() {
   set_attributes<0>();
   set_attributes<8>();
   set_attributes<16>();
+  set_attributes<168>();
 }
 
-// compile-time tile side of a tile shape: 16, 8, or 0 (any other shape)
+// compile-time tile code of a tile shape: 16 (16x16), 8 (8x8), 168 (16x8) or 0 (any other shape)
 static int tile_side(const ParticleGeom& pg) {
-  return pg.TX == 16 && pg.TY == 16 ? 16 : pg.TX == 8 && pg.TY == 8 ? 8 : 0;
+  return pg.TX == 16 && pg.TY == 16 ? 16 : pg.TX == 8 && pg.TY == 8 ? 8 : pg.TX == 16 && pg.TY == 8 ? 168 : 0;
 }
 
 int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysParams& pp, const FieldPtrs& fp,
@@ -1087,13 +1091,15 @@ int slot_step(Species* sp, int s0, int s1, const ParticleGeom& pg, const PhysPar
   const bool split = a.ns > 1 && (size_t)pg.ntiles() * TC < (size_t)148 * 512;
   const dim3 grid(pg.ntiles(), split ? a.ns : 1);
   if (pp.periodic_x)
-    ts == 16 ? launch_slot<BC_PERIODIC, 16>(push, move, comp, grid, TC, smem, st, a)
-    : ts == 8 ? launch_slot<BC_PERIODIC, 8>(push, move, comp, grid, TC, smem, st, a)
-              : launch_slot<BC_PERIODIC, 0>(push, move, comp, grid, TC, smem, st, a);
+    ts == 16    ? launch_slot<BC_PERIODIC, 16>(push, move, comp, grid, TC, smem, st, a)
+    : ts == 8   ? launch_slot<BC_PERIODIC, 8>(push, move, comp, grid, TC, smem, st, a)
+    : ts == 168 ? launch_slot<BC_PERIODIC, 168>(push, move, comp, grid, TC, smem, st, a)
+                : launch_slot<BC_PERIODIC, 0>(push, move, comp, grid, TC, smem, st, a);
   else
-    ts == 16 ? launch_slot<BC_WALL, 16>(push, move, comp, grid, TC, smem, st, a)
-    : ts == 8 ? launch_slot<BC_WALL, 8>(push, move, comp, grid, TC, smem, st, a)
-              : launch_slot<BC_WALL, 0>(push, move, comp, grid, TC, smem, st, a);
+    ts == 16    ? launch_slot<BC_WALL, 16>(push, move, comp, grid, TC, smem, st, a)
+    : ts == 8   ? launch_slot<BC_WALL, 8>(push, move, comp, grid, TC, smem, st, a)
+    : ts == 168 ? launch_slot<BC_WALL, 168>(push, move, comp, grid, TC, smem, st, a)
+                : launch_slot<BC_WALL, 0>(push, move, comp, grid, TC, smem, st, a);
   ++launches;
   for (int s = 0; s < a.ns; ++s) {
     // the overflow fallback reads its count on the device; a small fixed grid covers it
@@ -1168,9 +1174,10 @@ void slot_batch_build(SlotBatch& b, const std::vector<SlotBatchSim>& sims) {
   const size_t smem = slot_smem_floats(sims[0].pg.TX, sims[0].pg.TY, true, true) * sizeof(float);
   // resident CTAs of the instantiation the steps launch (its register budget depends on the tile shape)
   const int ts = tile_side(sims[0].pg);
-  const void* kern = ts == 16 ? (const void*)k_slot_batch<true, true, BC_ANY, 16>
-                     : ts == 8 ? (const void*)k_slot_batch<true, true, BC_ANY, 8>
-                               : (const void*)k_slot_batch<true, true, BC_ANY, 0>;
+  const void* kern = ts == 16    ? (const void*)k_slot_batch<true, true, BC_ANY, 16>
+                     : ts == 8   ? (const void*)k_slot_batch<true, true, BC_ANY, 8>
+                     : ts == 168 ? (const void*)k_slot_batch<true, true, BC_ANY, 168>
+                                 : (const void*)k_slot_batch<true, true, BC_ANY, 0>;
   int per_sm = 0;
   SPX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, sims[0].pg.TC(), smem));
   int dev = 0, nsm = 0;
@@ -1205,10 +1212,11 @@ int slot_batch_step(SlotBatch& b, std::vector<SlotBatchSim>& sims, bool push, bo
     all_wall = all_wall && !m.pp.periodic_x;
   }
   const int bc = all_periodic ? BC_PERIODIC : all_wall ? BC_WALL : BC_ANY;
-#define SPX_BATCH(BCV)                                                     \
-  (ts == 16  ? launch_batch<BCV, 16>(push, move, b, TC, smem, st, args)    \
-   : ts == 8 ? launch_batch<BCV, 8>(push, move, b, TC, smem, st, args)     \
-             : launch_batch<BCV, 0>(push, move, b, TC, smem, st, args))
+#define SPX_BATCH(BCV)                                                       \
+  (ts == 16    ? launch_batch<BCV, 16>(push, move, b, TC, smem, st, args)    \
+   : ts == 8   ? launch_batch<BCV, 8>(push, move, b, TC, smem, st, args)     \
+   : ts == 168 ? launch_batch<BCV, 168>(push, move, b, TC, smem, st, args)   \
+               : launch_batch<BCV, 0>(push, move, b, TC, smem, st, args))
   if (bc == BC_PERIODIC)
     SPX_BATCH(BC_PERIODIC);
   else if (bc == BC_WALL)

@@ -64,7 +64,7 @@ def _assert_moments_close(sim, o, names=("Jx", "Jy", "Jz", "Rho", "Dens"), rtol=
         assert err < rtol, (name, err)
 
 
-TILES = [(0, 0), (16, 16)]  # the library's choice for these small grids, and the 16x16 instantiation
+TILES = [(0, 0), (16, 16), (16, 8)]  # the library's choice (8x8), the 16x16 and 16x8 instantiations
 
 
 @pytest.mark.parametrize("tile", TILES)
@@ -126,7 +126,7 @@ def _uneven_species(p, seed, vth, gamma):
     return dict(ix=ix, iy=iy, dx=dx, dy=dy, px=px, py=py, pz=pz, psa=psa)
 
 
-@pytest.mark.parametrize("tile", [(8, 8), (16, 16)])
+@pytest.mark.parametrize("tile", [(8, 8), (16, 16), (16, 8)])
 @pytest.mark.parametrize("periodic", [True, False])
 def test_uneven_cells_bit_exact(periodic, tile):
     """Cells with very different counts (excess particles moved in helper rounds): particle
